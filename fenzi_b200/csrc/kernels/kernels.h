@@ -1,0 +1,120 @@
+// Launch interfaces of the sm_100a kernels (host side of each .cu file).
+#pragma once
+#include "common.cuh"
+
+namespace fzk {
+
+constexpr int kColCap = 4096;  // atoms per column sorted in shared memory
+enum : int { CNT_TILES = 0, CNT_MASKS, CNT_SLOTS, CNT_REBUILDS, CNT_PAIRS, CNT_COUNT = 8 };
+
+struct RebuildArgs {
+  SysParams p;
+  int* flag;
+  int* counters;
+  int* status;
+  float4* pos4;
+  float4* pos_build;
+  const int* type;
+  int *col_of, *col_count, *col_cursor, *col_start, *col_tmp;
+  int *perm, *inv_perm;
+  float4* xyzq_s;
+  int* typ_s;
+  float4 *bb_lo, *bb_hi;
+  const int *excl_off, *excl_idx;
+  int* tile_i;
+  uint32_t* tile_j;
+  int* tile_m;
+  uint32_t* masks;
+  int tile_cap, mask_cap, all_images;
+};
+void launch_rebuild(const RebuildArgs& a, cudaStream_t st);
+
+struct NonbondedArgs {
+  SysParams p;
+  const float4* xyzq_s;
+  const int* typ_s;
+  const int* perm;
+  const int* tile_i;
+  const uint32_t* tile_j;
+  const int* tile_m;
+  const uint32_t* masks;
+  const int* counters;
+  const float2* ljtab;  // (ntypes+1)^2 (4 eps, sigma^2)
+  long long* facc;      // 3 x n fixed point
+  long long* energy;    // energy slots
+  int tile_cap;
+  int grid;
+};
+void launch_nonbonded(const NonbondedArgs& a, bool energy, cudaStream_t st);
+
+struct PmeArgs {
+  SysParams p;
+  const float4* pos4;
+  int n;
+  int K[3];
+  int B[3];     // brick edge per dimension
+  int nb[3];    // bricks per dimension
+  int* brick_of;     // [n]
+  int* brick_count;  // [nbricks]
+  int* brick_cursor;
+  int* brick_start;  // [nbricks+1]
+  int* brick_atoms;  // [n]
+  float* grid;       // real grid Kz*Ky*Kx (charges, then potential)
+  float2* cgrid;     // complex half grid Kz*Ky*(Kx/2+1)
+  const float2* tw[3];     // twiddles per dimension (forward, e^{-2 pi i m/K})
+  const float* gfac[3];    // per-dim b^2 exp(-pi^2 f^2/beta^2)
+  const float* f2[3];      // per-dim f^2 = (m'/L)^2
+  float gscale;            // CC / (pi V)
+  long long* facc;
+  long long* energy;
+  int* status;
+};
+void launch_pme(const PmeArgs& a, bool energy, cudaStream_t st);
+
+struct BondedArgs {
+  SysParams p;
+  const float4* pos4;
+  int nbond, nangle, nub, ndihe, nimpr, nexcl, n14;
+  const int2* bond;   const float2* bond_prm;   // k, r0
+  const int4* angle;  const float2* angle_prm;  // k, t0
+  const int2* ub;     const float2* ub_prm;
+  const int4* dihe;   const float4* dihe_prm;   // k, n, cos d, sin d
+  const int4* impr;   const float2* impr_prm;   // k, psi0
+  const int2* excl;
+  const int2* p14;
+  const int* type;
+  const float2* lj14;  // (ntypes+1)^2
+  long long* facc;
+  long long* energy;
+};
+void launch_bonded(const BondedArgs& a, bool energy, cudaStream_t st);
+
+struct IntegrateArgs {
+  SysParams p;
+  int nunits;
+  const int4* unit_atoms;   // -1 padded
+  const int* unit_meta;     // na | nc<<4 | pairs<<8 (local a,b 2 bits each)
+  const float4* unit_d;     // constraint lengths
+  float4* pos4;
+  float4* vel4;             // xyz velocity, w = 1/m
+  long long* facc;
+  float4* xyzq_s;
+  const int* inv_perm;
+  const float4* pos_build;
+  int* flag;
+  int* status;
+  long long* energy;
+  double dtu;               // dt * TU
+  double shake_tol;
+  int shake_maxit;
+};
+// kick (F/2) + drift + SHAKE, zeroes the force accumulator, scatters sorted positions
+void launch_kick_drift(const IntegrateArgs& a, cudaStream_t st);
+// kick (F/2) + RATTLE (+ kinetic energy)
+void launch_kick_rattle(const IntegrateArgs& a, bool kinetic, bool kick, cudaStream_t st);
+void launch_kinetic(const IntegrateArgs& a, cudaStream_t st);
+// Maxwell-Boltzmann draw (counter-based), momentum removal, RATTLE projection
+void launch_reassign(const IntegrateArgs& a, double T, uint64_t seed, uint32_t counter, double inv_mtot,
+                     long long* psum, cudaStream_t st);
+
+}  // namespace fzk

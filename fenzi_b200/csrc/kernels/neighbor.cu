@@ -1,0 +1,368 @@
+// Device-side neighbour maintenance: replaces CellBuild/CellUpdate/CellClean and
+// nbbuild_exclbitvec/nbbuild_excllist (src/cell_based_kernels.cu:198-399, 1048-1493)
+// and the host-synchronised rebuild decision of SingleStep (src/dynamics.cu:695-737).
+//
+// Layout: atoms are binned into x-y columns of ~32/rho^(2/3) cross-section, each
+// column is sorted by (z, atom id) and padded to a multiple of 32 slots, so every
+// 32-slot "block" is a compact cell of ~32 atoms.  A tile is (i-block, 32 j-slots);
+// j-slots are individual atoms within the pair-list radius of the i-block's bounding
+// box, drawn from blocks J >= I (Newton's third law), each tagged with its periodic
+// image.  Every kernel first reads the device rebuild flag and returns when no
+// rebuild is due, so the sequence is launched unconditionally (graph friendly) and
+// no host synchronisation is needed.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace fzk {
+
+__global__ void k_rb_begin(const int* __restrict__ flag, int* col_count, int* col_cursor, int ncol, int* counters) {
+  if (!*flag) return;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncol; c += gridDim.x * blockDim.x) {
+    col_count[c] = 0;
+    col_cursor[c] = 0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    counters[CNT_TILES] = 0;
+    counters[CNT_MASKS] = 0;
+  }
+}
+
+// wrap positions into [-L/2, L/2), record build positions, bin into columns
+__global__ void k_rb_bin(SysParams p, const int* __restrict__ flag, float4* pos4, float4* pos_build, int* col_of,
+                         int* col_count, int* status) {
+  if (!*flag) return;
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= p.n) return;
+  float4 r = pos4[a];
+  if (!(fabsf(r.x) < 1e7f && fabsf(r.y) < 1e7f && fabsf(r.z) < 1e7f)) {
+    atomicOr(status, ST_BAD_COORD);
+    r.x = r.y = r.z = 0.f;
+  }
+  r.x -= p.box.x * floorf((r.x + 0.5f * p.box.x) * p.inv_box.x);
+  r.y -= p.box.y * floorf((r.y + 0.5f * p.box.y) * p.inv_box.y);
+  r.z -= p.box.z * floorf((r.z + 0.5f * p.box.z) * p.inv_box.z);
+  // guard the rounding edge x == L/2
+  if (r.x >= 0.5f * p.box.x) r.x -= p.box.x;
+  if (r.y >= 0.5f * p.box.y) r.y -= p.box.y;
+  if (r.z >= 0.5f * p.box.z) r.z -= p.box.z;
+  pos4[a] = r;
+  pos_build[a] = r;
+  int cx = (int)((r.x + 0.5f * p.box.x) * p.inv_box.x * p.ncol[0]);
+  int cy = (int)((r.y + 0.5f * p.box.y) * p.inv_box.y * p.ncol[1]);
+  cx = min(max(cx, 0), p.ncol[0] - 1);
+  cy = min(max(cy, 0), p.ncol[1] - 1);
+  const int c = cy * p.ncol[0] + cx;
+  col_of[a] = c;
+  atomicAdd(&col_count[c], 1);
+}
+
+// exclusive scan of the 32-padded column sizes (one block)
+__global__ void k_rb_scan(SysParams p, const int* __restrict__ flag, const int* __restrict__ col_count, int* col_start,
+                          int ncol, int* counters, int* status) {
+  if (!*flag) return;
+  __shared__ int part[1024];
+  const int t = threadIdx.x, nt = blockDim.x;
+  const int per = (ncol + nt - 1) / nt;
+  const int b = t * per, e = min(ncol, b + per);
+  int s = 0;
+  for (int c = b; c < e; ++c) s += (col_count[c] + 31) & ~31;
+  part[t] = s;
+  __syncthreads();
+  for (int o = 1; o < nt; o <<= 1) {
+    const int v = t >= o ? part[t - o] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int run = part[t] - s;
+  for (int c = b; c < e; ++c) {
+    col_start[c] = run;
+    run += (col_count[c] + 31) & ~31;
+  }
+  if (t == nt - 1) {
+    const int used = part[t];
+    // the last 32 slots are reserved for the permanent dummy block
+    if (used > p.nslots - 32) atomicOr(status, ST_SLOT_OVERFLOW);
+    counters[CNT_SLOTS] = min(used, p.nslots - 32);
+    col_start[ncol] = min(used, p.nslots - 32);
+  }
+}
+
+__global__ void k_rb_scatter(SysParams p, const int* __restrict__ flag, const int* __restrict__ col_of,
+                             const int* __restrict__ col_start, int* col_cursor, int* col_tmp) {
+  if (!*flag) return;
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= p.n) return;
+  const int c = col_of[a];
+  const int k = atomicAdd(&col_cursor[c], 1);
+  const int s = col_start[c] + k;
+  if (s < p.nslots - 32) col_tmp[s] = a;
+}
+
+__device__ __forceinline__ uint32_t float_key(float f) {
+  const uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+// one block per column: bitonic sort by (z, atom id), then fill the sorted arrays
+__global__ void __launch_bounds__(256) k_rb_colsort(SysParams p, const int* __restrict__ flag,
+                                                    const int* __restrict__ col_count,
+                                                    const int* __restrict__ col_start, const int* __restrict__ col_tmp,
+                                                    const float4* __restrict__ pos4, const int* __restrict__ type,
+                                                    int* perm, int* inv_perm, float4* xyzq_s, int* typ_s, int* status) {
+  if (!*flag) return;
+  extern __shared__ unsigned long long keys[];
+  const int c = blockIdx.x;
+  const int n = col_count[c];
+  const int start = col_start[c];
+  const int padded = (n + 31) & ~31;
+  if (start + padded > p.nslots - 32) return;  // slot overflow already flagged
+  if (n > kColCap) {
+    if (threadIdx.x == 0) atomicOr(status, ST_COLUMN_OVERFLOW);
+    return;
+  }
+  int m = 1;
+  while (m < n) m <<= 1;
+  for (int k = threadIdx.x; k < m; k += blockDim.x) {
+    if (k < n) {
+      const int a = col_tmp[start + k];
+      keys[k] = ((unsigned long long)float_key(pos4[a].z) << 32) | (unsigned)a;
+    } else {
+      keys[k] = ~0ull;
+    }
+  }
+  __syncthreads();
+  for (int size = 2; size <= m; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int k = threadIdx.x; k < m; k += blockDim.x) {
+        const int o = k ^ stride;
+        if (o > k) {
+          const bool up = (k & size) == 0;
+          const unsigned long long x = keys[k], y = keys[o];
+          if ((x > y) == up) {
+            keys[k] = y;
+            keys[o] = x;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (int k = threadIdx.x; k < padded; k += blockDim.x) {
+    const int s = start + k;
+    if (k < n) {
+      const int a = (int)(keys[k] & 0xffffffffu);
+      perm[s] = a;
+      inv_perm[a] = s;
+      xyzq_s[s] = pos4[a];
+      typ_s[s] = type[a];
+    } else {
+      perm[s] = -1;
+      // distinct far-away point, q = 0, padding LJ type: never within any cutoff
+      xyzq_s[s] = make_float4(1.0e6f + (float)s, 1.0e6f, 1.0e6f, 0.f);
+      typ_s[s] = p.ntypes;
+    }
+  }
+}
+
+// per-block bounding boxes (warp per block)
+__global__ void k_rb_bbox(SysParams p, const int* __restrict__ flag, const int* __restrict__ counters,
+                          const int* __restrict__ perm, const float4* __restrict__ xyzq_s, float4* bb_lo,
+                          float4* bb_hi) {
+  if (!*flag) return;
+  const int nblk = counters[CNT_SLOTS] >> 5;
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= nblk) return;
+  const int s = w * 32 + lane;
+  const bool ok = perm[s] >= 0;
+  const float4 r = xyzq_s[s];
+  float lx = ok ? r.x : 3e38f, ly = ok ? r.y : 3e38f, lz = ok ? r.z : 3e38f;
+  float hx = ok ? r.x : -3e38f, hy = ok ? r.y : -3e38f, hz = ok ? r.z : -3e38f;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lx = fminf(lx, __shfl_xor_sync(0xffffffffu, lx, o));
+    ly = fminf(ly, __shfl_xor_sync(0xffffffffu, ly, o));
+    lz = fminf(lz, __shfl_xor_sync(0xffffffffu, lz, o));
+    hx = fmaxf(hx, __shfl_xor_sync(0xffffffffu, hx, o));
+    hy = fmaxf(hy, __shfl_xor_sync(0xffffffffu, hy, o));
+    hz = fmaxf(hz, __shfl_xor_sync(0xffffffffu, hz, o));
+  }
+  if (lane == 0) {
+    bb_lo[w] = make_float4(lx, ly, lz, 0.f);
+    bb_hi[w] = make_float4(hx, hy, hz, 0.f);
+  }
+}
+
+// squared distance between two boxes given center offset d and half extents
+__device__ __forceinline__ float box_gap2(float3 d, float3 h) {
+  const float gx = fmaxf(0.f, fabsf(d.x) - h.x);
+  const float gy = fmaxf(0.f, fabsf(d.y) - h.y);
+  const float gz = fmaxf(0.f, fabsf(d.z) - h.z);
+  return gx * gx + gy * gy + gz * gz;
+}
+
+// warp per i-block: find j-blocks J >= I within rlist, compact their j atoms into
+// 32-entry tiles, build exclusion masks.  all_images: test all 27 images (small boxes)
+__global__ void __launch_bounds__(256) k_rb_tiles(SysParams p, const int* __restrict__ flag, int* counters,
+                                                  const int* __restrict__ perm, const int* __restrict__ inv_perm,
+                                                  const float4* __restrict__ xyzq_s, const float4* __restrict__ bb_lo,
+                                                  const float4* __restrict__ bb_hi, const int* __restrict__ excl_off,
+                                                  const int* __restrict__ excl_idx, int* tile_i, uint32_t* tile_j,
+                                                  int* tile_m, uint32_t* masks, int tile_cap, int mask_cap,
+                                                  int all_images, int* status) {
+  if (!*flag) return;
+  __shared__ uint32_t jbuf_all[8][64];
+  const int nblk = counters[CNT_SLOTS] >> 5;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int I = blockIdx.x * 8 + warp;
+  if (I >= nblk) return;
+  uint32_t* jbuf = jbuf_all[warp];
+  const float4 li = bb_lo[I], hi4 = bb_hi[I];
+  const float3 ci = make_float3(0.5f * (li.x + hi4.x), 0.5f * (li.y + hi4.y), 0.5f * (li.z + hi4.z));
+  const float3 hi = make_float3(0.5f * (hi4.x - li.x), 0.5f * (hi4.y - li.y), 0.5f * (hi4.z - li.z));
+  const float rl2 = p.rlist * p.rlist;
+  const uint32_t dummy = (uint32_t)(p.nslots - 1) | ((uint32_t)kNoShift << kSlotBits);
+  int count = 0;
+  // i-lane data for exclusion masks
+  const int ia = perm[I * 32 + lane];
+
+  auto emit = [&](bool diag) {
+    __syncwarp();
+    int t = 0;
+    if (lane == 0) t = atomicAdd(&counters[CNT_TILES], 1);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= tile_cap) {
+      if (lane == 0) atomicOr(status, ST_TILE_OVERFLOW);
+      return;
+    }
+    const uint32_t je = jbuf[lane];
+    tile_j[(size_t)t * 32 + lane] = je;
+    // exclusion bits: bit k set when j entry k is an excluded partner of this lane's atom
+    uint32_t mask = 0;
+    if (ia >= 0) {
+      const int e0 = excl_off[ia], e1 = excl_off[ia + 1];
+      for (int e = e0; e < e1; ++e) {
+        const uint32_t se = (uint32_t)inv_perm[excl_idx[e]];
+        for (int k = 0; k < 32; ++k)
+          if ((jbuf[k] & kSlotMask) == se) mask |= 1u << k;
+      }
+    }
+    const unsigned any = __ballot_sync(0xffffffffu, mask != 0);
+    int m = -1;
+    if (any) {
+      if (lane == 0) m = atomicAdd(&counters[CNT_MASKS], 1);
+      m = __shfl_sync(0xffffffffu, m, 0);
+      if (m >= mask_cap) {
+        if (lane == 0) atomicOr(status, ST_MASK_OVERFLOW);
+        m = -1;
+      } else {
+        masks[(size_t)m * 32 + lane] = mask;
+      }
+    }
+    if (lane == 0) {
+      tile_i[t] = I | (diag ? (int)0x80000000 : 0);
+      tile_m[t] = m;
+    }
+    __syncwarp();
+  };
+
+  const int ncodes = all_images ? 27 : 1;
+  for (int J0 = I; J0 < nblk; J0 += 32) {
+    const int J = J0 + lane;
+    float3 cj = make_float3(0.f, 0.f, 0.f), hj = cj;
+    if (J < nblk) {
+      const float4 lj = bb_lo[J], hj4 = bb_hi[J];
+      cj = make_float3(0.5f * (lj.x + hj4.x), 0.5f * (lj.y + hj4.y), 0.5f * (lj.z + hj4.z));
+      hj = make_float3(0.5f * (hj4.x - lj.x), 0.5f * (hj4.y - lj.y), 0.5f * (hj4.z - lj.z));
+    }
+    for (int ic = 0; ic < ncodes; ++ic) {
+      bool pass = false;
+      int code = kNoShift;
+      if (J < nblk) {
+        float3 d = make_float3(cj.x - ci.x, cj.y - ci.y, cj.z - ci.z);
+        if (all_images) {
+          code = ic;
+          const float3 s = shift_of(code, p);
+          d.x += s.x;
+          d.y += s.y;
+          d.z += s.z;
+        } else {
+          const float sx = -rintf(d.x * p.inv_box.x), sy = -rintf(d.y * p.inv_box.y), sz = -rintf(d.z * p.inv_box.z);
+          d.x += sx * p.box.x;
+          d.y += sy * p.box.y;
+          d.z += sz * p.box.z;
+          code = ((int)sx + 1) + 3 * ((int)sy + 1) + 9 * ((int)sz + 1);
+        }
+        pass = box_gap2(d, make_float3(hi.x + hj.x, hi.y + hj.y, hi.z + hj.z)) < rl2;
+        if (J == I && code > kNoShift) pass = false;  // each +-image pair of the self block once
+      }
+      unsigned bal = __ballot_sync(0xffffffffu, pass);
+      while (bal) {
+        const int src = __ffs(bal) - 1;
+        bal &= bal - 1;
+        const int Jc = J0 + src;
+        const int cc = __shfl_sync(0xffffffffu, code, src);
+        if (Jc == I && cc == kNoShift) {
+          // diagonal tile: the whole block on its own (upper triangle in the pair
+          // kernel); pending compacted entries (count < 32) are kept aside
+          const uint32_t save = jbuf[lane];
+          __syncwarp();
+          jbuf[lane] = (uint32_t)(I * 32 + lane) | ((uint32_t)kNoShift << kSlotBits);
+          emit(true);
+          jbuf[lane] = save;
+          __syncwarp();
+          continue;
+        }
+        const int s = Jc * 32 + lane;
+        const float3 sh = shift_of(cc, p);
+        const float4 r = xyzq_s[s];
+        const float3 d = make_float3(r.x + sh.x - ci.x, r.y + sh.y - ci.y, r.z + sh.z - ci.z);
+        const bool ok = perm[s] >= 0 && box_gap2(d, hi) < rl2;
+        const unsigned b2 = __ballot_sync(0xffffffffu, ok);
+        const int pos = __popc(b2 & ((1u << lane) - 1u));
+        if (ok) jbuf[count + pos] = (uint32_t)s | ((uint32_t)cc << kSlotBits);
+        __syncwarp();
+        count += __popc(b2);
+        if (count >= 32) {
+          emit(false);
+          const uint32_t rest = jbuf[32 + lane];
+          __syncwarp();
+          jbuf[lane] = rest;
+          __syncwarp();
+          count -= 32;
+        }
+      }
+    }
+  }
+  if (count > 0) {
+    if (lane >= count) jbuf[lane] = dummy;
+    __syncwarp();
+    emit(false);
+  }
+}
+
+__global__ void k_rb_end(int* flag, int* counters) {
+  if (!*flag) return;
+  counters[CNT_REBUILDS] += 1;
+  *flag = 0;
+}
+
+// ------------------------------------------------------------------ launchers
+void launch_rebuild(const RebuildArgs& a, cudaStream_t st) {
+  const SysParams& p = a.p;
+  const int ncol = p.ncol[0] * p.ncol[1];
+  k_rb_begin<<<(ncol + 255) / 256, 256, 0, st>>>(a.flag, a.col_count, a.col_cursor, ncol, a.counters);
+  k_rb_bin<<<(p.n + 255) / 256, 256, 0, st>>>(p, a.flag, a.pos4, a.pos_build, a.col_of, a.col_count, a.status);
+  k_rb_scan<<<1, 1024, 0, st>>>(p, a.flag, a.col_count, a.col_start, ncol, a.counters, a.status);
+  k_rb_scatter<<<(p.n + 255) / 256, 256, 0, st>>>(p, a.flag, a.col_of, a.col_start, a.col_cursor, a.col_tmp);
+  k_rb_colsort<<<ncol, 256, kColCap * sizeof(unsigned long long), st>>>(
+      p, a.flag, a.col_count, a.col_start, a.col_tmp, a.pos4, a.type, a.perm, a.inv_perm, a.xyzq_s, a.typ_s, a.status);
+  const int maxblk = (p.nslots) / 32;
+  k_rb_bbox<<<(maxblk * 32 + 255) / 256, 256, 0, st>>>(p, a.flag, a.counters, a.perm, a.xyzq_s, a.bb_lo, a.bb_hi);
+  k_rb_tiles<<<(maxblk + 7) / 8, 256, 0, st>>>(p, a.flag, a.counters, a.perm, a.inv_perm, a.xyzq_s, a.bb_lo, a.bb_hi,
+                                               a.excl_off, a.excl_idx, a.tile_i, a.tile_j, a.tile_m, a.masks,
+                                               a.tile_cap, a.mask_cap, a.all_images, a.status);
+  k_rb_end<<<1, 1, 0, st>>>(a.flag, a.counters);
+}
+
+}  // namespace fzk

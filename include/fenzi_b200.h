@@ -1,0 +1,170 @@
+/*
+ * fenzi_b200 — C ABI of the B200-native FEN ZI molecular-dynamics step.
+ *
+ * The reference (TauferLab/fen-zi) has no plugin API: its boundary is a set of
+ * `void f(void)` host functions on file-scope globals, called from main() in
+ * src/fenzi.cu:141-268,442-547.  Each entry point below names the reference
+ * function it replaces.  Differences in convention:
+ *   - state lives behind an opaque fz_system* handle instead of globals;
+ *   - every call returns an fz_status (the reference calls exit()); the detail
+ *     of the last error on the calling thread is available from fz_last_error();
+ *   - arrays are plain host pointers with explicit sizes; units are the
+ *     reference's AKMA units (Angstrom, kcal/mol, amu, e, AKMA time for
+ *     velocities: Angstrom per 1/20.4548 ps).
+ * One handle must be used from one host thread at a time.
+ */
+#ifndef FENZI_B200_H
+#define FENZI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int fz_status;
+#define FZ_OK 0
+#define FZ_ERR_IO 1        /* file missing / unreadable                     */
+#define FZ_ERR_PARSE 2     /* malformed input, missing parameter            */
+#define FZ_ERR_CUDA 3      /* CUDA runtime error                            */
+#define FZ_ERR_CAPACITY 4  /* a device capacity was exceeded (list, cell)   */
+#define FZ_ERR_SHAKE 5     /* SHAKE/RATTLE did not converge in its cap      */
+#define FZ_ERR_ARG 6       /* bad argument                                  */
+#define FZ_ERR_STATE 7     /* call out of order (e.g. step before upload)   */
+#define FZ_ERR_NOMEM 8     /* device memory budget refused                  */
+#define FZ_ERR_TIMEOUT 9   /* a bounded device wait ran out                 */
+
+typedef struct fz_system fz_system;
+
+/* Run-file settings, the keywords of ReadInput (src/prmread.cu:491-913). */
+typedef struct fz_config {
+  char coordinates[512];
+  char structure[512];
+  char parameters[512];
+  char topology[512];
+  char outputname[512];
+  char outputtrajectory[512];
+  char restartfilename[512];
+  double temperature;        /* K */
+  double thermostat;         /* "thermostat" (tau), stored, unused by NVE/reassignment */
+  int temp_reset_every;      /* tempresetTiming: velocity reassignment period (0 = never) */
+  int minimize_steps;
+  double conjgradfac, steepdesfac, conjgradrate, steepdesrate;
+  int start_step;
+  double timestep_ps;        /* timestep (ps) */
+  int dyna_steps;            /* dynasteps */
+  double kappa;              /* KAPPa = Ewald beta (1/A) */
+  int inbfrq;                /* INBFRQ: forced list rebuild period (0 = displacement-triggered) */
+  int output_every;          /* outputTiming */
+  int checkpoint_every;      /* checkpointTiming */
+  int traj_every;            /* trajfrequencyTiming */
+  double cuton, cutoff, pairlistdist;
+  int gpublocksize;
+  double box[3];             /* cellBasisVector1..3 diagonal */
+  int pme_grid[3];           /* PMEGridSizeX/Y/Z */
+  double pmass, pref;        /* Andersen piston mass, reference pressure (atm) */
+  int shake;                 /* shake on|off */
+  double shake_tol;
+  double hfac;               /* hydrogen mass factor when shake is off */
+  int printlevel, printtostdout, keepcheckpoints;
+  char checkpointformat;     /* 'a' ascii, 'b' binary, 0 unset */
+  long long seed;
+  int unknown_keywords;      /* count of unrecognised lines (the reference warns) */
+} fz_config;
+
+/* Energies, the EvalProps table (src/evalprops.cu:248-308), kcal/mol, FP64. */
+typedef struct fz_energies {
+  double bond, angle, ureyb, dihed, impr, vdw, elec, pme, ewexcl, ewself;
+  double potential;          /* sum of the above */
+  double kinetic;            /* 1/2 sum m v^2 */
+  double temperature;        /* 2 KE / (k_B (3N - 6 - Ncons)) */
+  double virial[3];          /* diagonal of the virial (kcal/mol) */
+  double pressure_atm;
+  long long step;
+} fz_energies;
+
+/* Sizes of a loaded system. */
+typedef struct fz_info {
+  int natom, ntypes, nbond, nangle, nureyb, ndihedral, nimproper;
+  int nconstraint, ncluster, nexcl_pairs, n14_pairs;
+  int ndihedral_terms;       /* dihedral rows after expanding multi-fold parameters */
+  int pme_grid[3];
+  double box[3];
+} fz_info;
+
+/* ---- errors ---------------------------------------------------------- */
+/* Copies the last error message of this thread into buf (always NUL-terminated). */
+fz_status fz_last_error(char* buf, size_t len);
+const char* fz_version(void);
+
+/* ---- input (host only, no GPU needed) ---------------------------------- */
+/* ReadInput, src/prmread.cu:491-913.  Relative paths in the file stay relative
+ * to the directory of in_path. */
+fz_status fz_read_input(const char* in_path, fz_config* out);
+/* LoadCoord (ReadCrd/ReadPdb/ReadXYZ, src/prmread.cu:285-488, picked by extension
+ * as at src/prmread.cu:762-779), ReadPsf_CHARMM (:1442), ReadPrm_CHARMM (:2181),
+ * build_constraints (:1303) and GenExcl_minimal_new (:2928), in that order. */
+fz_status fz_load_system(const fz_config* cfg, fz_system** out);
+fz_status fz_get_info(const fz_system* sys, fz_info* out);
+/* Copies a named topology array (for inspection/tests): "pos" (double 3n), "q", "mass"
+ * (double n), "type" (int n), "eps4","sig2","eps4_14","sig2_14" (double nt*nt),
+ * "bond" (int 2nb), "bond_k","bond_r0", "angle" (int 3na), "angle_k","angle_t0",
+ * "ureyb" (int 2), "ureyb_k","ureyb_r0", "dihe" (int 4nd, one row per fold),
+ * "dihe_k","dihe_d" (double), "dihe_n" (int), "impr" (int 4ni), "impr_k","impr_p0",
+ * "cons" (int 2nc), "cons_d", "excl" (int 2 x nexcl, 1-2/1-3 pairs), "p14" (int 2 x n14).
+ * bytes must equal the array size. */
+fz_status fz_get_array(const fz_system* sys, const char* name, void* out, size_t bytes);
+fz_status fz_free(fz_system* sys);
+
+/* ---- device ------------------------------------------------------------ */
+/* InitMem (src/mem.cu:49) + InitDeviceConstants (src/cell_based_kernels.cu:1831):
+ * allocates and fills device state on `device`; work is queued on `stream`
+ * (a cudaStream_t, NULL = a stream owned by the system). */
+fz_status fz_upload(fz_system* sys, int device, void* stream);
+/* InitVelocity (src/init.cu:19-211): Maxwell-Boltzmann velocities at T (K) from a
+ * counter-based generator keyed on (seed, counter), COM momentum removed, constraint
+ * components removed (RATTLE). */
+fz_status fz_reassign_velocities(fz_system* sys, double T, uint64_t seed, uint32_t counter);
+/* ComputeAccelGPU (src/mdcuda.cu:557-849): forces at the current positions.  With
+ * energies != 0 also evaluates the energy terms (read them with fz_eval_props). */
+fz_status fz_compute_forces(fz_system* sys, int energies);
+/* As fz_compute_forces, restricted to the selected terms (bitwise OR of FZ_TERM_*):
+ * the real-space pair kernel (nonbondforce), the bonded kernel (bondedforce: bonds,
+ * angles, Urey-Bradley, dihedrals, impropers, 1-4 pairs, Ewald exclusion correction)
+ * and the PME reciprocal sum (ChargeSpread + FFT + BCMultiply + PMEForce). */
+#define FZ_TERM_NONBONDED 1
+#define FZ_TERM_BONDED 2
+#define FZ_TERM_PME 4
+#define FZ_TERM_ALL 7
+fz_status fz_compute_forces_terms(fz_system* sys, int terms, int energies);
+/* SingleStep (src/dynamics.cu:623-820) x nsteps: velocity Verlet with SHAKE/RATTLE,
+ * device-side neighbour maintenance, velocity reassignment every temp_reset_every
+ * steps when set.  Returns after the work is queued and checked. */
+fz_status fz_step(fz_system* sys, int nsteps);
+/* EvalProps (src/evalprops.cu:17-308): energies of the current state. */
+fz_status fz_eval_props(fz_system* sys, fz_energies* out);
+/* Host <-> device state (original atom order). */
+fz_status fz_get_positions(fz_system* sys, double* out3n);
+fz_status fz_set_positions(fz_system* sys, const double* in3n);
+fz_status fz_get_velocities(fz_system* sys, double* out3n);
+fz_status fz_set_velocities(fz_system* sys, const double* in3n);
+/* Forces of the last evaluation (kcal/mol/A). */
+fz_status fz_get_forces(fz_system* sys, double* out3n);
+/* Bit-exact force accumulator (int64 fixed point, scale 2^32, x[n] y[n] z[n]). */
+fz_status fz_get_forces_fixed(fz_system* sys, long long* out3n);
+/* float32 state transfer through caller-pinned host buffers (x,y,z per atom). */
+fz_status fz_set_state_f32(fz_system* sys, const float* pos3n, const float* vel3n);
+fz_status fz_get_state_f32(fz_system* sys, float* pos3n, float* vel3n);
+/* Device-side work counters of the last fz_step: [0] kernel launches issued,
+ * [1] neighbour-list rebuilds, [2] tiles in the current list, [3] pair tiles capacity. */
+fz_status fz_get_counters(fz_system* sys, long long* out4);
+/* Synchronises the system's stream and reports any sticky device error status. */
+fz_status fz_sync(fz_system* sys);
+/* The system's CUDA stream (cudaStream_t), for callers that time or order work. */
+void* fz_stream(fz_system* sys);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

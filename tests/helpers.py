@@ -1,0 +1,42 @@
+"""Shared builders for the tests: seeded systems written through the drop-in file
+formats, loaded by the product readers, with the oracle built from the same topology."""
+import os
+import tempfile
+
+import numpy as np
+
+from fenzi_b200 import gen_system
+
+_CACHE = {}
+_TMP = tempfile.mkdtemp(prefix="fzb200_")
+
+ORACLE_BONDED = 16 | 32 | 64 | 128 | 256 | 2 | 4  # bonds angles ub dihe impr excl p14
+
+
+def system(key="small", **kw):
+    """(System, in_path): cached per key."""
+    if key in _CACHE:
+        return _CACHE[key]
+    presets = {
+        "small": dict(name="custom", nw=400, nchains=2, chain_len=10, rc=8.0, ron=6.5, seed=7),
+        "water3000": dict(name="water3000"),
+        "mid": dict(name="custom", nw=8760, nchains=6, chain_len=30, box=64.0, kgrid=64, rc=10.0, ron=8.0, seed=11),
+        "tiny": dict(name="custom", nw=60, nchains=1, chain_len=8, box=14.0, kgrid=16, rc=6.0, ron=5.0, seed=3),
+    }
+    args = dict(presets.get(key, {}))
+    args.update(kw)
+    s = gen_system.build(**args)
+    path = gen_system.write(s, os.path.join(_TMP, key))
+    _CACHE[key] = (s, path)
+    return s, path
+
+
+def rel_rms(a, b):
+    a = np.asarray(a, float)
+    b = np.asarray(b, float)
+    return float(np.sqrt(((a - b) ** 2).sum() / max((b ** 2).sum(), 1e-300)))
+
+
+def oracle_for(fz_sys, nthreads=0):
+    from oracle.oracle import Oracle
+    return Oracle(fz_sys.topology(), nthreads=nthreads)

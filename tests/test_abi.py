@@ -1,0 +1,42 @@
+"""The C-ABI library loads and exports every symbol include/fenzi_b200.h declares."""
+import ctypes
+import os
+import re
+
+import fenzi_b200 as fz
+
+HDR = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "fenzi_b200.h")
+
+
+def declared():
+    txt = open(HDR).read()
+    return sorted(set(re.findall(r"^\s*(?:fz_status|const char\*|void\*)\s+(fz_\w+)\s*\(", txt, re.M)))
+
+
+def test_header_symbols_exported():
+    names = declared()
+    assert len(names) >= 20
+    lib = ctypes.CDLL(fz.LIB_PATH)
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) <= set(fz.EXPORTS)
+
+
+def test_version_and_error_channel():
+    assert b"sm_100a" in fz.lib().fz_version()
+    import ctypes as C
+    cfg = fz.Config()
+    rc = fz.lib().fz_read_input(b"/nonexistent/x.in", C.byref(cfg))
+    assert rc == 1 and "not found" in fz.last_error()
+
+
+def test_device_calls_before_upload_fail_cleanly():
+    from tests.helpers import system
+    _, path = system("small")
+    s = fz.FenZi.ReadInput(path).LoadSystem()
+    try:
+        s.SingleStep(1)
+    except fz.FenZiError as e:
+        assert e.code == 7
+    else:
+        raise AssertionError("expected FZ_ERR_STATE")
