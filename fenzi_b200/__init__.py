@@ -77,7 +77,9 @@ EXPORTS = ["fz_last_error", "fz_version", "fz_read_input", "fz_load_system", "fz
            "fz_free", "fz_upload", "fz_reassign_velocities", "fz_compute_forces", "fz_compute_forces_terms", "fz_step", "fz_eval_props",
            "fz_get_positions", "fz_set_positions", "fz_get_velocities", "fz_set_velocities", "fz_get_forces",
            "fz_get_forces_fixed", "fz_set_state_f32", "fz_get_state_f32", "fz_get_counters", "fz_sync",
-           "fz_stream"]
+           "fz_stream", "fz_set_stage_timing", "fz_get_stage_times", "fz_measure_fp32_peak"]
+
+STAGES = ["neighbour", "nonbonded", "bonded", "pme", "integrate"]
 
 TERM_NONBONDED, TERM_BONDED, TERM_PME, TERM_ALL = 1, 2, 4, 7
 
@@ -116,6 +118,9 @@ def lib():
             "fz_get_state_f32": ([vp, vp, vp], C.c_int),
             "fz_get_counters": ([vp, C.POINTER(C.c_longlong)], C.c_int),
             "fz_sync": ([vp], C.c_int),
+            "fz_set_stage_timing": ([vp, C.c_int], C.c_int),
+            "fz_get_stage_times": ([vp, dp], C.c_int),
+            "fz_measure_fp32_peak": ([C.c_int, dp], C.c_int),
             "fz_stream": ([vp], vp),
         }
         for name, (args, res) in sig.items():
@@ -270,6 +275,16 @@ class FenZi:
         _check(lib().fz_get_counters(self.h, out))
         return dict(launches=out[0], rebuilds=out[1], tiles=out[2], tile_capacity=out[3])
 
+    def stage_timing(self, enable=True):
+        _check(lib().fz_set_stage_timing(self.h, 1 if enable else 0))
+
+    def stage_times(self):
+        """Mean milliseconds per step of each stage over the steps timed so far."""
+        out = np.zeros(6)
+        _check(lib().fz_get_stage_times(self.h, _dp(out)))
+        n = max(1.0, out[5])
+        return {k: out[i] / n for i, k in enumerate(STAGES)} | {"steps": int(out[5])}
+
     def sync(self):
         _check(lib().fz_sync(self.h))
 
@@ -286,6 +301,12 @@ class FenZi:
             self.close()
         except Exception:
             pass
+
+
+def fp32_peak_tflops(device: int = 0) -> float:
+    out = C.c_double()
+    _check(lib().fz_measure_fp32_peak(int(device), C.byref(out)))
+    return out.value
 
 
 def load(in_path: str, device: int | None = None) -> FenZi:

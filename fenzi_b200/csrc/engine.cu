@@ -78,6 +78,11 @@ struct Engine {
   double temperature = 300.0;
   unsigned long long seed = 0;
   long long launches = 0;
+  // per-stage timing
+  bool timing = false;
+  cudaEvent_t ev[12] = {};
+  double stage_ms[5] = {0, 0, 0, 0, 0};
+  long long timed_steps = 0;
   // pinned staging
   void* pinned = nullptr;
   size_t pinned_bytes = 0;
@@ -121,6 +126,8 @@ struct Engine {
   }
   ~Engine() {
     if (st) cudaStreamSynchronize(st);
+    for (auto& x : ev)
+      if (x) cudaEventDestroy(x);
     for (void* p : allocs) cudaFree(p);
     if (pinned) cudaFreeHost(pinned);
     if (own_stream && st) cudaStreamDestroy(st);
@@ -253,21 +260,44 @@ struct Engine {
   }
 
   // ---------------------------------------------------------------- step pieces
+  void mark(int k) {
+    if (timing) cudaEventRecord(ev[k], st);
+  }
   void forces(bool energies, int terms = FZ_TERM_ALL) {
+    mark(1);
     fzk::launch_rebuild(rebuild_args(), st);
     launches += 8;
+    mark(2);
     if (terms & FZ_TERM_NONBONDED) {
       fzk::launch_nonbonded(nb_args(), energies, st);
       launches += 1;
     }
+    mark(3);
     if (terms & FZ_TERM_BONDED) {
       fzk::launch_bonded(bonded_args(), energies, st);
       launches += (nbond + nangle + nub + ndihe + nimpr + nexcl + n14 > 0) ? 1 : 0;
     }
+    mark(4);
     if (terms & FZ_TERM_PME) {
       fzk::launch_pme(pme_args(), energies, st);
       launches += 11;
     }
+    mark(5);
+  }
+  // accumulates the events of one timed step: 0 start, 1..5 forces, 6 end
+  void collect_step() {
+    cudaEventSynchronize(ev[6]);
+    float ms = 0.f;
+    auto el = [&](int a, int b) {
+      cudaEventElapsedTime(&ms, ev[a], ev[b]);
+      return (double)ms;
+    };
+    stage_ms[0] += el(1, 2);
+    stage_ms[1] += el(2, 3);
+    stage_ms[2] += el(3, 4);
+    stage_ms[3] += el(4, 5);
+    stage_ms[4] += el(0, 1) + el(5, 6);
+    timed_steps++;
   }
   fz_status check() {
     int h = 0;
@@ -616,9 +646,12 @@ extern "C" fz_status fz_step(fz_system* s, int nsteps) {
   }
   const fzk::IntegrateArgs ia = e->int_args();
   for (int k = 0; k < nsteps; ++k) {
+    e->mark(0);
     fzk::launch_kick_drift(ia, e->st);
     e->forces(false);
     fzk::launch_kick_rattle(ia, false, true, e->st);
+    e->mark(6);
+    if (e->timing) e->collect_step();
     e->launches += 2;
     e->step++;
     if (e->temp_reset_every > 0 && e->step % e->temp_reset_every == 0) {
@@ -801,6 +834,34 @@ extern "C" fz_status fz_get_counters(fz_system* s, long long* out4) {
   out4[2] = cnt[fzk::CNT_TILES];
   out4[3] = e->tile_cap;
   return FZ_OK;
+}
+
+extern "C" fz_status fz_set_stage_timing(fz_system* s, int enable) {
+  fz_status r;
+  if ((r = need_engine(s))) return r;
+  Engine* e = s->eng;
+  if (enable && !e->ev[0])
+    for (auto& x : e->ev) FZ_CUDA(cudaEventCreate(&x));
+  e->timing = enable != 0;
+  for (double& x : e->stage_ms) x = 0;
+  e->timed_steps = 0;
+  return FZ_OK;
+}
+
+extern "C" fz_status fz_get_stage_times(fz_system* s, double* out6) {
+  fz_status r;
+  if ((r = need_engine(s))) return r;
+  if (!out6) return fail(FZ_ERR_ARG, "null output");
+  for (int k = 0; k < 5; ++k) out6[k] = s->eng->stage_ms[k];
+  out6[5] = (double)s->eng->timed_steps;
+  return FZ_OK;
+}
+
+extern "C" fz_status fz_measure_fp32_peak(int device, double* tflops) {
+  if (!tflops) return fail(FZ_ERR_ARG, "null output");
+  *tflops = fzk::measure_fp32_peak(device);
+  FZ_CUDA(cudaGetLastError());
+  return *tflops > 0 ? FZ_OK : fail(FZ_ERR_CUDA, "FMA benchmark failed");
 }
 
 extern "C" fz_status fz_sync(fz_system* s) {

@@ -117,4 +117,6 @@ void launch_kinetic(const IntegrateArgs& a, cudaStream_t st);
 void launch_reassign(const IntegrateArgs& a, double T, uint64_t seed, uint32_t counter, double inv_mtot,
                      long long* psum, cudaStream_t st);
 
+double measure_fp32_peak(int device);
+
 }  // namespace fzk

@@ -212,41 +212,32 @@ def _grow_chains(rng, box, nchains, nlen, clash=2.5):
 
 
 def _place_waters(rng, box, nw, chain_atoms, excl=2.5, jitter=0.2):
+    """TIP3P oxygens on a cubic lattice (finest lattice that still leaves nw free sites
+    after removing sites within `excl` of chain atoms), random subset, +-jitter."""
     L = float(box[0])
     n0 = max(1, int(math.ceil(nw ** (1.0 / 3.0))))
+    ca = np.asarray(chain_atoms, float).reshape(-1, 3)
     for n in range(n0, n0 + 40):
         s = L / n
+        keep = np.ones((n, n, n), bool)
+        if len(ca):
+            # lattice index of each chain atom, then test the +-r neighbourhood of sites
+            u = (ca + L / 2) / s - 0.5
+            base = np.floor(u).astype(int)
+            r = int(math.ceil(excl / s)) + 1
+            offs = np.arange(-r, r + 1)
+            ox, oy, oz = np.meshgrid(offs, offs, offs, indexing="ij")
+            off = np.stack([ox.ravel(), oy.ravel(), oz.ravel()], 1)
+            for o in off:
+                idx = base + o
+                site = (idx + 0.5) * s - L / 2
+                d = site - ca
+                d -= L * np.round(d / L)
+                hit = (d * d).sum(1) < excl * excl
+                ii = idx[hit] % n
+                keep[ii[:, 0], ii[:, 1], ii[:, 2]] = False
         g = (np.arange(n) + 0.5) * s - L / 2
-        sites = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
-        if len(chain_atoms):
-            keep = np.ones(len(sites), bool)
-            # bin chain atoms
-            nc = max(1, int(L // 3.0))
-            cs = L / nc
-            cells = {}
-            ca = chain_atoms - np.floor((chain_atoms + L / 2) / L) * L
-            for idx, p in enumerate(ca):
-                key = tuple((np.floor((p + L / 2) / cs).astype(int)) % nc)
-                cells.setdefault(key, []).append(idx)
-            sk = (np.floor((sites + L / 2) / cs).astype(int)) % nc
-            for si in range(len(sites)):
-                k = sk[si]
-                for dz in (-1, 0, 1):
-                    for dy in (-1, 0, 1):
-                        for dx in (-1, 0, 1):
-                            for idx in cells.get(((k[0] + dx) % nc, (k[1] + dy) % nc, (k[2] + dz) % nc), ()):
-                                d = sites[si] - ca[idx]
-                                d -= L * np.round(d / L)
-                                if d @ d < excl * excl:
-                                    keep[si] = False
-                                    break
-                            if not keep[si]:
-                                break
-                        if not keep[si]:
-                            break
-                    if not keep[si]:
-                        break
-            sites = sites[keep]
+        sites = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1)[keep]
         if len(sites) >= nw:
             sel = np.sort(rng.choice(len(sites), nw, replace=False))
             return sites[sel] + rng.uniform(-jitter, jitter, size=(nw, 3))

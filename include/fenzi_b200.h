@@ -159,6 +159,15 @@ fz_status fz_get_state_f32(fz_system* sys, float* pos3n, float* vel3n);
 /* Device-side work counters of the last fz_step: [0] kernel launches issued,
  * [1] neighbour-list rebuilds, [2] tiles in the current list, [3] pair tiles capacity. */
 fz_status fz_get_counters(fz_system* sys, long long* out4);
+/* Per-stage device timing (CUDA events on the system stream) for the steps run
+ * while enabled.  Stages: 0 neighbour maintenance, 1 real-space pairs, 2 bonded,
+ * 3 PME, 4 integrate (kick/drift/SHAKE + kick/RATTLE).  fz_get_stage_times returns
+ * accumulated milliseconds per stage and the number of steps timed in out[5]. */
+fz_status fz_set_stage_timing(fz_system* sys, int enable);
+fz_status fz_get_stage_times(fz_system* sys, double* out6);
+/* Measures this GPU's FP32 FMA throughput (TFLOP/s) with a register-resident FMA
+ * kernel; the roof of the pair kernel, which no table of peaks carries. */
+fz_status fz_measure_fp32_peak(int device, double* tflops);
 /* Synchronises the system's stream and reports any sticky device error status. */
 fz_status fz_sync(fz_system* sys);
 /* The system's CUDA stream (cudaStream_t), for callers that time or order work. */
