@@ -36,6 +36,8 @@ struct Engine {
   fzk::SysParams p{};
   int n = 0, nunits = 0, ncol = 0, nslots = 0, tile_cap = 0, mask_cap = 0, all_images = 0;
   int nb_grid = 0;
+  int dcx = 1, dcy = 1;
+  int* blk_col = nullptr;
   std::vector<void*> allocs;
   // atoms
   float4 *pos4 = nullptr, *vel4 = nullptr, *pos_build = nullptr;
@@ -73,6 +75,7 @@ struct Engine {
   bool forces_valid = false;
   long long step = 0;
   double self_energy = 0, inv_mtot = 0, dtu = 0, shake_tol = 1e-10;
+  double box_d[3] = {0, 0, 0};
   int ncons = 0;
   int temp_reset_every = 0;
   double temperature = 300.0;
@@ -83,6 +86,11 @@ struct Engine {
   cudaEvent_t ev[12] = {};
   double stage_ms[5] = {0, 0, 0, 0, 0};
   long long timed_steps = 0;
+  // CUDA graph of one MD step (kick/drift/SHAKE, neighbour maintenance, forces,
+  // kick/RATTLE); captured on first use, replayed with one launch per step
+  cudaGraph_t step_graph = nullptr;
+  cudaGraphExec_t step_exec = nullptr;
+  bool use_graph = true;
   // pinned staging
   void* pinned = nullptr;
   size_t pinned_bytes = 0;
@@ -126,6 +134,8 @@ struct Engine {
   }
   ~Engine() {
     if (st) cudaStreamSynchronize(st);
+    if (step_exec) cudaGraphExecDestroy(step_exec);
+    if (step_graph) cudaGraphDestroy(step_graph);
     for (auto& x : ev)
       if (x) cudaEventDestroy(x);
     for (void* p : allocs) cudaFree(p);
@@ -162,6 +172,9 @@ struct Engine {
     a.tile_cap = tile_cap;
     a.mask_cap = mask_cap;
     a.all_images = all_images;
+    a.blk_col = blk_col;
+    a.dcx = dcx;
+    a.dcy = dcy;
     return a;
   }
   fzk::NonbondedArgs nb_args() const {
@@ -254,6 +267,10 @@ struct Engine {
     a.status = status;
     a.energy = energy;
     a.dtu = dtu;
+    for (int d = 0; d < 3; ++d) {
+      a.box_d[d] = box_d[d];
+      a.inv_box_d[d] = 1.0 / box_d[d];
+    }
     a.shake_tol = shake_tol;
     a.shake_maxit = 500;
     return a;
@@ -298,6 +315,33 @@ struct Engine {
     stage_ms[3] += el(4, 5);
     stage_ms[4] += el(0, 1) + el(5, 6);
     timed_steps++;
+  }
+  void step_body() {
+    const fzk::IntegrateArgs ia = int_args();
+    fzk::launch_kick_drift(ia, st);
+    forces(false);
+    fzk::launch_kick_rattle(ia, false, true, st);
+  }
+  fz_status graph_step() {
+    if (!step_exec) {
+      FZ_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      const long long l0 = launches;
+      step_body();
+      launches = l0;
+      cudaGraph_t g = nullptr;
+      FZ_CUDA(cudaStreamEndCapture(st, &g));
+      step_graph = g;
+      FZ_CUDA(cudaGraphInstantiate(&step_exec, step_graph, 0));
+    }
+    FZ_CUDA(cudaGraphLaunch(step_exec, st));
+    launches += 2 + 8 + 1 + ((nbond + nangle + nub + ndihe + nimpr + nexcl + n14 > 0) ? 1 : 0) + 11;
+    return FZ_OK;
+  }
+  void drop_graph() {
+    if (step_exec) cudaGraphExecDestroy(step_exec);
+    if (step_graph) cudaGraphDestroy(step_graph);
+    step_exec = nullptr;
+    step_graph = nullptr;
   }
   fz_status check() {
     int h = 0;
@@ -368,6 +412,7 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
   // ---- parameters
   fzk::SysParams& p = e->p;
   p.box = make_float3((float)c.box[0], (float)c.box[1], (float)c.box[2]);
+  for (int d = 0; d < 3; ++d) e->box_d[d] = c.box[d];
   p.inv_box = make_float3((float)(1.0 / c.box[0]), (float)(1.0 / c.box[1]), (float)(1.0 / c.box[2]));
   const double rc = c.cutoff, ron = std::min(c.cuton, c.cutoff);
   p.rc2 = (float)(rc * rc);
@@ -395,6 +440,9 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
   e->ncol = ncx * ncy;
   const double colw = std::max(c.box[0] / ncx, c.box[1] / ncy);
   e->all_images = (0.5 * lmin < plist + 3.0 * std::max(colw, a)) ? 1 : 0;
+  // column offsets whose x-y rectangles can lie within the pair-list radius
+  e->dcx = std::min(ncx, (int)std::ceil(plist / (c.box[0] / ncx)));
+  e->dcy = std::min(ncy, (int)std::ceil(plist / (c.box[1] / ncy)));
   e->nslots = ((n + 32 * e->ncol + 64 + 31) / 32) * 32;
   p.nslots = e->nslots;
   for (int d = 0; d < 3; ++d) {
@@ -439,7 +487,7 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
   if ((r = e->alloc(&e->xyzq_s, nslots)) || (r = e->alloc(&e->typ_s, nslots)) || (r = e->alloc(&e->perm, nslots)) ||
       (r = e->alloc(&e->inv_perm, n)) || (r = e->alloc(&e->col_of, n)) || (r = e->alloc(&e->col_count, e->ncol)) ||
       (r = e->alloc(&e->col_cursor, e->ncol)) || (r = e->alloc(&e->col_start, e->ncol + 1)) ||
-      (r = e->alloc(&e->col_tmp, nslots)) || (r = e->alloc(&e->bb_lo, nblk)) || (r = e->alloc(&e->bb_hi, nblk)) ||
+      (r = e->alloc(&e->col_tmp, nslots)) || (r = e->alloc(&e->bb_lo, nblk)) || (r = e->alloc(&e->blk_col, nblk)) || (r = e->alloc(&e->bb_hi, nblk)) ||
       (r = e->alloc(&e->tile_i, e->tile_cap)) || (r = e->alloc(&e->tile_m, e->tile_cap)) ||
       (r = e->alloc(&e->tile_j, (size_t)e->tile_cap * 32)) || (r = e->alloc(&e->masks, (size_t)e->mask_cap * 32)) ||
       (r = e->alloc(&e->flag, 1)) || (r = e->alloc(&e->counters, fzk::CNT_COUNT)) || (r = e->alloc(&e->status, 1)))
@@ -646,13 +694,17 @@ extern "C" fz_status fz_step(fz_system* s, int nsteps) {
   }
   const fzk::IntegrateArgs ia = e->int_args();
   for (int k = 0; k < nsteps; ++k) {
-    e->mark(0);
-    fzk::launch_kick_drift(ia, e->st);
-    e->forces(false);
-    fzk::launch_kick_rattle(ia, false, true, e->st);
-    e->mark(6);
-    if (e->timing) e->collect_step();
-    e->launches += 2;
+    if (e->use_graph && !e->timing) {
+      if ((r = e->graph_step())) return r;
+    } else {
+      e->mark(0);
+      fzk::launch_kick_drift(ia, e->st);
+      e->forces(false);
+      fzk::launch_kick_rattle(ia, false, true, e->st);
+      e->mark(6);
+      if (e->timing) e->collect_step();
+      e->launches += 2;
+    }
     e->step++;
     if (e->temp_reset_every > 0 && e->step % e->temp_reset_every == 0) {
       fzk::launch_reassign(ia, e->temperature, e->seed, (uint32_t)(e->step / e->temp_reset_every), e->inv_mtot,

@@ -45,101 +45,155 @@ __device__ __forceinline__ double3 force_of(const long long* facc, int n, int i)
   return make_double3((double)facc[i] * s, (double)facc[n + i] * s, (double)facc[2 * n + i] * s);
 }
 
-__device__ bool gauss3(int n, double J[3][3], double* rhs, double* x) {
-  for (int k = 0; k < n; ++k) {
-    if (J[k][k] == 0.0) return false;
-    for (int r = k + 1; r < n; ++r) {
-      const double m = J[r][k] / J[k][k];
-      for (int c = k + 1; c < n; ++c) J[r][c] -= m * J[k][c];
-      rhs[r] -= m * rhs[k];
-    }
+// solves J x = r for n <= 3 (Cramer's rule); false if singular
+__device__ __forceinline__ bool solve3(int n, const double J[3][3], const double* r, double* x) {
+  if (n == 1) {
+    if (J[0][0] == 0.0) return false;
+    x[0] = r[0] / J[0][0];
+    return true;
   }
-  for (int k = n - 1; k >= 0; --k) {
-    double t = rhs[k];
-    for (int c = k + 1; c < n; ++c) t -= J[k][c] * x[c];
-    x[k] = t / J[k][k];
+  if (n == 2) {
+    const double det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+    if (det == 0.0) return false;
+    const double id = 1.0 / det;
+    x[0] = (r[0] * J[1][1] - J[0][1] * r[1]) * id;
+    x[1] = (J[0][0] * r[1] - r[0] * J[1][0]) * id;
+    return true;
   }
+  const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+  const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+  const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+  const double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+  if (det == 0.0) return false;
+  const double id = 1.0 / det;
+  x[0] = (r[0] * c00 + J[0][1] * (r[2] * J[1][2] - r[1] * J[2][2]) + J[0][2] * (r[1] * J[2][1] - r[2] * J[1][1])) * id;
+  x[1] = (J[0][0] * (r[1] * J[2][2] - r[2] * J[1][2]) + r[0] * c01 + J[0][2] * (r[2] * J[1][0] - r[1] * J[2][0])) * id;
+  x[2] = (J[0][0] * (r[2] * J[1][1] - r[1] * J[2][1]) + J[0][1] * (r[1] * J[2][0] - r[2] * J[1][0]) + r[0] * c02) * id;
   return true;
 }
 
-__device__ __forceinline__ double coef_of(const Unit& U, int k, int l, const double* im) {
-  const int a = U.ca[k], b = U.cb[k];
-  double c = 0;
-  if (U.ca[l] == a) c += im[a];
-  if (U.cb[l] == a) c -= im[a];
-  if (U.ca[l] == b) c -= im[b];
-  if (U.cb[l] == b) c += im[b];
-  return c;
+__device__ __forceinline__ void minimg3(double* d, const IntegrateArgs& a) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) d[c] -= a.box_d[c] * rint(d[c] * a.inv_box_d[c]);
+}
+
+// Sign of atom `at` in constraint k: +1 first atom, -1 second, 0 absent.  All cluster
+// indexing below runs through compile-time-unrolled loops over (atom, constraint) with
+// these selects, so the per-cluster arrays stay in registers.
+__device__ __forceinline__ double sgn(const Unit& U, int k, int at) {
+  return (U.ca[k] == at ? 1.0 : 0.0) - (U.cb[k] == at ? 1.0 : 0.0);
+}
+
+// bond vector of constraint k from per-atom positions x (min-imaged)
+__device__ __forceinline__ void bond_vec(const Unit& U, int k, const double x[4][3], double* out,
+                                         const IntegrateArgs& a) {
+  out[0] = out[1] = out[2] = 0.0;
+#pragma unroll
+  for (int at = 0; at < 4; ++at) {
+    const double sg = sgn(U, k, at);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) out[c] += sg * x[at][c];
+  }
+  minimg3(out, a);
+}
+
+// c_kl = sum over atoms of sgn(k, at) sgn(l, at) / m_at
+__device__ __forceinline__ void coef_matrix(const Unit& U, const double* im, double cf[3][3]) {
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int l = 0; l < 3; ++l) {
+      double c = 0.0;
+#pragma unroll
+      for (int at = 0; at < 4; ++at) c += sgn(U, k, at) * sgn(U, l, at) * im[at];
+      cf[k][l] = c;
+    }
 }
 
 // SHAKE: Newton iteration on |r_a - r_b + dr_a - dr_b|^2 = d^2 with displacements along
-// the reference bond vectors (src/shake.cu:159-271).  rn: unconstrained positions (in/out)
+// the reference bond vectors (src/shake.cu:159-271).  With s_k the unconstrained bond
+// vector and c_kl the inverse-mass coupling of constraints k and l,
+// C_k = s_k + sum_l c_kl lambda_l rd_l.  rn: unconstrained positions (in/out).
 __device__ int shake_unit(const Unit& U, const double rref[4][3], double rn[4][3], const double* im,
-                          const SysParams& p, double tol, int maxit) {
-  double rd[3][3];
-  for (int k = 0; k < U.nc; ++k) {
-    for (int c = 0; c < 3; ++c) rd[k][c] = rref[U.ca[k]][c] - rref[U.cb[k]][c];
-    min_image_d(rd[k], p);
+                          const IntegrateArgs& a) {
+  double rd[3][3], s0[3][3], cf[3][3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    bond_vec(U, k, rref, rd[k], a);
+    bond_vec(U, k, rn, s0[k], a);
   }
+  coef_matrix(U, im, cf);
   double lam[3] = {0, 0, 0};
   int it = 0;
-  for (; it < maxit; ++it) {
-    double dr[4][3] = {};
-    for (int k = 0; k < U.nc; ++k)
-      for (int c = 0; c < 3; ++c) {
-        dr[U.ca[k]][c] += rd[k][c] * lam[k] * im[U.ca[k]];
-        dr[U.cb[k]][c] -= rd[k][c] * lam[k] * im[U.cb[k]];
-      }
+  const int nc = U.nc;
+  for (; it < a.shake_maxit; ++it) {
     double J[3][3], sig[3], dl[3];
-    for (int k = 0; k < U.nc; ++k) {
-      double C[3];
-      for (int c = 0; c < 3; ++c) C[c] = rn[U.ca[k]][c] - rn[U.cb[k]][c];
-      min_image_d(C, p);
-      for (int c = 0; c < 3; ++c) C[c] += dr[U.ca[k]][c] - dr[U.cb[k]][c];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      double C[3] = {s0[k][0], s0[k][1], s0[k][2]};
+#pragma unroll
+      for (int l = 0; l < 3; ++l) {
+        const double w = (l < nc) ? cf[k][l] * lam[l] : 0.0;
+        C[0] += w * rd[l][0];
+        C[1] += w * rd[l][1];
+        C[2] += w * rd[l][2];
+      }
       sig[k] = C[0] * C[0] + C[1] * C[1] + C[2] * C[2] - U.d[k] * U.d[k];
-      for (int l = 0; l < U.nc; ++l)
-        J[k][l] = 2.0 * coef_of(U, k, l, im) * (rd[l][0] * C[0] + rd[l][1] * C[1] + rd[l][2] * C[2]);
+#pragma unroll
+      for (int l = 0; l < 3; ++l) J[k][l] = 2.0 * cf[k][l] * (rd[l][0] * C[0] + rd[l][1] * C[1] + rd[l][2] * C[2]);
     }
-    if (!gauss3(U.nc, J, sig, dl)) return 2;
+    if (!solve3(nc, J, sig, dl)) return 2;
     double t = 0;
-    for (int k = 0; k < U.nc; ++k) {
-      lam[k] -= dl[k];
-      t += dl[k] * dl[k];
-    }
-    if (t < tol) break;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      if (k < nc) {
+        lam[k] -= dl[k];
+        t += dl[k] * dl[k];
+      }
+    if (t < a.shake_tol) break;
   }
-  double dr[4][3] = {};
-  for (int k = 0; k < U.nc; ++k)
-    for (int c = 0; c < 3; ++c) {
-      dr[U.ca[k]][c] += rd[k][c] * lam[k] * im[U.ca[k]];
-      dr[U.cb[k]][c] -= rd[k][c] * lam[k] * im[U.cb[k]];
+#pragma unroll
+  for (int at = 0; at < 4; ++at)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double w = (k < nc) ? sgn(U, k, at) * lam[k] * im[at] : 0.0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) rn[at][c] += w * rd[k][c];
     }
-  for (int a = 0; a < U.na; ++a)
-    for (int c = 0; c < 3; ++c) rn[a][c] += dr[a][c];
-  return it >= maxit ? 1 : 0;
+  return it >= a.shake_maxit ? 1 : 0;
 }
 
 // RATTLE velocity stage: (v_a - v_b) . r_ab = 0, linear, solved directly
 __device__ void rattle_unit(const Unit& U, const double r[4][3], double v[4][3], const double* im,
-                            const SysParams& p) {
-  double rd[3][3];
-  for (int k = 0; k < U.nc; ++k) {
-    for (int c = 0; c < 3; ++c) rd[k][c] = r[U.ca[k]][c] - r[U.cb[k]][c];
-    min_image_d(rd[k], p);
+                            const IntegrateArgs& a) {
+  double rd[3][3], vd[3][3], cf[3][3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    bond_vec(U, k, r, rd[k], a);
+    vd[k][0] = vd[k][1] = vd[k][2] = 0.0;
+#pragma unroll
+    for (int at = 0; at < 4; ++at) {
+      const double sg = sgn(U, k, at);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) vd[k][c] += sg * v[at][c];
+    }
   }
+  coef_matrix(U, im, cf);
   double J[3][3], rhs[3], mu[3];
-  for (int k = 0; k < U.nc; ++k) {
-    double vab[3];
-    for (int c = 0; c < 3; ++c) vab[c] = v[U.ca[k]][c] - v[U.cb[k]][c];
-    rhs[k] = vab[0] * rd[k][0] + vab[1] * rd[k][1] + vab[2] * rd[k][2];
-    for (int l = 0; l < U.nc; ++l)
-      J[k][l] = coef_of(U, k, l, im) * (rd[l][0] * rd[k][0] + rd[l][1] * rd[k][1] + rd[l][2] * rd[k][2]);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    rhs[k] = vd[k][0] * rd[k][0] + vd[k][1] * rd[k][1] + vd[k][2] * rd[k][2];
+#pragma unroll
+    for (int l = 0; l < 3; ++l) J[k][l] = cf[k][l] * (rd[l][0] * rd[k][0] + rd[l][1] * rd[k][1] + rd[l][2] * rd[k][2]);
   }
-  if (!gauss3(U.nc, J, rhs, mu)) return;
-  for (int k = 0; k < U.nc; ++k)
-    for (int c = 0; c < 3; ++c) {
-      v[U.ca[k]][c] -= rd[k][c] * mu[k] * im[U.ca[k]];
-      v[U.cb[k]][c] += rd[k][c] * mu[k] * im[U.cb[k]];
+  if (!solve3(U.nc, J, rhs, mu)) return;
+#pragma unroll
+  for (int at = 0; at < 4; ++at)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double w = (k < U.nc) ? sgn(U, k, at) * mu[k] * im[at] : 0.0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) v[at][c] -= w * rd[k][c];
     }
 }
 
@@ -150,32 +204,44 @@ __global__ void __launch_bounds__(128) k_kick_drift(IntegrateArgs a) {
   const int n = a.p.n;
   double r0[4][3], rn[4][3], v[4][3], im[4];
   float q[4];
-  for (int k = 0; k < U.na; ++k) {
-    const int i = U.atom[k];
-    const float4 pr = a.pos4[i], vl = a.vel4[i];
-    const double3 F = force_of(a.facc, n, i);
-    a.facc[i] = 0;
-    a.facc[n + i] = 0;
-    a.facc[2 * n + i] = 0;
-    im[k] = vl.w;
-    q[k] = pr.w;
-    const double h = 0.5 * a.dtu * im[k];
-    v[k][0] = vl.x + h * F.x;
-    v[k][1] = vl.y + h * F.y;
-    v[k][2] = vl.z + h * F.z;
-    r0[k][0] = pr.x;
-    r0[k][1] = pr.y;
-    r0[k][2] = pr.z;
-    for (int c = 0; c < 3; ++c) rn[k][c] = r0[k][c] + a.dtu * v[k][c];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    im[k] = 0.0;
+    q[k] = 0.f;
+    for (int c = 0; c < 3; ++c) r0[k][c] = rn[k][c] = v[k][c] = 0.0;
+    if (k < U.na) {
+      const int i = U.atom[k];
+      const float4 pr = a.pos4[i], vl = a.vel4[i];
+      const double3 F = force_of(a.facc, n, i);
+      a.facc[i] = 0;
+      a.facc[n + i] = 0;
+      a.facc[2 * n + i] = 0;
+      im[k] = vl.w;
+      q[k] = pr.w;
+      const double h = 0.5 * a.dtu * im[k];
+      v[k][0] = vl.x + h * F.x;
+      v[k][1] = vl.y + h * F.y;
+      v[k][2] = vl.z + h * F.z;
+      r0[k][0] = pr.x;
+      r0[k][1] = pr.y;
+      r0[k][2] = pr.z;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) rn[k][c] = r0[k][c] + a.dtu * v[k][c];
+    }
   }
   if (U.nc > 0) {
-    const int st = shake_unit(U, r0, rn, im, a.p, a.shake_tol, a.shake_maxit);
+    const int st = shake_unit(U, r0, rn, im, a);
     if (st) atomicOr(a.status, ST_SHAKE_NOCONV);
-    for (int k = 0; k < U.na; ++k)
-      for (int c = 0; c < 3; ++c) v[k][c] = (rn[k][c] - r0[k][c]) / a.dtu;  // v += dr/(dt TU)
+    const double idt = 1.0 / a.dtu;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) v[k][c] = (rn[k][c] - r0[k][c]) * idt;  // v += dr/(dt TU)
   }
   bool far = false;
-  for (int k = 0; k < U.na; ++k) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (k >= U.na) continue;
     const int i = U.atom[k];
     const float4 np = make_float4((float)rn[k][0], (float)rn[k][1], (float)rn[k][2], q[k]);
     a.pos4[i] = np;
@@ -196,7 +262,11 @@ __global__ void __launch_bounds__(128) k_kick_rattle(IntegrateArgs a, int kick) 
     const Unit U = load_unit(a, u);
     const int n = a.p.n;
     double r[4][3], v[4][3], im[4];
-    for (int k = 0; k < U.na; ++k) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      im[k] = 0.0;
+      for (int c = 0; c < 3; ++c) r[k][c] = v[k][c] = 0.0;
+      if (k >= U.na) continue;
       const int i = U.atom[k];
       const float4 pr = a.pos4[i], vl = a.vel4[i];
       im[k] = vl.w;
@@ -214,8 +284,10 @@ __global__ void __launch_bounds__(128) k_kick_rattle(IntegrateArgs a, int kick) 
       r[k][1] = pr.y;
       r[k][2] = pr.z;
     }
-    if (U.nc > 0) rattle_unit(U, r, v, im, a.p);
-    for (int k = 0; k < U.na; ++k) {
+    if (U.nc > 0) rattle_unit(U, r, v, im, a);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (k >= U.na) continue;
       const int i = U.atom[k];
       a.vel4[i] = make_float4((float)v[k][0], (float)v[k][1], (float)v[k][2], (float)im[k]);
       if (KIN && im[k] > 0.0) {

@@ -26,6 +26,8 @@ struct RebuildArgs {
   int* tile_m;
   uint32_t* masks;
   int tile_cap, mask_cap, all_images;
+  int* blk_col;   // block -> column
+  int dcx, dcy;   // column offsets searched for neighbour blocks
 };
 void launch_rebuild(const RebuildArgs& a, cudaStream_t st);
 
@@ -105,6 +107,7 @@ struct IntegrateArgs {
   int* status;
   long long* energy;
   double dtu;               // dt * TU
+  double box_d[3], inv_box_d[3];
   double shake_tol;
   int shake_maxit;
 };

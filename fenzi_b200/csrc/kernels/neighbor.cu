@@ -53,7 +53,8 @@ __global__ void k_rb_bin(SysParams p, const int* __restrict__ flag, float4* pos4
   cy = min(max(cy, 0), p.ncol[1] - 1);
   const int c = cy * p.ncol[0] + cx;
   col_of[a] = c;
-  atomicAdd(&col_count[c], 1);
+  const unsigned peers = __match_any_sync(__activemask(), c);
+  if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&col_count[c], __popc(peers));
 }
 
 // exclusive scan of the 32-padded column sizes (one block)
@@ -94,7 +95,12 @@ __global__ void k_rb_scatter(SysParams p, const int* __restrict__ flag, const in
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= p.n) return;
   const int c = col_of[a];
-  const int k = atomicAdd(&col_cursor[c], 1);
+  const unsigned peers = __match_any_sync(__activemask(), c);
+  const int leader = __ffs(peers) - 1;
+  int base = 0;
+  if ((threadIdx.x & 31) == leader) base = atomicAdd(&col_cursor[c], __popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  const int k = base + __popc(peers & ((1u << (threadIdx.x & 31)) - 1u));
   const int s = col_start[c] + k;
   if (s < p.nslots - 32) col_tmp[s] = a;
 }
@@ -109,7 +115,8 @@ __global__ void __launch_bounds__(256) k_rb_colsort(SysParams p, const int* __re
                                                     const int* __restrict__ col_count,
                                                     const int* __restrict__ col_start, const int* __restrict__ col_tmp,
                                                     const float4* __restrict__ pos4, const int* __restrict__ type,
-                                                    int* perm, int* inv_perm, float4* xyzq_s, int* typ_s, int* status) {
+                                                    int* perm, int* inv_perm, float4* xyzq_s, int* typ_s, int* blk_col,
+                                                    int* status) {
   if (!*flag) return;
   extern __shared__ unsigned long long keys[];
   const int c = blockIdx.x;
@@ -148,6 +155,7 @@ __global__ void __launch_bounds__(256) k_rb_colsort(SysParams p, const int* __re
       __syncthreads();
     }
   }
+  for (int k = threadIdx.x * 32; k < padded; k += 32 * blockDim.x) blk_col[(start + k) >> 5] = c;
   for (int k = threadIdx.x; k < padded; k += blockDim.x) {
     const int s = start + k;
     if (k < n) {
@@ -209,7 +217,8 @@ __global__ void __launch_bounds__(256) k_rb_tiles(SysParams p, const int* __rest
                                                   const float4* __restrict__ bb_hi, const int* __restrict__ excl_off,
                                                   const int* __restrict__ excl_idx, int* tile_i, uint32_t* tile_j,
                                                   int* tile_m, uint32_t* masks, int tile_cap, int mask_cap,
-                                                  int all_images, int* status) {
+                                                  int all_images, const int* __restrict__ blk_col,
+                                                  const int* __restrict__ col_start, int dcx, int dcy, int* status) {
   if (!*flag) return;
   __shared__ uint32_t jbuf_all[8][64];
   const int nblk = counters[CNT_SLOTS] >> 5;
@@ -266,70 +275,78 @@ __global__ void __launch_bounds__(256) k_rb_tiles(SysParams p, const int* __rest
     __syncwarp();
   };
 
-  const int ncodes = all_images ? 27 : 1;
-  for (int J0 = I; J0 < nblk; J0 += 32) {
-    const int J = J0 + lane;
-    float3 cj = make_float3(0.f, 0.f, 0.f), hj = cj;
-    if (J < nblk) {
-      const float4 lj = bb_lo[J], hj4 = bb_hi[J];
-      cj = make_float3(0.5f * (lj.x + hj4.x), 0.5f * (lj.y + hj4.y), 0.5f * (lj.z + hj4.z));
-      hj = make_float3(0.5f * (hj4.x - lj.x), 0.5f * (hj4.y - lj.y), 0.5f * (hj4.z - lj.z));
-    }
-    for (int ic = 0; ic < ncodes; ++ic) {
-      bool pass = false;
-      int code = kNoShift;
-      if (J < nblk) {
-        float3 d = make_float3(cj.x - ci.x, cj.y - ci.y, cj.z - ci.z);
-        if (all_images) {
-          code = ic;
-          const float3 s = shift_of(code, p);
-          d.x += s.x;
-          d.y += s.y;
-          d.z += s.z;
-        } else {
-          const float sx = -rintf(d.x * p.inv_box.x), sy = -rintf(d.y * p.inv_box.y), sz = -rintf(d.z * p.inv_box.z);
-          d.x += sx * p.box.x;
-          d.y += sy * p.box.y;
-          d.z += sz * p.box.z;
-          code = ((int)sx + 1) + 3 * ((int)sy + 1) + 9 * ((int)sz + 1);
+  // candidate j blocks: the blocks of the columns within rlist in x-y (periodic column
+  // offsets carry the x/y image), each tested in z at its minimum image (or at all three
+  // z images for small boxes)
+  const int cI = blk_col[I];
+  const int cx = cI % p.ncol[0], cy = cI / p.ncol[0];
+  const int nz = all_images ? 3 : 1;
+  for (int oy = -dcy; oy <= dcy; ++oy) {
+    int yy = cy + oy;
+    const int sy = yy < 0 ? -1 : (yy >= p.ncol[1] ? 1 : 0);
+    yy -= sy * p.ncol[1];
+    for (int ox = -dcx; ox <= dcx; ++ox) {
+      int xx = cx + ox;
+      const int sx = xx < 0 ? -1 : (xx >= p.ncol[0] ? 1 : 0);
+      xx -= sx * p.ncol[0];
+      const int col = yy * p.ncol[0] + xx;
+      const int b0 = col_start[col] >> 5, b1 = col_start[col + 1] >> 5;
+      for (int J0 = b0; J0 < b1; J0 += 32) {
+        const int J = J0 + lane;
+        const bool inr = J < b1 && J >= I;
+        float3 cj = make_float3(0.f, 0.f, 0.f), hj = cj;
+        if (inr) {
+          const float4 lj = bb_lo[J], hj4 = bb_hi[J];
+          cj = make_float3(0.5f * (lj.x + hj4.x), 0.5f * (lj.y + hj4.y), 0.5f * (lj.z + hj4.z));
+          hj = make_float3(0.5f * (hj4.x - lj.x), 0.5f * (hj4.y - lj.y), 0.5f * (hj4.z - lj.z));
         }
-        pass = box_gap2(d, make_float3(hi.x + hj.x, hi.y + hj.y, hi.z + hj.z)) < rl2;
-        if (J == I && code > kNoShift) pass = false;  // each +-image pair of the self block once
-      }
-      unsigned bal = __ballot_sync(0xffffffffu, pass);
-      while (bal) {
-        const int src = __ffs(bal) - 1;
-        bal &= bal - 1;
-        const int Jc = J0 + src;
-        const int cc = __shfl_sync(0xffffffffu, code, src);
-        if (Jc == I && cc == kNoShift) {
-          // diagonal tile: the whole block on its own (upper triangle in the pair
-          // kernel); pending compacted entries (count < 32) are kept aside
-          const uint32_t save = jbuf[lane];
-          __syncwarp();
-          jbuf[lane] = (uint32_t)(I * 32 + lane) | ((uint32_t)kNoShift << kSlotBits);
-          emit(true);
-          jbuf[lane] = save;
-          __syncwarp();
-          continue;
-        }
-        const int s = Jc * 32 + lane;
-        const float3 sh = shift_of(cc, p);
-        const float4 r = xyzq_s[s];
-        const float3 d = make_float3(r.x + sh.x - ci.x, r.y + sh.y - ci.y, r.z + sh.z - ci.z);
-        const bool ok = perm[s] >= 0 && box_gap2(d, hi) < rl2;
-        const unsigned b2 = __ballot_sync(0xffffffffu, ok);
-        const int pos = __popc(b2 & ((1u << lane) - 1u));
-        if (ok) jbuf[count + pos] = (uint32_t)s | ((uint32_t)cc << kSlotBits);
-        __syncwarp();
-        count += __popc(b2);
-        if (count >= 32) {
-          emit(false);
-          const uint32_t rest = jbuf[32 + lane];
-          __syncwarp();
-          jbuf[lane] = rest;
-          __syncwarp();
-          count -= 32;
+        for (int iz = 0; iz < nz; ++iz) {
+          bool pass = false;
+          int code = kNoShift;
+          if (inr) {
+            float3 d = make_float3(cj.x - ci.x + sx * p.box.x, cj.y - ci.y + sy * p.box.y, cj.z - ci.z);
+            const float sz = all_images ? (float)(iz - 1) : -rintf(d.z * p.inv_box.z);
+            d.z += sz * p.box.z;
+            code = (sx + 1) + 3 * (sy + 1) + 9 * ((int)sz + 1);
+            pass = box_gap2(d, make_float3(hi.x + hj.x, hi.y + hj.y, hi.z + hj.z)) < rl2;
+            if (J == I && code > kNoShift) pass = false;  // each +-image pair of the self block once
+          }
+          unsigned bal = __ballot_sync(0xffffffffu, pass);
+          while (bal) {
+            const int src = __ffs(bal) - 1;
+            bal &= bal - 1;
+            const int Jc = J0 + src;
+            const int cc = __shfl_sync(0xffffffffu, code, src);
+            if (Jc == I && cc == kNoShift) {
+              // diagonal tile: the whole block on its own (upper triangle in the pair
+              // kernel); pending compacted entries (count < 32) are kept aside
+              const uint32_t save = jbuf[lane];
+              __syncwarp();
+              jbuf[lane] = (uint32_t)(I * 32 + lane) | ((uint32_t)kNoShift << kSlotBits);
+              emit(true);
+              jbuf[lane] = save;
+              __syncwarp();
+              continue;
+            }
+            const int s = Jc * 32 + lane;
+            const float3 sh = shift_of(cc, p);
+            const float4 r = xyzq_s[s];
+            const float3 d = make_float3(r.x + sh.x - ci.x, r.y + sh.y - ci.y, r.z + sh.z - ci.z);
+            const bool ok = perm[s] >= 0 && box_gap2(d, hi) < rl2;
+            const unsigned b2 = __ballot_sync(0xffffffffu, ok);
+            const int pos = __popc(b2 & ((1u << lane) - 1u));
+            if (ok) jbuf[count + pos] = (uint32_t)s | ((uint32_t)cc << kSlotBits);
+            __syncwarp();
+            count += __popc(b2);
+            if (count >= 32) {
+              emit(false);
+              const uint32_t rest = jbuf[32 + lane];
+              __syncwarp();
+              jbuf[lane] = rest;
+              __syncwarp();
+              count -= 32;
+            }
+          }
         }
       }
     }
@@ -356,12 +373,14 @@ void launch_rebuild(const RebuildArgs& a, cudaStream_t st) {
   k_rb_scan<<<1, 1024, 0, st>>>(p, a.flag, a.col_count, a.col_start, ncol, a.counters, a.status);
   k_rb_scatter<<<(p.n + 255) / 256, 256, 0, st>>>(p, a.flag, a.col_of, a.col_start, a.col_cursor, a.col_tmp);
   k_rb_colsort<<<ncol, 256, kColCap * sizeof(unsigned long long), st>>>(
-      p, a.flag, a.col_count, a.col_start, a.col_tmp, a.pos4, a.type, a.perm, a.inv_perm, a.xyzq_s, a.typ_s, a.status);
+      p, a.flag, a.col_count, a.col_start, a.col_tmp, a.pos4, a.type, a.perm, a.inv_perm, a.xyzq_s, a.typ_s,
+      a.blk_col, a.status);
   const int maxblk = (p.nslots) / 32;
   k_rb_bbox<<<(maxblk * 32 + 255) / 256, 256, 0, st>>>(p, a.flag, a.counters, a.perm, a.xyzq_s, a.bb_lo, a.bb_hi);
   k_rb_tiles<<<(maxblk + 7) / 8, 256, 0, st>>>(p, a.flag, a.counters, a.perm, a.inv_perm, a.xyzq_s, a.bb_lo, a.bb_hi,
                                                a.excl_off, a.excl_idx, a.tile_i, a.tile_j, a.tile_m, a.masks,
-                                               a.tile_cap, a.mask_cap, a.all_images, a.status);
+                                               a.tile_cap, a.mask_cap, a.all_images, a.blk_col, a.col_start, a.dcx,
+                                               a.dcy, a.status);
   k_rb_end<<<1, 1, 0, st>>>(a.flag, a.counters);
 }
 

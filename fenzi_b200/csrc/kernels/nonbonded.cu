@@ -2,16 +2,22 @@
 // erfc real-space Ewald, the functional form of nonbondforce (src/nonbonded_forces.cu:114-245).
 //
 // B200 design: one warp per tile (32 i-atoms of a sorted block x 32 j-atoms of the
-// pair list).  i data stay in registers; j data (x, y, z, q, LJ type) and the j force
-// accumulator rotate through the warp with shuffles, so each pair is evaluated once
-// (Newton's third law) with no shared-memory traffic.  Forces are converted to int64
-// fixed point at the end of each tile and added with RED atomics: the result does not
-// depend on tile order, so forces are bit-reproducible run to run.
-//
-// erfc uses Abramowitz & Stegun, Handbook of Mathematical Functions (1964), eq. 7.1.26
-// (|error| <= 1.5e-7), which shares its exp(-x^2) with the force term.
-// The LJ switch derivative is the exact one; the reference's force expression
-// (src/nonbonded_forces.cu:210-214) carries an extra Swcoeff2*invDist term.
+// pair list), each pair evaluated once (Newton's third law).  i data live in
+// registers; the tile's j data (x, y, z, q, LJ type, periodic image applied) are
+// staged once into a doubled 64-entry shared-memory ring, so at step k lane l reads
+// j = l + k with a constant-offset load and no wrap arithmetic; only the j force
+// accumulator rotates through the warp (3 shuffles per pair step).  Tiles without
+// excluded pairs (the large majority) run a mask-free loop.  The kernel is FP32-issue
+// bound, so every pair-step instruction counts:
+//   erfc(x) = t P(t) exp(-x^2), t = 1/(1 + p x)  (Abramowitz & Stegun, Handbook of
+//     Mathematical Functions (1964) eq. 7.1.26, |error| <= 1.5e-7), with exp2 and the
+//     constants pre-scaled so exp(-x^2) is one multiply and one MUFU.EX2;
+//   the CHARMM switch (rc^2-r^2)^2 (rc^2+2r^2-3ron^2)/(rc^2-ron^2)^3 written as
+//     1 - t^2 (3 - 2t) with t = sat((r^2-ron^2)/(rc^2-ron^2)) (identical polynomial),
+//     its derivative exact (the reference's force at src/nonbonded_forces.cu:210-214
+//     carries an extra Swcoeff2*invDist term);
+// Forces go to int64 fixed point at the end of each tile (RED atomics, order
+// independent): bit-reproducible run to run.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -24,34 +30,93 @@ constexpr float kAS_a3 = 1.421413741f;
 constexpr float kAS_a4 = -1.453152027f;
 constexpr float kAS_a5 = 1.061405429f;
 constexpr float kTwoOverSqrtPi = 1.1283791670955126f;
+constexpr float kLog2e = 1.4426950408889634f;
+constexpr int kWarps = 8;
+
+// single-instruction MUFU approximations (PTX ISA: rsqrt/ex2/rcp .approx.ftz.f32)
+__device__ __forceinline__ float rsqrt_a(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float ex2_a(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rcp_a(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+struct PairConst {
+  float rc2, beta, eb2;   // eb2 = -beta^2 log2(e)
+  float p_b;              // p * beta
+  float c2b;              // 2 beta / sqrt(pi)
+  float sw_a, sw_b;       // t = sat(r2 * sw_a + sw_b)
+  float dsw_k;            // 12 / (rc^2 - ron^2)
+};
+
+// force/r for one pair (FP32); returns 0 outside the cutoff or when masked
+template <bool ENERGY>
+__device__ __forceinline__ float pair_force(const PairConst& c, float r2, float qq, float2 ls, bool ok, float& ev,
+                                            float& ee) {
+  const float rinv = rsqrt_a(r2);
+  const float r2inv = rinv * rinv;
+  const float br = r2 * rinv * c.beta;                   // beta r
+  const float ex = ex2_a(r2 * c.eb2);                    // exp(-beta^2 r^2)
+  const float tt = rcp_a(fmaf(kAS_p, br, 1.f));
+  const float poly = tt * fmaf(tt, fmaf(tt, fmaf(tt, fmaf(tt, kAS_a5, kAS_a4), kAS_a3), kAS_a2), kAS_a1);
+  const float qe = qq * ex * rinv;
+  // F_C r / r^2 = qq (erfc(br)/r + 2 beta/sqrt(pi) exp(-b^2 r^2)) / r^2
+  const float fc = qe * fmaf(c.c2b, r2 * rinv, poly) * r2inv;
+  const float s2 = ls.y * r2inv;
+  const float s6 = s2 * s2 * s2;
+  const float a = ls.x * s6;
+  const float b = a * s6;
+  const float elj = b - a;
+  const float flj = fmaf(2.f, b, -a) * (6.f * r2inv);
+  const float t = __saturatef(fmaf(r2, c.sw_a, c.sw_b));
+  const float t2 = t * t;
+  const float sw = fmaf(-t2, fmaf(-2.f, t, 3.f), 1.f);
+  const float dsw = (t - t2) * c.dsw_k;
+  float fr = fmaf(flj, sw, fmaf(elj, dsw, fc));
+  if (ENERGY) {
+    ev += ok ? elj * sw : 0.f;
+    ee += ok ? qe * poly : 0.f;
+  }
+  return ok ? fr : 0.f;
+}
 
 template <bool ENERGY>
 __global__ void __launch_bounds__(256, 3)
-    k_nonbonded(SysParams p, const float4* __restrict__ xyzq, const int* __restrict__ typ,
+    k_nonbonded(SysParams p, PairConst c, const float4* __restrict__ xyzq, const int* __restrict__ typ,
                 const int* __restrict__ perm, const int* __restrict__ tile_i, const uint32_t* __restrict__ tile_j,
                 const int* __restrict__ tile_m, const uint32_t* __restrict__ masks, const int* __restrict__ counters,
                 const float2* __restrict__ ljtab, long long* __restrict__ facc, long long* __restrict__ energy,
                 int tile_cap) {
   extern __shared__ float2 lj[];
+  __shared__ float4 jx_all[kWarps][64];
+  __shared__ int jt_all[kWarps][64];
   const int nt1 = p.ntypes + 1;
   for (int k = threadIdx.x; k < nt1 * nt1; k += blockDim.x) lj[k] = ljtab[k];
   __syncthreads();
   const int ntiles = min(counters[CNT_TILES], tile_cap);
-  const int lane = threadIdx.x & 31;
-  const int nwarps = gridDim.x * (blockDim.x >> 5);
-  const float rc2 = p.rc2, ron2 = p.ron2, c3 = p.sw_c3;
-  const float c2 = rc2 - 3.f * ron2;
-  const float beta = p.beta;
-  const float bc = beta * kTwoOverSqrtPi;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float4* jx = jx_all[warp];
+  int* jt = jt_all[warp];
+  const int nwarps = gridDim.x * kWarps;
   const int n = p.n;
+  const int src = (lane + 1) & 31;
   double e_vdw = 0.0, e_el = 0.0;
-  for (int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < ntiles; t += nwarps) {
+  for (int t = blockIdx.x * kWarps + warp; t < ntiles; t += nwarps) {
     const int ti = tile_i[t];
     const bool diag = ti < 0;
     const int I = ti & 0x7fffffff;
     const int islot = I * 32 + lane;
     const float4 xi = xyzq[islot];
-    const int tyi = typ[islot] * nt1;
+    const float2* ljrow = lj + typ[islot] * nt1;
     const float qi = xi.w * p.cc;
     const uint32_t je = tile_j[(size_t)t * 32 + lane];
     const int jslot = (int)(je & kSlotMask);
@@ -63,63 +128,52 @@ __global__ void __launch_bounds__(256, 3)
       xj.y += s.y;
       xj.z += s.z;
     }
-    int tyj = typ[jslot];
+    const int tyj = typ[jslot];
+    __syncwarp();
+    jx[lane] = xj;
+    jx[lane + 32] = xj;
+    jt[lane] = tyj;
+    jt[lane + 32] = tyj;
     const int m = tile_m[t];
     uint32_t excl = m >= 0 ? masks[(size_t)m * 32 + lane] : 0u;
     if (diag) excl |= (lane == 31) ? 0xffffffffu : ((2u << lane) - 1u);  // j <= i
+    __syncwarp();
+    // bit k of mrot: pair (lane, lane + k) excluded
+    const uint32_t mrot = __funnelshift_r(excl, excl, lane);
+    const float4* jxl = jx + lane;
+    const int* jtl = jt + lane;
     float fix = 0.f, fiy = 0.f, fiz = 0.f;
     float fjx = 0.f, fjy = 0.f, fjz = 0.f;
     float ev = 0.f, ee = 0.f;
-#pragma unroll 4
-    for (int k = 0; k < 32; ++k) {
-      const int jl = (lane + k) & 31;
-      const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-      const bool ok = (r2 < rc2) && !((excl >> jl) & 1u);
-      const float rinv = rsqrtf(r2);
-      const float r2inv = rinv * rinv;
-      // Coulomb, erfc real-space Ewald
-      const float qq = qi * xj.w;
-      const float br = beta * r2 * rinv;
-      const float tt = __fdividef(1.f, fmaf(kAS_p, br, 1.f));
-      const float ex = __expf(-br * br);
-      const float poly = tt * fmaf(tt, fmaf(tt, fmaf(tt, fmaf(tt, kAS_a5, kAS_a4), kAS_a3), kAS_a2), kAS_a1);
-      const float ec = qq * poly * ex * rinv;
-      const float fc = fmaf(qq * bc, ex, ec) * r2inv;
-      // Lennard-Jones with CHARMM switch
-      const float2 ls = lj[tyi + tyj];
-      const float s2 = ls.y * r2inv;
-      const float s6 = s2 * s2 * s2;
-      const float a = ls.x * s6;
-      const float b = a * s6;
-      const float elj = b - a;
-      const float flj = fmaf(12.f, b, -6.f * a) * r2inv;
-      const float u = rc2 - r2;
-      const bool on = r2 > ron2;
-      const float sw = on ? u * u * fmaf(2.f, r2, c2) * c3 : 1.f;
-      const float dsw = on ? 12.f * u * (r2 - ron2) * c3 : 0.f;
-      float fr = fmaf(flj, sw, fmaf(elj, dsw, fc));
-      fr = ok ? fr : 0.f;
-      fix = fmaf(fr, dx, fix);
-      fiy = fmaf(fr, dy, fiy);
-      fiz = fmaf(fr, dz, fiz);
-      fjx = fmaf(-fr, dx, fjx);
-      fjy = fmaf(-fr, dy, fjy);
-      fjz = fmaf(-fr, dz, fjz);
-      if (ENERGY) {
-        ev += ok ? elj * sw : 0.f;
-        ee += ok ? ec : 0.f;
+    if (__any_sync(0xffffffffu, mrot != 0u)) {
+#pragma unroll 8
+      for (int k = 0; k < 32; ++k) {
+        const float4 b = jxl[k];
+        const float dx = xi.x - b.x, dy = xi.y - b.y, dz = xi.z - b.z;
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        const bool ok = (r2 < c.rc2) && !((mrot >> k) & 1u);
+        const float fr = pair_force<ENERGY>(c, r2, qi * b.w, ljrow[jtl[k]], ok, ev, ee);
+        fix = fmaf(fr, dx, fix);
+        fiy = fmaf(fr, dy, fiy);
+        fiz = fmaf(fr, dz, fiz);
+        fjx = __shfl_sync(0xffffffffu, fmaf(-fr, dx, fjx), src);
+        fjy = __shfl_sync(0xffffffffu, fmaf(-fr, dy, fjy), src);
+        fjz = __shfl_sync(0xffffffffu, fmaf(-fr, dz, fjz), src);
       }
-      // rotate j data and j force one lane down
-      const int src = (lane + 1) & 31;
-      xj.x = __shfl_sync(0xffffffffu, xj.x, src);
-      xj.y = __shfl_sync(0xffffffffu, xj.y, src);
-      xj.z = __shfl_sync(0xffffffffu, xj.z, src);
-      xj.w = __shfl_sync(0xffffffffu, xj.w, src);
-      tyj = __shfl_sync(0xffffffffu, tyj, src);
-      fjx = __shfl_sync(0xffffffffu, fjx, src);
-      fjy = __shfl_sync(0xffffffffu, fjy, src);
-      fjz = __shfl_sync(0xffffffffu, fjz, src);
+    } else {
+#pragma unroll 8
+      for (int k = 0; k < 32; ++k) {
+        const float4 b = jxl[k];
+        const float dx = xi.x - b.x, dy = xi.y - b.y, dz = xi.z - b.z;
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        const float fr = pair_force<ENERGY>(c, r2, qi * b.w, ljrow[jtl[k]], r2 < c.rc2, ev, ee);
+        fix = fmaf(fr, dx, fix);
+        fiy = fmaf(fr, dy, fiy);
+        fiz = fmaf(fr, dz, fiz);
+        fjx = __shfl_sync(0xffffffffu, fmaf(-fr, dx, fjx), src);
+        fjy = __shfl_sync(0xffffffffu, fmaf(-fr, dy, fjy), src);
+        fjz = __shfl_sync(0xffffffffu, fmaf(-fr, dz, fjz), src);
+      }
     }
     const int ai = perm[islot];
     if (ai >= 0) {
@@ -147,12 +201,24 @@ __global__ void __launch_bounds__(256, 3)
 void launch_nonbonded(const NonbondedArgs& a, bool energy, cudaStream_t st) {
   const int nt1 = a.p.ntypes + 1;
   const size_t smem = (size_t)nt1 * nt1 * sizeof(float2);
+  PairConst c;
+  c.rc2 = a.p.rc2;
+  c.beta = a.p.beta;
+  c.eb2 = -a.p.beta * a.p.beta * kLog2e;
+  c.p_b = kAS_p * a.p.beta;
+  c.c2b = kTwoOverSqrtPi * a.p.beta;
+  const float d = a.p.rc2 - a.p.ron2;
+  c.sw_a = d > 0.f ? 1.f / d : 0.f;
+  c.sw_b = d > 0.f ? -a.p.ron2 / d : 0.f;
+  c.dsw_k = d > 0.f ? 12.f / d : 0.f;
   if (energy)
-    k_nonbonded<true><<<a.grid, 256, smem, st>>>(a.p, a.xyzq_s, a.typ_s, a.perm, a.tile_i, a.tile_j, a.tile_m,
-                                                 a.masks, a.counters, a.ljtab, a.facc, a.energy, a.tile_cap);
+    k_nonbonded<true><<<a.grid, kWarps * 32, smem, st>>>(a.p, c, a.xyzq_s, a.typ_s, a.perm, a.tile_i, a.tile_j,
+                                                          a.tile_m, a.masks, a.counters, a.ljtab, a.facc, a.energy,
+                                                          a.tile_cap);
   else
-    k_nonbonded<false><<<a.grid, 256, smem, st>>>(a.p, a.xyzq_s, a.typ_s, a.perm, a.tile_i, a.tile_j, a.tile_m,
-                                                  a.masks, a.counters, a.ljtab, a.facc, a.energy, a.tile_cap);
+    k_nonbonded<false><<<a.grid, kWarps * 32, smem, st>>>(a.p, c, a.xyzq_s, a.typ_s, a.perm, a.tile_i, a.tile_j,
+                                                           a.tile_m, a.masks, a.counters, a.ljtab, a.facc, a.energy,
+                                                           a.tile_cap);
 }
 
 }  // namespace fzk

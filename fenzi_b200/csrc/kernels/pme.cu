@@ -74,7 +74,9 @@ __global__ void k_pme_bin(PmeArgs a) {
   const int kz = grid_base(r.z, a.p.inv_box.z, a.K[2], &t);
   const int b = ((kz / a.B[2]) * a.nb[1] + ky / a.B[1]) * a.nb[0] + kx / a.B[0];
   a.brick_of[i] = b;
-  atomicAdd(&a.brick_count[b], 1);
+  // warp-aggregated increment: one atomic per distinct brick in the warp
+  const unsigned peers = __match_any_sync(__activemask(), b);
+  if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&a.brick_count[b], __popc(peers));
 }
 
 __global__ void k_pme_scan(PmeArgs a, int nbr) {
@@ -104,12 +106,21 @@ __global__ void k_pme_scatter(PmeArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.n) return;
   const int b = a.brick_of[i];
-  const int k = atomicAdd(&a.brick_cursor[b], 1);
+  const unsigned peers = __match_any_sync(__activemask(), b);
+  const int leader = __ffs(peers) - 1;
+  int base = 0;
+  if ((threadIdx.x & 31) == leader) base = atomicAdd(&a.brick_cursor[b], __popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  const int k = base + __popc(peers & ((1u << (threadIdx.x & 31)) - 1u));
   a.brick_atoms[a.brick_start[b] + k] = i;
 }
 
+// charge-grid accumulation in shared memory: int32 fixed point, 2^24 per e (values
+// stay far below the +-128 e range a grid point could hold), native shared atomics
+constexpr float kFixQ32 = 16777216.0f;
+
 __global__ void __launch_bounds__(128) k_pme_spread(PmeArgs a) {
-  extern __shared__ long long acc[];
+  extern __shared__ int acc[];
   const int Bx = a.B[0], By = a.B[1], Bz = a.B[2];
   const int nbx = a.nb[0], nby = a.nb[1], nbz = a.nb[2];
   const int b = blockIdx.x;
@@ -136,12 +147,18 @@ __global__ void __launch_bounds__(128) k_pme_spread(PmeArgs a) {
           bsp4(ty, wy, nullptr);
           bsp4(tz, wz, nullptr);
           const float q = r.w;
+          // local offsets of grid points k0 - j inside this brick (k0 - j - o lies in
+          // (-K, K) so one conditional wrap suffices); >= B means another brick owns it
           int lxs[4], lys[4], lzs[4];
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
-            lxs[j] = ((kx - j - ox) % Kx + Kx) % Kx;
-            lys[j] = ((ky - j - oy) % Ky + Ky) % Ky;
-            lzs[j] = ((kz - j - oz) % Kz + Kz) % Kz;
+            int vx = kx - j - ox, vy = ky - j - oy, vz = kz - j - oz;
+            vx += vx < 0 ? Kx : 0;
+            vy += vy < 0 ? Ky : 0;
+            vz += vz < 0 ? Kz : 0;
+            lxs[j] = vx;
+            lys[j] = vy;
+            lzs[j] = vz;
           }
 #pragma unroll
           for (int jz = 0; jz < 4; ++jz) {
@@ -150,12 +167,11 @@ __global__ void __launch_bounds__(128) k_pme_spread(PmeArgs a) {
             for (int jy = 0; jy < 4; ++jy) {
               if (lys[jy] >= By) continue;
               const float qzy = q * wz[jz] * wy[jy];
-              long long* rowp = &acc[(lzs[jz] * By + lys[jy]) * Bx];
+              int* rowp = &acc[(lzs[jz] * By + lys[jy]) * Bx];
 #pragma unroll
               for (int jx = 0; jx < 4; ++jx) {
                 if (lxs[jx] >= Bx) continue;
-                const long long v = __double2ll_rn((double)(qzy * wx[jx]) * kFixQ);
-                atomicAdd(reinterpret_cast<unsigned long long*>(rowp + lxs[jx]), (unsigned long long)v);
+                atomicAdd(rowp + lxs[jx], __float2int_rn(qzy * wx[jx] * kFixQ32));
               }
             }
           }
@@ -164,7 +180,7 @@ __global__ void __launch_bounds__(128) k_pme_spread(PmeArgs a) {
   __syncthreads();
   for (int k = threadIdx.x; k < vol; k += blockDim.x) {
     const int lx = k % Bx, ly = (k / Bx) % By, lz = k / (Bx * By);
-    a.grid[((size_t)(oz + lz) * Ky + (oy + ly)) * Kx + (ox + lx)] = (float)((double)acc[k] * (1.0 / kFixQ));
+    a.grid[((size_t)(oz + lz) * Ky + (oy + ly)) * Kx + (ox + lx)] = (float)acc[k] * (1.0f / kFixQ32);
   }
 }
 
@@ -172,7 +188,7 @@ __global__ void __launch_bounds__(128) k_pme_spread(PmeArgs a) {
 // Stockham autosort FFT of nl lines of length n in shared memory (x at a[l*n + i]).
 // Returns the buffer holding the result.
 __device__ float2* fft_lines(float2* a, float2* b, const float2* tw, const FftPlan& pl, int nl, bool inv) {
-  const int n = pl.n;
+  const int n = pl.n, ld = n + 1;
   int Ns = 1;
   for (int s = 0; s < pl.nrad; ++s) {
     const int R = pl.rad[s];
@@ -180,8 +196,8 @@ __device__ float2* fft_lines(float2* a, float2* b, const float2* tw, const FftPl
     const int step = n / (Ns * R);
     for (int idx = threadIdx.x; idx < nl * nbf; idx += blockDim.x) {
       const int l = idx / nbf, j = idx - l * nbf;
-      const float2* x = a + l * n;
-      float2* y = b + l * n;
+      const float2* x = a + l * ld;
+      float2* y = b + l * ld;
       const int k = j % Ns;
       float2 v[5], V[5];
 #pragma unroll
@@ -254,22 +270,23 @@ __global__ void __launch_bounds__(256) k_fft_x_r2c(PmeArgs a, FftPlan pl, int nl
   extern __shared__ float2 sm[];
   const int Kx = a.K[0], Kxh = Kx / 2 + 1;
   const int nrows = a.K[1] * a.K[2];
+  const int ld = Kx + 1;
   float2* tw = sm;
   float2* A = sm + Kx;
-  float2* B = A + nl * Kx;
+  float2* B = A + nl * ld;
   load_tw(tw, a.tw[0], Kx);
   const int r0 = blockIdx.x * nl;
   for (int idx = threadIdx.x; idx < nl * Kx; idx += blockDim.x) {
     const int l = idx / Kx, x = idx - l * Kx;
     const int row = r0 + l;
-    A[idx] = make_float2(row < nrows ? a.grid[(size_t)row * Kx + x] : 0.f, 0.f);
+    A[l * ld + x] = make_float2(row < nrows ? a.grid[(size_t)row * Kx + x] : 0.f, 0.f);
   }
   __syncthreads();
   const float2* R = fft_lines(A, B, tw, pl, nl, false);
   for (int idx = threadIdx.x; idx < nl * Kxh; idx += blockDim.x) {
     const int l = idx / Kxh, m = idx - l * Kxh;
     const int row = r0 + l;
-    if (row < nrows) a.cgrid[(size_t)row * Kxh + m] = R[l * Kx + m];
+    if (row < nrows) a.cgrid[(size_t)row * Kxh + m] = R[l * ld + m];
   }
 }
 
@@ -279,21 +296,22 @@ __global__ void __launch_bounds__(256) k_fft_y(PmeArgs a, FftPlan pl, int nl, in
   const int Kx = a.K[0], Ky = a.K[1], Kxh = Kx / 2 + 1;
   const int ng = (Kxh + nl - 1) / nl;
   const int z = blockIdx.x / ng, mx0 = (blockIdx.x % ng) * nl;
+  const int ld = Ky + 1;
   float2* tw = sm;
   float2* A = sm + Ky;
-  float2* B = A + nl * Ky;
+  float2* B = A + nl * ld;
   load_tw(tw, a.tw[1], Ky);
   for (int idx = threadIdx.x; idx < nl * Ky; idx += blockDim.x) {
     const int y = idx / nl, l = idx - y * nl;
     const int mx = mx0 + l;
-    A[l * Ky + y] = mx < Kxh ? a.cgrid[((size_t)z * Ky + y) * Kxh + mx] : make_float2(0.f, 0.f);
+    A[l * ld + y] = mx < Kxh ? a.cgrid[((size_t)z * Ky + y) * Kxh + mx] : make_float2(0.f, 0.f);
   }
   __syncthreads();
   const float2* R = fft_lines(A, B, tw, pl, nl, inv != 0);
   for (int idx = threadIdx.x; idx < nl * Ky; idx += blockDim.x) {
     const int y = idx / nl, l = idx - y * nl;
     const int mx = mx0 + l;
-    if (mx < Kxh) a.cgrid[((size_t)z * Ky + y) * Kxh + mx] = R[l * Ky + y];
+    if (mx < Kxh) a.cgrid[((size_t)z * Ky + y) * Kxh + mx] = R[l * ld + y];
   }
 }
 
@@ -304,14 +322,15 @@ __global__ void __launch_bounds__(256) k_fft_z_conv(PmeArgs a, FftPlan pl, int n
   const int Kx = a.K[0], Ky = a.K[1], Kz = a.K[2], Kxh = Kx / 2 + 1;
   const int ng = (Kxh + nl - 1) / nl;
   const int y = blockIdx.x / ng, mx0 = (blockIdx.x % ng) * nl;
+  const int ld = Kz + 1;
   float2* tw = sm;
   float2* A = sm + Kz;
-  float2* B = A + nl * Kz;
+  float2* B = A + nl * ld;
   load_tw(tw, a.tw[2], Kz);
   for (int idx = threadIdx.x; idx < nl * Kz; idx += blockDim.x) {
     const int z = idx / nl, l = idx - z * nl;
     const int mx = mx0 + l;
-    A[l * Kz + z] = mx < Kxh ? a.cgrid[((size_t)z * Ky + y) * Kxh + mx] : make_float2(0.f, 0.f);
+    A[l * ld + z] = mx < Kxh ? a.cgrid[((size_t)z * Ky + y) * Kxh + mx] : make_float2(0.f, 0.f);
   }
   __syncthreads();
   float2* R = fft_lines(A, B, tw, pl, nl, false);
@@ -321,7 +340,7 @@ __global__ void __launch_bounds__(256) k_fft_z_conv(PmeArgs a, FftPlan pl, int n
   for (int idx = threadIdx.x; idx < nl * Kz; idx += blockDim.x) {
     const int l = idx / Kz, z = idx - l * Kz;
     const int mx = mx0 + l;
-    float2 v = R[idx];
+    float2 v = R[l * ld + z];
     float G = 0.f;
     if (mx < Kxh && (mx | y | z) != 0) {
       const float den = a.f2[0][mx] + fy2 + a.f2[2][z];
@@ -333,14 +352,14 @@ __global__ void __launch_bounds__(256) k_fft_z_conv(PmeArgs a, FftPlan pl, int n
     }
     v.x *= G;
     v.y *= G;
-    R[idx] = v;
+    R[l * ld + z] = v;
   }
   __syncthreads();
   const float2* Q = fft_lines(R, O, tw, pl, nl, true);
   for (int idx = threadIdx.x; idx < nl * Kz; idx += blockDim.x) {
     const int z = idx / nl, l = idx - z * nl;
     const int mx = mx0 + l;
-    if (mx < Kxh) a.cgrid[((size_t)z * Ky + y) * Kxh + mx] = Q[l * Kz + z];
+    if (mx < Kxh) a.cgrid[((size_t)z * Ky + y) * Kxh + mx] = Q[l * ld + z];
   }
   if (ENERGY) energy_add(a.energy + EN_PME, e);
 }
@@ -350,9 +369,10 @@ __global__ void __launch_bounds__(256) k_fft_x_c2r(PmeArgs a, FftPlan pl, int nl
   extern __shared__ float2 sm[];
   const int Kx = a.K[0], Kxh = Kx / 2 + 1;
   const int nrows = a.K[1] * a.K[2];
+  const int ld = Kx + 1;
   float2* tw = sm;
   float2* A = sm + Kx;
-  float2* B = A + nl * Kx;
+  float2* B = A + nl * ld;
   load_tw(tw, a.tw[0], Kx);
   const int r0 = blockIdx.x * nl;
   for (int idx = threadIdx.x; idx < nl * Kx; idx += blockDim.x) {
@@ -366,20 +386,22 @@ __global__ void __launch_bounds__(256) k_fft_x_c2r(PmeArgs a, FftPlan pl, int nl
         v.y = -v.y;
       }
     }
-    A[idx] = v;
+    A[l * ld + m] = v;
   }
   __syncthreads();
   const float2* R = fft_lines(A, B, tw, pl, nl, true);
   for (int idx = threadIdx.x; idx < nl * Kx; idx += blockDim.x) {
     const int l = idx / Kx, x = idx - l * Kx;
     const int row = r0 + l;
-    if (row < nrows) a.grid[(size_t)row * Kx + x] = R[idx].x;
+    if (row < nrows) a.grid[(size_t)row * Kx + x] = R[l * ld + x].x;
   }
 }
 
+// one thread per atom, atoms taken in brick order so a warp reads neighbouring grid lines
 __global__ void __launch_bounds__(256) k_pme_gather(PmeArgs a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.n) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.n) return;
+  const int i = a.brick_atoms[t];
   const int Kx = a.K[0], Ky = a.K[1], Kz = a.K[2];
   const float4 r = a.pos4[i];
   float tx, ty, tz, wx[4], wy[4], wz[4], dx[4], dy[4], dz[4];
@@ -439,15 +461,15 @@ void launch_pme(const PmeArgs& a, bool energy, cudaStream_t st) {
   k_pme_bin<<<(a.n + 255) / 256, 256, 0, st>>>(a);
   k_pme_scan<<<1, 1024, 0, st>>>(a, nbr);
   k_pme_scatter<<<(a.n + 255) / 256, 256, 0, st>>>(a);
-  const size_t sp = (size_t)a.B[0] * a.B[1] * a.B[2] * sizeof(long long);
+  const size_t sp = (size_t)a.B[0] * a.B[1] * a.B[2] * sizeof(int);
   k_pme_spread<<<nbr, 128, sp, st>>>(a);
   const int Kx = a.K[0], Ky = a.K[1], Kz = a.K[2], Kxh = Kx / 2 + 1;
   const FftPlan px = make_plan(Kx), py = make_plan(Ky), pz = make_plan(Kz);
   const int lx = lines_for(Kx), ly = lines_for(Ky), lz = lines_for(Kz);
   const int rows = Ky * Kz;
-  const size_t smx = (size_t)(Kx + 2 * lx * Kx) * sizeof(float2);
-  const size_t smy = (size_t)(Ky + 2 * ly * Ky) * sizeof(float2);
-  const size_t smz = (size_t)(Kz + 2 * lz * Kz) * sizeof(float2);
+  const size_t smx = (size_t)(Kx + 2 * lx * (Kx + 1)) * sizeof(float2);
+  const size_t smy = (size_t)(Ky + 2 * ly * (Ky + 1)) * sizeof(float2);
+  const size_t smz = (size_t)(Kz + 2 * lz * (Kz + 1)) * sizeof(float2);
   k_fft_x_r2c<<<(rows + lx - 1) / lx, 256, smx, st>>>(a, px, lx);
   k_fft_y<<<Kz * ((Kxh + ly - 1) / ly), 256, smy, st>>>(a, py, ly, 0);
   if (energy)
