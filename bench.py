@@ -309,6 +309,7 @@ def main():
                                   "model": "60 FLOP/pair / FP32 peak + (56N + 24K^3 + 120N) B / HBM"},
                 "stages_ms": stages, "rebuilds_in_timed_steps": rebuilds,
                 "pair_tiles": sysm.counters()["tiles"],
+                "prunes_total": sysm.counters()["prunes"],
                 "pair_slot_efficiency": pairs / (sysm.counters()["tiles"] * 1024.0),
                 "roofline": roof, "cpu_baseline": cpu,
                 "e2e": {"value": e2e_nsd, "unit": "ns/day", "h2d_bytes_per_step": 24 * natom,

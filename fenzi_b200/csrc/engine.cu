@@ -8,12 +8,14 @@
 //   pos4  float4[n]   x, y, z, q          vel4 float4[n]  vx, vy, vz, 1/m
 //   facc  int64[3n]   force accumulator, fixed point 2^32, SoA x|y|z
 //   xyzq_s float4[S], typ_s int[S], perm int[S]   sorted slots (S = n + 32*columns + 32)
-//   tile_i/tile_j/tile_m/masks                   pair tiles (see kernels/neighbor.cu)
+//   outer/inner uint32[blocks x ocap]            per-block pair lists (kernels/neighbor.cu):
+//                                                outer at rlist (rebuild), inner at rc + 0.3 (prune)
 //   grid float[K^3], cgrid float2[Kz*Ky*(Kx/2+1)] PME
 // A step is ~20 launches and no host synchronisation; fz_step checks the sticky
 // device status word once per call.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -34,7 +36,9 @@ struct Engine {
   cudaStream_t st = nullptr;
   bool own_stream = false;
   fzk::SysParams p{};
-  int n = 0, nunits = 0, ncol = 0, nslots = 0, tile_cap = 0, mask_cap = 0, all_images = 0;
+  int n = 0, nunits = 0, ncol = 0, nslots = 0, mask_cap = 0, all_images = 0;
+  int ocap = 0;            // per-block pair-list capacity (multiple of 32)
+  float rp2 = 0.f, prune_half2 = 0.f;
   int nb_grid = 0;
   int dcx = 1, dcy = 1;
   int* blk_col = nullptr;
@@ -47,8 +51,11 @@ struct Engine {
   float4 *xyzq_s = nullptr, *bb_lo = nullptr, *bb_hi = nullptr;
   int *typ_s = nullptr, *perm = nullptr, *inv_perm = nullptr, *col_of = nullptr, *col_count = nullptr,
       *col_cursor = nullptr, *col_start = nullptr, *col_tmp = nullptr;
-  int *tile_i = nullptr, *tile_m = nullptr;
-  uint32_t *tile_j = nullptr, *masks = nullptr;
+  uint32_t *outer = nullptr, *inner = nullptr, *masks = nullptr, *dmask = nullptr;
+  int *outer_n = nullptr, *inner_nt = nullptr, *inner_m = nullptr, *flag_prune = nullptr;
+  float4* pos_prune = nullptr;
+  int2* items = nullptr;
+  int chunk = 16;
   int *excl_off = nullptr, *excl_idx = nullptr;
   int *flag = nullptr, *counters = nullptr, *status = nullptr;
   float2 *ljtab = nullptr, *lj14 = nullptr;
@@ -91,6 +98,9 @@ struct Engine {
   cudaGraph_t step_graph = nullptr;
   cudaGraphExec_t step_exec = nullptr;
   bool use_graph = true;
+  // PME runs on a second stream concurrently with the pair and bonded kernels
+  cudaStream_t st2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // pinned staging
   void* pinned = nullptr;
   size_t pinned_bytes = 0;
@@ -136,6 +146,9 @@ struct Engine {
     if (st) cudaStreamSynchronize(st);
     if (step_exec) cudaGraphExecDestroy(step_exec);
     if (step_graph) cudaGraphDestroy(step_graph);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (st2) cudaStreamDestroy(st2);
     for (auto& x : ev)
       if (x) cudaEventDestroy(x);
     for (void* p : allocs) cudaFree(p);
@@ -165,13 +178,21 @@ struct Engine {
     a.bb_hi = bb_hi;
     a.excl_off = excl_off;
     a.excl_idx = excl_idx;
-    a.tile_i = tile_i;
-    a.tile_j = tile_j;
-    a.tile_m = tile_m;
     a.masks = masks;
-    a.tile_cap = tile_cap;
     a.mask_cap = mask_cap;
     a.all_images = all_images;
+    a.outer = outer;
+    a.outer_n = outer_n;
+    a.inner = inner;
+    a.inner_nt = inner_nt;
+    a.inner_m = inner_m;
+    a.dmask = dmask;
+    a.ocap = ocap;
+    a.flag_prune = flag_prune;
+    a.rp2 = rp2;
+    a.pos_prune = pos_prune;
+    a.items = items;
+    a.chunk = chunk;
     a.blk_col = blk_col;
     a.dcx = dcx;
     a.dcy = dcy;
@@ -183,15 +204,18 @@ struct Engine {
     a.xyzq_s = xyzq_s;
     a.typ_s = typ_s;
     a.perm = perm;
-    a.tile_i = tile_i;
-    a.tile_j = tile_j;
-    a.tile_m = tile_m;
+    a.inner = inner;
+    a.inner_nt = inner_nt;
+    a.inner_m = inner_m;
+    a.dmask = dmask;
     a.masks = masks;
     a.counters = counters;
     a.ljtab = ljtab;
     a.facc = facc;
     a.energy = energy;
-    a.tile_cap = tile_cap;
+    a.ocap = ocap;
+    a.items = items;
+    a.chunk = chunk;
     a.grid = nb_grid;
     return a;
   }
@@ -263,7 +287,10 @@ struct Engine {
     a.xyzq_s = xyzq_s;
     a.inv_perm = inv_perm;
     a.pos_build = pos_build;
+    a.pos_prune = pos_prune;
     a.flag = flag;
+    a.flag_prune = flag_prune;
+    a.prune_half2 = prune_half2;
     a.status = status;
     a.energy = energy;
     a.dtu = dtu;
@@ -283,7 +310,7 @@ struct Engine {
   void forces(bool energies, int terms = FZ_TERM_ALL) {
     mark(1);
     fzk::launch_rebuild(rebuild_args(), st);
-    launches += 8;
+    launches += 11;
     mark(2);
     if (terms & FZ_TERM_NONBONDED) {
       fzk::launch_nonbonded(nb_args(), energies, st);
@@ -316,10 +343,24 @@ struct Engine {
     stage_ms[4] += el(0, 1) + el(5, 6);
     timed_steps++;
   }
+  // forces with PME on st2, overlapping the pair and bonded kernels on st
+  void forces_overlapped() {
+    fzk::launch_rebuild(rebuild_args(), st);
+    cudaEventRecord(ev_fork, st);
+    cudaStreamWaitEvent(st2, ev_fork, 0);
+    fzk::launch_pme(pme_args(), false, st2);
+    fzk::launch_nonbonded(nb_args(), false, st);
+    fzk::launch_bonded(bonded_args(), false, st);
+    cudaEventRecord(ev_join, st2);
+    cudaStreamWaitEvent(st, ev_join, 0);
+  }
   void step_body() {
     const fzk::IntegrateArgs ia = int_args();
     fzk::launch_kick_drift(ia, st);
-    forces(false);
+    if (st2)
+      forces_overlapped();
+    else
+      forces(false);
     fzk::launch_kick_rattle(ia, false, true, st);
   }
   fz_status graph_step() {
@@ -334,7 +375,7 @@ struct Engine {
       FZ_CUDA(cudaGraphInstantiate(&step_exec, step_graph, 0));
     }
     FZ_CUDA(cudaGraphLaunch(step_exec, st));
-    launches += 2 + 8 + 1 + ((nbond + nangle + nub + ndihe + nimpr + nexcl + n14 > 0) ? 1 : 0) + 11;
+    launches += 2 + 11 + 1 + ((nbond + nangle + nub + ndihe + nimpr + nexcl + n14 > 0) ? 1 : 0) + 11;
     return FZ_OK;
   }
   void drop_graph() {
@@ -406,6 +447,9 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
     FZ_CUDA(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
     e->own_stream = true;
   }
+  FZ_CUDA(cudaStreamCreateWithFlags(&e->st2, cudaStreamNonBlocking));
+  FZ_CUDA(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
+  FZ_CUDA(cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming));
   const int n = t.n;
   e->n = n;
   const int nt = (int)t.type_names.size();
@@ -452,12 +496,17 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
     e->nbk[d] = e->K[d] / e->B[d];
     p.K[d] = e->K[d];
   }
-  // tile capacity: j atoms within rlist of a block box (Minkowski volume), half by Newton-3
+  // per-block list capacity: atoms within rlist of a block box (Minkowski volume of a
+  // box ~1.4 a), with room for blocks that see all their neighbours at higher index
   const double ab = 1.4 * a, R = plist;
   const double vm = ab * ab * ab + 6 * ab * ab * R + 3 * M_PI * ab * R * R + 4.0 / 3.0 * M_PI * R * R * R;
-  const double per_blk = rho * vm * 0.5 / 32.0 + 3.0;
-  e->tile_cap = (int)std::min(2.0e9 / 132.0, 1.5 * per_blk * (e->nslots / 32) + 4096);
-  e->mask_cap = e->tile_cap;
+  e->ocap = (int)std::ceil(std::max(256.0, 1.25 * rho * vm) / 32.0) * 32;
+  e->mask_cap = (e->nslots / 32) * (e->ocap / 32);
+  {
+    const double delta = std::min(0.3, plist - c.cutoff);
+    e->rp2 = (float)((c.cutoff + delta) * (c.cutoff + delta));
+    e->prune_half2 = (float)(0.25 * delta * delta);
+  }
   e->dtu = c.timestep_ps * kTU;
   e->shake_tol = c.shake_tol > 0 ? c.shake_tol : 1e-10;
   e->temp_reset_every = c.temp_reset_every;
@@ -467,7 +516,12 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
   e->ncons = (int)t.cons_d.size();
   int dev_sms = 148;
   cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device);
-  e->nb_grid = dev_sms * 3;
+  // pair kernel CTAs per SM (3 = register-limited maximum); PME overlaps it on a second stream
+  {
+    const char* v = std::getenv("FZ_NB_CTAS_PER_SM");
+    const int per = v ? std::max(1, std::min(3, std::atoi(v))) : 3;
+    e->nb_grid = dev_sms * per;
+  }
   // ---- atom arrays
   std::vector<float4> pos4(n), vel4(n);
   double mt = 0;
@@ -488,8 +542,11 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
       (r = e->alloc(&e->inv_perm, n)) || (r = e->alloc(&e->col_of, n)) || (r = e->alloc(&e->col_count, e->ncol)) ||
       (r = e->alloc(&e->col_cursor, e->ncol)) || (r = e->alloc(&e->col_start, e->ncol + 1)) ||
       (r = e->alloc(&e->col_tmp, nslots)) || (r = e->alloc(&e->bb_lo, nblk)) || (r = e->alloc(&e->blk_col, nblk)) || (r = e->alloc(&e->bb_hi, nblk)) ||
-      (r = e->alloc(&e->tile_i, e->tile_cap)) || (r = e->alloc(&e->tile_m, e->tile_cap)) ||
-      (r = e->alloc(&e->tile_j, (size_t)e->tile_cap * 32)) || (r = e->alloc(&e->masks, (size_t)e->mask_cap * 32)) ||
+      (r = e->alloc(&e->outer, (size_t)nblk * e->ocap)) || (r = e->alloc(&e->inner, (size_t)nblk * e->ocap)) ||
+      (r = e->alloc(&e->outer_n, nblk)) || (r = e->alloc(&e->inner_nt, nblk)) ||
+      (r = e->alloc(&e->inner_m, (size_t)nblk * (e->ocap / 32))) || (r = e->alloc(&e->dmask, (size_t)nblk * 32)) ||
+      (r = e->alloc(&e->masks, (size_t)e->mask_cap * 32)) || (r = e->alloc(&e->pos_prune, n)) ||
+      (r = e->alloc(&e->flag_prune, 1)) || (r = e->alloc(&e->items, (size_t)nblk * (e->ocap / 32 + 1))) ||
       (r = e->alloc(&e->flag, 1)) || (r = e->alloc(&e->counters, fzk::CNT_COUNT)) || (r = e->alloc(&e->status, 1)))
     return r;
   {
@@ -617,24 +674,40 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
   FZ_CUDA(cudaMemcpyAsync(cnt, e->counters, sizeof(cnt), cudaMemcpyDeviceToHost, e->st));
   FZ_CUDA(cudaStreamSynchronize(e->st));
   FZ_CUDA(cudaGetLastError());
-  // size tile storage to the measured list (2x headroom for density fluctuations)
+  // grow the per-block lists if the measured neighbourhood did not fit (status bit)
   int st_h = 0;
   FZ_CUDA(cudaMemcpy(&st_h, e->status, sizeof(int), cudaMemcpyDeviceToHost));
-  if ((st_h & (fzk::ST_TILE_OVERFLOW | fzk::ST_MASK_OVERFLOW)) || cnt[fzk::CNT_TILES] * 2 > e->tile_cap) {
-    const int want = std::max(cnt[fzk::CNT_TILES], e->tile_cap) * 2 + 4096;
+  for (int tries = 0; (st_h & (fzk::ST_TILE_OVERFLOW | fzk::ST_MASK_OVERFLOW)) && tries < 4; ++tries) {
     FZ_CUDA(cudaStreamSynchronize(e->st));
-    e->release(e->tile_i);
-    e->release(e->tile_m);
-    e->release(e->tile_j);
+    e->release(e->outer);
+    e->release(e->inner);
+    e->release(e->inner_m);
     e->release(e->masks);
-    e->tile_cap = e->mask_cap = want;
-    if ((r = e->alloc(&e->tile_i, want)) || (r = e->alloc(&e->tile_m, want)) ||
-        (r = e->alloc(&e->tile_j, (size_t)want * 32)) || (r = e->alloc(&e->masks, (size_t)want * 32)))
+    e->ocap *= 2;
+    e->mask_cap = nblk * (e->ocap / 32);
+    e->release(e->items);
+    if ((r = e->alloc(&e->items, (size_t)nblk * (e->ocap / 32 + 1))) ||
+        (r = e->alloc(&e->outer, (size_t)nblk * e->ocap)) || (r = e->alloc(&e->inner, (size_t)nblk * e->ocap)) ||
+        (r = e->alloc(&e->inner_m, (size_t)nblk * (e->ocap / 32))) || (r = e->alloc(&e->masks, (size_t)e->mask_cap * 32)))
       return r;
     const int zero = 0;
     FZ_CUDA(cudaMemcpyAsync(e->status, &zero, sizeof(int), cudaMemcpyHostToDevice, e->st));
     FZ_CUDA(cudaMemcpyAsync(e->flag, &one, sizeof(int), cudaMemcpyHostToDevice, e->st));
     fzk::launch_rebuild(e->rebuild_args(), e->st);
+    FZ_CUDA(cudaMemcpyAsync(&st_h, e->status, sizeof(int), cudaMemcpyDeviceToHost, e->st));
+    FZ_CUDA(cudaStreamSynchronize(e->st));
+  }
+  // tiles per pair-kernel work item: enough items to keep ~24 warps per SM busy
+  {
+    int cnt2[fzk::CNT_COUNT];
+    FZ_CUDA(cudaMemcpyAsync(cnt2, e->counters, sizeof(cnt2), cudaMemcpyDeviceToHost, e->st));
+    FZ_CUDA(cudaStreamSynchronize(e->st));
+    const int want = std::max(1, std::min(16, cnt2[fzk::CNT_TILES] / (dev_sms * 24)));
+    if (want != e->chunk) {
+      e->chunk = want;
+      FZ_CUDA(cudaMemcpyAsync(e->flag_prune, &one, sizeof(int), cudaMemcpyHostToDevice, e->st));
+      fzk::launch_rebuild(e->rebuild_args(), e->st);
+    }
   }
   FZ_CUDA(cudaStreamSynchronize(e->st));
   return e->check();
@@ -884,7 +957,7 @@ extern "C" fz_status fz_get_counters(fz_system* s, long long* out4) {
   out4[0] = e->launches;
   out4[1] = cnt[fzk::CNT_REBUILDS];
   out4[2] = cnt[fzk::CNT_TILES];
-  out4[3] = e->tile_cap;
+  out4[3] = cnt[fzk::CNT_PRUNES];
   return FZ_OK;
 }
 

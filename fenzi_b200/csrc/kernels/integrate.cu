@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(128) k_kick_drift(IntegrateArgs a) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) v[k][c] = (rn[k][c] - r0[k][c]) * idt;  // v += dr/(dt TU)
   }
-  bool far = false;
+  bool far = false, moved = false;
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     if (k >= U.na) continue;
@@ -250,8 +250,12 @@ __global__ void __launch_bounds__(128) k_kick_drift(IntegrateArgs a) {
     const float4 pb = a.pos_build[i];
     const float dx = np.x - pb.x, dy = np.y - pb.y, dz = np.z - pb.z;
     far |= dx * dx + dy * dy + dz * dz > a.p.skin_half2;
+    const float4 pp = a.pos_prune[i];
+    const float ex = np.x - pp.x, ey = np.y - pp.y, ez = np.z - pp.z;
+    moved |= ex * ex + ey * ey + ez * ez > a.prune_half2;
   }
   if (far) *a.flag = 1;
+  if (moved) *a.flag_prune = 1;
 }
 
 template <bool KIN>

@@ -5,7 +5,7 @@
 namespace fzk {
 
 constexpr int kColCap = 4096;  // atoms per column sorted in shared memory
-enum : int { CNT_TILES = 0, CNT_MASKS, CNT_SLOTS, CNT_REBUILDS, CNT_PAIRS, CNT_COUNT = 8 };
+enum : int { CNT_TILES = 0, CNT_MASKS, CNT_SLOTS, CNT_REBUILDS, CNT_PRUNES, CNT_WORK, CNT_ITEMS, CNT_COUNT = 8 };
 
 struct RebuildArgs {
   SysParams p;
@@ -21,13 +21,23 @@ struct RebuildArgs {
   int* typ_s;
   float4 *bb_lo, *bb_hi;
   const int *excl_off, *excl_idx;
-  int* tile_i;
-  uint32_t* tile_j;
-  int* tile_m;
   uint32_t* masks;
-  int tile_cap, mask_cap, all_images;
+  int mask_cap, all_images;
   int* blk_col;   // block -> column
   int dcx, dcy;   // column offsets searched for neighbour blocks
+  // per-i-block pair lists: outer (rlist, at rebuild) and inner (rc + delta, at prune)
+  uint32_t* outer;
+  int* outer_n;
+  uint32_t* inner;
+  int* inner_nt;
+  int* inner_m;
+  uint32_t* dmask;
+  int ocap;
+  int* flag_prune;
+  float rp2;
+  float4* pos_prune;
+  int2* items;   // pair-kernel work items (i-block, first tile)
+  int chunk;     // tiles per work item
 };
 void launch_rebuild(const RebuildArgs& a, cudaStream_t st);
 
@@ -36,15 +46,18 @@ struct NonbondedArgs {
   const float4* xyzq_s;
   const int* typ_s;
   const int* perm;
-  const int* tile_i;
-  const uint32_t* tile_j;
-  const int* tile_m;
+  const uint32_t* inner;
+  const int* inner_nt;
+  const int* inner_m;
+  const uint32_t* dmask;
   const uint32_t* masks;
-  const int* counters;
+  int* counters;        // CNT_ITEMS (work items), CNT_WORK (dynamic item counter, zeroed per launch)
+  const int2* items;
+  int chunk;
   const float2* ljtab;  // (ntypes+1)^2 (4 eps, sigma^2)
   long long* facc;      // 3 x n fixed point
   long long* energy;    // energy slots
-  int tile_cap;
+  int ocap;
   int grid;
 };
 void launch_nonbonded(const NonbondedArgs& a, bool energy, cudaStream_t st);
@@ -103,7 +116,10 @@ struct IntegrateArgs {
   float4* xyzq_s;
   const int* inv_perm;
   const float4* pos_build;
+  const float4* pos_prune;
   int* flag;
+  int* flag_prune;
+  float prune_half2;        // (delta/2)^2
   int* status;
   long long* energy;
   double dtu;               // dt * TU

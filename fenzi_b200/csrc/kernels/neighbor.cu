@@ -21,10 +21,7 @@ __global__ void k_rb_begin(const int* __restrict__ flag, int* col_count, int* co
     col_count[c] = 0;
     col_cursor[c] = 0;
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    counters[CNT_TILES] = 0;
-    counters[CNT_MASKS] = 0;
-  }
+
 }
 
 // wrap positions into [-L/2, L/2), record build positions, bin into columns
@@ -209,72 +206,27 @@ __device__ __forceinline__ float box_gap2(float3 d, float3 h) {
   return gx * gx + gy * gy + gz * gz;
 }
 
-// warp per i-block: find j-blocks J >= I within rlist, compact their j atoms into
-// 32-entry tiles, build exclusion masks.  all_images: test all 27 images (small boxes)
-__global__ void __launch_bounds__(256) k_rb_tiles(SysParams p, const int* __restrict__ flag, int* counters,
-                                                  const int* __restrict__ perm, const int* __restrict__ inv_perm,
+// Outer pair list, warp per i-block: every atom of a block J >= I (Newton's third law),
+// at every periodic image, whose position lies within rlist of block I's bounding box.
+// The diagonal block (J == I, no image) is implicit and not stored.  Entries append to
+// the block's own region outer[I * ocap ...] in a fixed order (deterministic).
+__global__ void __launch_bounds__(256) k_rb_outer(SysParams p, const int* __restrict__ flag,
+                                                  const int* __restrict__ counters, const int* __restrict__ perm,
                                                   const float4* __restrict__ xyzq_s, const float4* __restrict__ bb_lo,
-                                                  const float4* __restrict__ bb_hi, const int* __restrict__ excl_off,
-                                                  const int* __restrict__ excl_idx, int* tile_i, uint32_t* tile_j,
-                                                  int* tile_m, uint32_t* masks, int tile_cap, int mask_cap,
-                                                  int all_images, const int* __restrict__ blk_col,
-                                                  const int* __restrict__ col_start, int dcx, int dcy, int* status) {
+                                                  const float4* __restrict__ bb_hi, const int* __restrict__ blk_col,
+                                                  const int* __restrict__ col_start, int dcx, int dcy, int all_images,
+                                                  uint32_t* outer, int* outer_n, int ocap, int* status) {
   if (!*flag) return;
-  __shared__ uint32_t jbuf_all[8][64];
   const int nblk = counters[CNT_SLOTS] >> 5;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int I = blockIdx.x * 8 + warp;
+  const int lane = threadIdx.x & 31;
+  const int I = blockIdx.x * 8 + (threadIdx.x >> 5);
   if (I >= nblk) return;
-  uint32_t* jbuf = jbuf_all[warp];
   const float4 li = bb_lo[I], hi4 = bb_hi[I];
   const float3 ci = make_float3(0.5f * (li.x + hi4.x), 0.5f * (li.y + hi4.y), 0.5f * (li.z + hi4.z));
   const float3 hi = make_float3(0.5f * (hi4.x - li.x), 0.5f * (hi4.y - li.y), 0.5f * (hi4.z - li.z));
   const float rl2 = p.rlist * p.rlist;
-  const uint32_t dummy = (uint32_t)(p.nslots - 1) | ((uint32_t)kNoShift << kSlotBits);
+  uint32_t* out = outer + (size_t)I * ocap;
   int count = 0;
-  // i-lane data for exclusion masks
-  const int ia = perm[I * 32 + lane];
-
-  auto emit = [&](bool diag) {
-    __syncwarp();
-    int t = 0;
-    if (lane == 0) t = atomicAdd(&counters[CNT_TILES], 1);
-    t = __shfl_sync(0xffffffffu, t, 0);
-    if (t >= tile_cap) {
-      if (lane == 0) atomicOr(status, ST_TILE_OVERFLOW);
-      return;
-    }
-    const uint32_t je = jbuf[lane];
-    tile_j[(size_t)t * 32 + lane] = je;
-    // exclusion bits: bit k set when j entry k is an excluded partner of this lane's atom
-    uint32_t mask = 0;
-    if (ia >= 0) {
-      const int e0 = excl_off[ia], e1 = excl_off[ia + 1];
-      for (int e = e0; e < e1; ++e) {
-        const uint32_t se = (uint32_t)inv_perm[excl_idx[e]];
-        for (int k = 0; k < 32; ++k)
-          if ((jbuf[k] & kSlotMask) == se) mask |= 1u << k;
-      }
-    }
-    const unsigned any = __ballot_sync(0xffffffffu, mask != 0);
-    int m = -1;
-    if (any) {
-      if (lane == 0) m = atomicAdd(&counters[CNT_MASKS], 1);
-      m = __shfl_sync(0xffffffffu, m, 0);
-      if (m >= mask_cap) {
-        if (lane == 0) atomicOr(status, ST_MASK_OVERFLOW);
-        m = -1;
-      } else {
-        masks[(size_t)m * 32 + lane] = mask;
-      }
-    }
-    if (lane == 0) {
-      tile_i[t] = I | (diag ? (int)0x80000000 : 0);
-      tile_m[t] = m;
-    }
-    __syncwarp();
-  };
-
   // candidate j blocks: the blocks of the columns within rlist in x-y (periodic column
   // offsets carry the x/y image), each tested in z at its minimum image (or at all three
   // z images for small boxes)
@@ -309,7 +261,8 @@ __global__ void __launch_bounds__(256) k_rb_tiles(SysParams p, const int* __rest
             d.z += sz * p.box.z;
             code = (sx + 1) + 3 * (sy + 1) + 9 * ((int)sz + 1);
             pass = box_gap2(d, make_float3(hi.x + hj.x, hi.y + hj.y, hi.z + hj.z)) < rl2;
-            if (J == I && code > kNoShift) pass = false;  // each +-image pair of the self block once
+            // the self block: its diagonal is implicit, each +-image pair is taken once
+            if (J == I && code >= kNoShift) pass = false;
           }
           unsigned bal = __ballot_sync(0xffffffffu, pass);
           while (bal) {
@@ -317,51 +270,165 @@ __global__ void __launch_bounds__(256) k_rb_tiles(SysParams p, const int* __rest
             bal &= bal - 1;
             const int Jc = J0 + src;
             const int cc = __shfl_sync(0xffffffffu, code, src);
-            if (Jc == I && cc == kNoShift) {
-              // diagonal tile: the whole block on its own (upper triangle in the pair
-              // kernel); pending compacted entries (count < 32) are kept aside
-              const uint32_t save = jbuf[lane];
-              __syncwarp();
-              jbuf[lane] = (uint32_t)(I * 32 + lane) | ((uint32_t)kNoShift << kSlotBits);
-              emit(true);
-              jbuf[lane] = save;
-              __syncwarp();
-              continue;
-            }
             const int s = Jc * 32 + lane;
             const float3 sh = shift_of(cc, p);
             const float4 r = xyzq_s[s];
             const float3 d = make_float3(r.x + sh.x - ci.x, r.y + sh.y - ci.y, r.z + sh.z - ci.z);
             const bool ok = perm[s] >= 0 && box_gap2(d, hi) < rl2;
             const unsigned b2 = __ballot_sync(0xffffffffu, ok);
-            const int pos = __popc(b2 & ((1u << lane) - 1u));
-            if (ok) jbuf[count + pos] = (uint32_t)s | ((uint32_t)cc << kSlotBits);
-            __syncwarp();
+            const int pos = count + __popc(b2 & ((1u << lane) - 1u));
+            if (ok && pos < ocap) out[pos] = (uint32_t)s | ((uint32_t)cc << kSlotBits);
             count += __popc(b2);
-            if (count >= 32) {
-              emit(false);
-              const uint32_t rest = jbuf[32 + lane];
-              __syncwarp();
-              jbuf[lane] = rest;
-              __syncwarp();
-              count -= 32;
-            }
           }
         }
       }
     }
   }
-  if (count > 0) {
-    if (lane >= count) jbuf[lane] = dummy;
-    __syncwarp();
-    emit(false);
+  if (lane == 0) {
+    outer_n[I] = min(count, ocap);
+    if (count > ocap) atomicOr(status, ST_TILE_OVERFLOW);
   }
 }
 
-__global__ void k_rb_end(int* flag, int* counters) {
+__global__ void k_prune_begin(const int* __restrict__ flag_prune, int* counters) {
+  if (!*flag_prune) return;
+  counters[CNT_MASKS] = 0;
+  counters[CNT_TILES] = 0;
+  counters[CNT_ITEMS] = 0;
+}
+
+// exclusion bits of one tile for this lane's i atom: bit k set when j entry k (slot in
+// jb[k]) is an excluded partner (1-2, 1-3, 1-4)
+__device__ __forceinline__ uint32_t excl_bits(int ia, const uint32_t* jb, const int* __restrict__ excl_off,
+                                              const int* __restrict__ excl_idx, const int* __restrict__ inv_perm) {
+  uint32_t mask = 0;
+  if (ia >= 0) {
+    const int e0 = excl_off[ia], e1 = excl_off[ia + 1];
+    for (int e = e0; e < e1; ++e) {
+      const uint32_t se = (uint32_t)inv_perm[excl_idx[e]];
+      for (int k = 0; k < 32; ++k)
+        if ((jb[k] & kSlotMask) == se) mask |= 1u << k;
+    }
+  }
+  return mask;
+}
+
+// Inner (pruned) pair list, warp per i-block: keeps the outer entries that lie within
+// rc + delta of at least one atom of the block at the current positions, packs them
+// into full 32-entry tiles with their exclusion masks, and records the positions the
+// list was made at.  Run after every rebuild and whenever an atom has moved more than
+// delta/2 since the last prune, so no pair within rc is ever missed.
+__global__ void __launch_bounds__(256) k_prune(SysParams p, const int* __restrict__ flag_prune, int* counters,
+                                               const int* __restrict__ perm, const int* __restrict__ inv_perm,
+                                               const float4* __restrict__ xyzq_s, const int* __restrict__ excl_off,
+                                               const int* __restrict__ excl_idx, const uint32_t* __restrict__ outer,
+                                               const int* __restrict__ outer_n, uint32_t* inner, int* inner_nt,
+                                               int* inner_m, uint32_t* masks, uint32_t* dmask, int mask_cap, int ocap,
+                                               float rp2, float4* pos_prune, int2* items, int chunk, int* status) {
+  if (!*flag_prune) return;
+  __shared__ float4 ipos_all[8][32];
+  __shared__ uint32_t buf_all[8][64];
+  const int nblk = counters[CNT_SLOTS] >> 5;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int I = blockIdx.x * 8 + warp;
+  if (I >= nblk) return;
+  float4* ipos = ipos_all[warp];
+  uint32_t* buf = buf_all[warp];
+  const int islot = I * 32 + lane;
+  const float4 pi = xyzq_s[islot];
+  const int ia = perm[islot];
+  if (ia >= 0) pos_prune[ia] = pi;
+  ipos[lane] = pi;
+  // diagonal tile mask (exclusions inside the block)
+  buf[lane] = (uint32_t)islot | ((uint32_t)kNoShift << kSlotBits);
+  __syncwarp();
+  dmask[islot] = excl_bits(ia, buf, excl_off, excl_idx, inv_perm);
+  __syncwarp();
+  const uint32_t dummy = (uint32_t)(p.nslots - 1) | ((uint32_t)kNoShift << kSlotBits);
+  const int n = outer_n[I];
+  const uint32_t* src = outer + (size_t)I * ocap;
+  uint32_t* dst = inner + (size_t)I * ocap;
+  int* mdst = inner_m + (size_t)I * (ocap >> 5);
+  int count = 0, ntile = 0;
+  auto emit = [&]() {
+    const uint32_t je = buf[lane];
+    dst[ntile * 32 + lane] = je;
+    const uint32_t mask = excl_bits(ia, buf, excl_off, excl_idx, inv_perm);
+    int m = -1;
+    if (__ballot_sync(0xffffffffu, mask != 0)) {
+      if (lane == 0) m = atomicAdd(&counters[CNT_MASKS], 1);
+      m = __shfl_sync(0xffffffffu, m, 0);
+      if (m >= mask_cap) {
+        if (lane == 0) atomicOr(status, ST_MASK_OVERFLOW);
+        m = -1;
+      } else {
+        masks[(size_t)m * 32 + lane] = mask;
+      }
+    }
+    if (lane == 0) mdst[ntile] = m;
+    ++ntile;
+    __syncwarp();
+  };
+  for (int c0 = 0; c0 < n; c0 += 32) {
+    const bool valid = c0 + lane < n;
+    const uint32_t e = valid ? src[c0 + lane] : dummy;
+    float4 r = xyzq_s[e & kSlotMask];
+    const int code = (int)(e >> kSlotBits);
+    if (code != kNoShift) {
+      const float3 sh = shift_of(code, p);
+      r.x += sh.x;
+      r.y += sh.y;
+      r.z += sh.z;
+    }
+    float m2 = 3e38f;
+#pragma unroll 8
+    for (int k = 0; k < 32; ++k) {
+      const float4 q = ipos[k];
+      const float dx = r.x - q.x, dy = r.y - q.y, dz = r.z - q.z;
+      m2 = fminf(m2, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+    }
+    const bool keep = valid && m2 < rp2;
+    const unsigned b = __ballot_sync(0xffffffffu, keep);
+    if (keep) buf[count + __popc(b & ((1u << lane) - 1u))] = e;
+    __syncwarp();
+    count += __popc(b);
+    if (count >= 32) {
+      emit();
+      const uint32_t rest = buf[32 + lane];
+      __syncwarp();
+      buf[lane] = rest;
+      __syncwarp();
+      count -= 32;
+    }
+  }
+  if (count > 0) {
+    if (lane >= count) buf[lane] = dummy;
+    __syncwarp();
+    emit();
+  }
+  // work items for the pair kernel: chunks of <= `chunk` tiles (tile 0 is the diagonal)
+  const int nitems = (ntile + 1 + chunk - 1) / chunk;
+  int base = 0;
+  if (lane == 0) {
+    inner_nt[I] = ntile;
+    atomicAdd(&counters[CNT_TILES], ntile + 1);
+    base = atomicAdd(&counters[CNT_ITEMS], nitems);
+  }
+  base = __shfl_sync(0xffffffffu, base, 0);
+  for (int k = lane; k < nitems; k += 32) items[base + k] = make_int2(I, k * chunk);
+}
+
+__global__ void k_prune_end(int* flag_prune, int* counters) {
+  if (!*flag_prune) return;
+  counters[CNT_PRUNES] += 1;
+  *flag_prune = 0;
+}
+
+__global__ void k_rb_end(int* flag, int* flag_prune, int* counters) {
   if (!*flag) return;
   counters[CNT_REBUILDS] += 1;
   *flag = 0;
+  *flag_prune = 1;  // a new outer list always gets a fresh inner list
 }
 
 // ------------------------------------------------------------------ launchers
@@ -377,11 +444,16 @@ void launch_rebuild(const RebuildArgs& a, cudaStream_t st) {
       a.blk_col, a.status);
   const int maxblk = (p.nslots) / 32;
   k_rb_bbox<<<(maxblk * 32 + 255) / 256, 256, 0, st>>>(p, a.flag, a.counters, a.perm, a.xyzq_s, a.bb_lo, a.bb_hi);
-  k_rb_tiles<<<(maxblk + 7) / 8, 256, 0, st>>>(p, a.flag, a.counters, a.perm, a.inv_perm, a.xyzq_s, a.bb_lo, a.bb_hi,
-                                               a.excl_off, a.excl_idx, a.tile_i, a.tile_j, a.tile_m, a.masks,
-                                               a.tile_cap, a.mask_cap, a.all_images, a.blk_col, a.col_start, a.dcx,
-                                               a.dcy, a.status);
-  k_rb_end<<<1, 1, 0, st>>>(a.flag, a.counters);
+  k_rb_outer<<<(maxblk + 7) / 8, 256, 0, st>>>(p, a.flag, a.counters, a.perm, a.xyzq_s, a.bb_lo, a.bb_hi, a.blk_col,
+                                               a.col_start, a.dcx, a.dcy, a.all_images, a.outer, a.outer_n, a.ocap,
+                                               a.status);
+  k_rb_end<<<1, 1, 0, st>>>(a.flag, a.flag_prune, a.counters);
+  k_prune_begin<<<1, 1, 0, st>>>(a.flag_prune, a.counters);
+  k_prune<<<(maxblk + 7) / 8, 256, 0, st>>>(p, a.flag_prune, a.counters, a.perm, a.inv_perm, a.xyzq_s, a.excl_off,
+                                            a.excl_idx, a.outer, a.outer_n, a.inner, a.inner_nt, a.inner_m, a.masks,
+                                            a.dmask, a.mask_cap, a.ocap, a.rp2, a.pos_prune, a.items, a.chunk,
+                                            a.status);
+  k_prune_end<<<1, 1, 0, st>>>(a.flag_prune, a.counters);
 }
 
 }  // namespace fzk

@@ -89,103 +89,132 @@ __device__ __forceinline__ float pair_force(const PairConst& c, float r2, float 
   return ok ? fr : 0.f;
 }
 
+// One 32 x 32 tile: j data (image shift applied) staged in this warp's shared ring,
+// i force accumulated in registers, j force rotated and flushed at the end.
+template <bool ENERGY>
+__device__ __forceinline__ void run_tile(const PairConst& c, const SysParams& p, const float4& xi, float qi,
+                                         const float2* ljrow, uint32_t je, uint32_t excl, float4* jx, int* jt,
+                                         const float4* __restrict__ xyzq, const int* __restrict__ typ,
+                                         const int* __restrict__ perm, long long* __restrict__ facc, int lane,
+                                         int src, float& fix, float& fiy, float& fiz, float& ev, float& ee) {
+  const int jslot = (int)(je & kSlotMask);
+  const int code = (int)(je >> kSlotBits);
+  float4 xj = xyzq[jslot];
+  if (code != kNoShift) {
+    const float3 s = shift_of(code, p);
+    xj.x += s.x;
+    xj.y += s.y;
+    xj.z += s.z;
+  }
+  const int tyj = typ[jslot];
+  __syncwarp();
+  jx[lane] = xj;
+  jx[lane + 32] = xj;
+  jt[lane] = tyj;
+  jt[lane + 32] = tyj;
+  __syncwarp();
+  // bit k of mrot: pair (lane, lane + k) excluded
+  const uint32_t mrot = __funnelshift_r(excl, excl, lane);
+  const float4* jxl = jx + lane;
+  const int* jtl = jt + lane;
+  float fjx = 0.f, fjy = 0.f, fjz = 0.f;
+  if (__any_sync(0xffffffffu, mrot != 0u)) {
+#pragma unroll 8
+    for (int k = 0; k < 32; ++k) {
+      const float4 b = jxl[k];
+      const float dx = xi.x - b.x, dy = xi.y - b.y, dz = xi.z - b.z;
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      const bool ok = (r2 < c.rc2) && !((mrot >> k) & 1u);
+      const float fr = pair_force<ENERGY>(c, r2, qi * b.w, ljrow[jtl[k]], ok, ev, ee);
+      fix = fmaf(fr, dx, fix);
+      fiy = fmaf(fr, dy, fiy);
+      fiz = fmaf(fr, dz, fiz);
+      fjx = __shfl_sync(0xffffffffu, fmaf(-fr, dx, fjx), src);
+      fjy = __shfl_sync(0xffffffffu, fmaf(-fr, dy, fjy), src);
+      fjz = __shfl_sync(0xffffffffu, fmaf(-fr, dz, fjz), src);
+    }
+  } else {
+#pragma unroll 8
+    for (int k = 0; k < 32; ++k) {
+      const float4 b = jxl[k];
+      const float dx = xi.x - b.x, dy = xi.y - b.y, dz = xi.z - b.z;
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      const float fr = pair_force<ENERGY>(c, r2, qi * b.w, ljrow[jtl[k]], r2 < c.rc2, ev, ee);
+      fix = fmaf(fr, dx, fix);
+      fiy = fmaf(fr, dy, fiy);
+      fiz = fmaf(fr, dz, fiz);
+      fjx = __shfl_sync(0xffffffffu, fmaf(-fr, dx, fjx), src);
+      fjy = __shfl_sync(0xffffffffu, fmaf(-fr, dy, fjy), src);
+      fjz = __shfl_sync(0xffffffffu, fmaf(-fr, dz, fjz), src);
+    }
+  }
+  const int aj = perm[jslot];
+  if (aj >= 0) {
+    const int n = p.n;
+    red_add(facc + aj, to_fix(fjx));
+    red_add(facc + n + aj, to_fix(fjy));
+    red_add(facc + 2 * n + aj, to_fix(fjz));
+  }
+}
+
+// Warp per i-block (blocks taken from a dynamic counter): the diagonal tile, then the
+// block's inner tiles; the i force stays in registers across tiles and is flushed once.
 template <bool ENERGY>
 __global__ void __launch_bounds__(256, 3)
     k_nonbonded(SysParams p, PairConst c, const float4* __restrict__ xyzq, const int* __restrict__ typ,
-                const int* __restrict__ perm, const int* __restrict__ tile_i, const uint32_t* __restrict__ tile_j,
-                const int* __restrict__ tile_m, const uint32_t* __restrict__ masks, const int* __restrict__ counters,
-                const float2* __restrict__ ljtab, long long* __restrict__ facc, long long* __restrict__ energy,
-                int tile_cap) {
+                const int* __restrict__ perm, const uint32_t* __restrict__ inner, const int* __restrict__ inner_nt,
+                const int* __restrict__ inner_m, const uint32_t* __restrict__ dmask,
+                const uint32_t* __restrict__ masks, int* __restrict__ counters, const int2* __restrict__ items,
+                int chunk, const float2* __restrict__ ljtab, long long* __restrict__ facc,
+                long long* __restrict__ energy, int ocap) {
   extern __shared__ float2 lj[];
   __shared__ float4 jx_all[kWarps][64];
   __shared__ int jt_all[kWarps][64];
   const int nt1 = p.ntypes + 1;
   for (int k = threadIdx.x; k < nt1 * nt1; k += blockDim.x) lj[k] = ljtab[k];
   __syncthreads();
-  const int ntiles = min(counters[CNT_TILES], tile_cap);
+  const int nitems = counters[CNT_ITEMS];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float4* jx = jx_all[warp];
   int* jt = jt_all[warp];
-  const int nwarps = gridDim.x * kWarps;
   const int n = p.n;
   const int src = (lane + 1) & 31;
   double e_vdw = 0.0, e_el = 0.0;
-  for (int t = blockIdx.x * kWarps + warp; t < ntiles; t += nwarps) {
-    const int ti = tile_i[t];
-    const bool diag = ti < 0;
-    const int I = ti & 0x7fffffff;
+  for (;;) {
+    int it = 0;
+    if (lane == 0) it = atomicAdd(&counters[CNT_WORK], 1);
+    it = __shfl_sync(0xffffffffu, it, 0);
+    if (it >= nitems) break;
+    const int2 item = items[it];
+    const int I = item.x;
     const int islot = I * 32 + lane;
     const float4 xi = xyzq[islot];
     const float2* ljrow = lj + typ[islot] * nt1;
     const float qi = xi.w * p.cc;
-    const uint32_t je = tile_j[(size_t)t * 32 + lane];
-    const int jslot = (int)(je & kSlotMask);
-    const int code = (int)(je >> kSlotBits);
-    float4 xj = xyzq[jslot];
-    if (code != kNoShift) {
-      const float3 s = shift_of(code, p);
-      xj.x += s.x;
-      xj.y += s.y;
-      xj.z += s.z;
-    }
-    const int tyj = typ[jslot];
-    __syncwarp();
-    jx[lane] = xj;
-    jx[lane + 32] = xj;
-    jt[lane] = tyj;
-    jt[lane + 32] = tyj;
-    const int m = tile_m[t];
-    uint32_t excl = m >= 0 ? masks[(size_t)m * 32 + lane] : 0u;
-    if (diag) excl |= (lane == 31) ? 0xffffffffu : ((2u << lane) - 1u);  // j <= i
-    __syncwarp();
-    // bit k of mrot: pair (lane, lane + k) excluded
-    const uint32_t mrot = __funnelshift_r(excl, excl, lane);
-    const float4* jxl = jx + lane;
-    const int* jtl = jt + lane;
     float fix = 0.f, fiy = 0.f, fiz = 0.f;
-    float fjx = 0.f, fjy = 0.f, fjz = 0.f;
     float ev = 0.f, ee = 0.f;
-    if (__any_sync(0xffffffffu, mrot != 0u)) {
-#pragma unroll 8
-      for (int k = 0; k < 32; ++k) {
-        const float4 b = jxl[k];
-        const float dx = xi.x - b.x, dy = xi.y - b.y, dz = xi.z - b.z;
-        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        const bool ok = (r2 < c.rc2) && !((mrot >> k) & 1u);
-        const float fr = pair_force<ENERGY>(c, r2, qi * b.w, ljrow[jtl[k]], ok, ev, ee);
-        fix = fmaf(fr, dx, fix);
-        fiy = fmaf(fr, dy, fiy);
-        fiz = fmaf(fr, dz, fiz);
-        fjx = __shfl_sync(0xffffffffu, fmaf(-fr, dx, fjx), src);
-        fjy = __shfl_sync(0xffffffffu, fmaf(-fr, dy, fjy), src);
-        fjz = __shfl_sync(0xffffffffu, fmaf(-fr, dz, fjz), src);
-      }
-    } else {
-#pragma unroll 8
-      for (int k = 0; k < 32; ++k) {
-        const float4 b = jxl[k];
-        const float dx = xi.x - b.x, dy = xi.y - b.y, dz = xi.z - b.z;
-        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        const float fr = pair_force<ENERGY>(c, r2, qi * b.w, ljrow[jtl[k]], r2 < c.rc2, ev, ee);
-        fix = fmaf(fr, dx, fix);
-        fiy = fmaf(fr, dy, fiy);
-        fiz = fmaf(fr, dz, fiz);
-        fjx = __shfl_sync(0xffffffffu, fmaf(-fr, dx, fjx), src);
-        fjy = __shfl_sync(0xffffffffu, fmaf(-fr, dy, fjy), src);
-        fjz = __shfl_sync(0xffffffffu, fmaf(-fr, dz, fjz), src);
-      }
+    // tile 0 of a block is the diagonal (the block with itself, upper triangle j > i)
+    int t = item.y;
+    const int tend = min(inner_nt[I] + 1, t + chunk);
+    if (t == 0) {
+      const uint32_t tri = (lane == 31) ? 0xffffffffu : ((2u << lane) - 1u);
+      run_tile<ENERGY>(c, p, xi, qi, ljrow, (uint32_t)islot | ((uint32_t)kNoShift << kSlotBits),
+                       dmask[islot] | tri, jx, jt, xyzq, typ, perm, facc, lane, src, fix, fiy, fiz, ev, ee);
+      t = 1;
+    }
+    const uint32_t* jl = inner + (size_t)I * ocap - 32;  // inner tile t-1
+    const int* ml = inner_m + (size_t)I * (ocap >> 5) - 1;
+    for (; t < tend; ++t) {
+      const int m = ml[t];
+      const uint32_t excl = m >= 0 ? masks[(size_t)m * 32 + lane] : 0u;
+      run_tile<ENERGY>(c, p, xi, qi, ljrow, jl[t * 32 + lane], excl, jx, jt, xyzq, typ, perm, facc, lane, src, fix,
+                       fiy, fiz, ev, ee);
     }
     const int ai = perm[islot];
     if (ai >= 0) {
       red_add(facc + ai, to_fix(fix));
       red_add(facc + n + ai, to_fix(fiy));
       red_add(facc + 2 * n + ai, to_fix(fiz));
-    }
-    const int aj = perm[jslot];
-    if (aj >= 0) {
-      red_add(facc + aj, to_fix(fjx));
-      red_add(facc + n + aj, to_fix(fjy));
-      red_add(facc + 2 * n + aj, to_fix(fjz));
     }
     if (ENERGY) {
       e_vdw += (double)ev;
@@ -211,14 +240,15 @@ void launch_nonbonded(const NonbondedArgs& a, bool energy, cudaStream_t st) {
   c.sw_a = d > 0.f ? 1.f / d : 0.f;
   c.sw_b = d > 0.f ? -a.p.ron2 / d : 0.f;
   c.dsw_k = d > 0.f ? 12.f / d : 0.f;
+  cudaMemsetAsync(a.counters + CNT_WORK, 0, sizeof(int), st);
   if (energy)
-    k_nonbonded<true><<<a.grid, kWarps * 32, smem, st>>>(a.p, c, a.xyzq_s, a.typ_s, a.perm, a.tile_i, a.tile_j,
-                                                          a.tile_m, a.masks, a.counters, a.ljtab, a.facc, a.energy,
-                                                          a.tile_cap);
+    k_nonbonded<true><<<a.grid, kWarps * 32, smem, st>>>(a.p, c, a.xyzq_s, a.typ_s, a.perm, a.inner, a.inner_nt,
+                                                          a.inner_m, a.dmask, a.masks, a.counters, a.items, a.chunk,
+                                                          a.ljtab, a.facc, a.energy, a.ocap);
   else
-    k_nonbonded<false><<<a.grid, kWarps * 32, smem, st>>>(a.p, c, a.xyzq_s, a.typ_s, a.perm, a.tile_i, a.tile_j,
-                                                           a.tile_m, a.masks, a.counters, a.ljtab, a.facc, a.energy,
-                                                           a.tile_cap);
+    k_nonbonded<false><<<a.grid, kWarps * 32, smem, st>>>(a.p, c, a.xyzq_s, a.typ_s, a.perm, a.inner, a.inner_nt,
+                                                           a.inner_m, a.dmask, a.masks, a.counters, a.items, a.chunk,
+                                                           a.ljtab, a.facc, a.energy, a.ocap);
 }
 
 }  // namespace fzk

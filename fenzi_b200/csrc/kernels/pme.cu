@@ -119,7 +119,21 @@ __global__ void k_pme_scatter(PmeArgs a) {
 // stay far below the +-128 e range a grid point could hold), native shared atomics
 constexpr float kFixQ32 = 16777216.0f;
 
-__global__ void __launch_bounds__(128) k_pme_spread(PmeArgs a) {
+// cubic B-spline weight M4(t + j) (j = 0..3, t in [0,1))
+__device__ __forceinline__ float bsp4_w(float t, int j) {
+  const float t2 = t * t, t3 = t2 * t, u = 1.f - t;
+  const float s = 1.f / 6.f;
+  const float w0 = t3 * s;
+  const float w1 = fmaf(-3.f, t3, fmaf(3.f, t2, fmaf(3.f, t, 1.f))) * s;
+  const float w2 = fmaf(3.f, t3, fmaf(-6.f, t2, 4.f)) * s;
+  const float w3 = u * u * u * s;
+  return j == 0 ? w0 : (j == 1 ? w1 : (j == 2 ? w2 : w3));
+}
+
+// One CTA per brick; each warp takes one candidate atom at a time and its 32 lanes
+// cover 32 of the atom's 64 stencil points (two passes), so a warp's shared atomics
+// never collide with each other.
+__global__ void __launch_bounds__(256) k_pme_spread(PmeArgs a) {
   extern __shared__ int acc[];
   const int Bx = a.B[0], By = a.B[1], Bz = a.B[2];
   const int nbx = a.nb[0], nby = a.nb[1], nbz = a.nb[2];
@@ -131,49 +145,32 @@ __global__ void __launch_bounds__(128) k_pme_spread(PmeArgs a) {
   const int Kx = a.K[0], Ky = a.K[1], Kz = a.K[2];
   const int ox = bx * Bx, oy = by * By, oz = bz * Bz;
   const int sdx = nbx > 1 ? 2 : 1, sdy = nby > 1 ? 2 : 1, sdz = nbz > 1 ? 2 : 1;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int jx = lane & 3, jy = (lane >> 2) & 3, jz0 = lane >> 4;  // jz = jz0 and jz0 + 2
   for (int dz = 0; dz < sdz; ++dz)
     for (int dy = 0; dy < sdy; ++dy)
       for (int dx = 0; dx < sdx; ++dx) {
         const int sb = (((bz + dz) % nbz) * nby + (by + dy) % nby) * nbx + (bx + dx) % nbx;
         const int s0 = a.brick_start[sb], s1 = a.brick_start[sb + 1];
-        for (int idx = s0 + threadIdx.x; idx < s1; idx += blockDim.x) {
+        for (int idx = s0 + warp; idx < s1; idx += nw) {
           const int i = a.brick_atoms[idx];
           const float4 r = a.pos4[i];
-          float tx, ty, tz, wx[4], wy[4], wz[4];
+          float tx, ty, tz;
           const int kx = grid_base(r.x, a.p.inv_box.x, Kx, &tx);
           const int ky = grid_base(r.y, a.p.inv_box.y, Ky, &ty);
           const int kz = grid_base(r.z, a.p.inv_box.z, Kz, &tz);
-          bsp4(tx, wx, nullptr);
-          bsp4(ty, wy, nullptr);
-          bsp4(tz, wz, nullptr);
-          const float q = r.w;
-          // local offsets of grid points k0 - j inside this brick (k0 - j - o lies in
-          // (-K, K) so one conditional wrap suffices); >= B means another brick owns it
-          int lxs[4], lys[4], lzs[4];
+          // local offsets of grid point k0 - j in this brick; k0 - j - o lies in (-K, K)
+          int lx = kx - jx - ox, ly = ky - jy - oy;
+          lx += lx < 0 ? Kx : 0;
+          ly += ly < 0 ? Ky : 0;
+          const float qxy = r.w * bsp4_w(tx, jx) * bsp4_w(ty, jy);
 #pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            int vx = kx - j - ox, vy = ky - j - oy, vz = kz - j - oz;
-            vx += vx < 0 ? Kx : 0;
-            vy += vy < 0 ? Ky : 0;
-            vz += vz < 0 ? Kz : 0;
-            lxs[j] = vx;
-            lys[j] = vy;
-            lzs[j] = vz;
-          }
-#pragma unroll
-          for (int jz = 0; jz < 4; ++jz) {
-            if (lzs[jz] >= Bz) continue;
-#pragma unroll
-            for (int jy = 0; jy < 4; ++jy) {
-              if (lys[jy] >= By) continue;
-              const float qzy = q * wz[jz] * wy[jy];
-              int* rowp = &acc[(lzs[jz] * By + lys[jy]) * Bx];
-#pragma unroll
-              for (int jx = 0; jx < 4; ++jx) {
-                if (lxs[jx] >= Bx) continue;
-                atomicAdd(rowp + lxs[jx], __float2int_rn(qzy * wx[jx] * kFixQ32));
-              }
-            }
+          for (int h = 0; h < 2; ++h) {
+            const int jz = jz0 + 2 * h;
+            int lz = kz - jz - oz;
+            lz += lz < 0 ? Kz : 0;
+            if (lx < Bx && ly < By && lz < Bz)
+              atomicAdd(&acc[(lz * By + ly) * Bx + lx], __float2int_rn(qxy * bsp4_w(tz, jz) * kFixQ32));
           }
         }
       }
@@ -442,6 +439,278 @@ __global__ void __launch_bounds__(256) k_pme_gather(PmeArgs a) {
   red_add(a.facc + 2 * n + i, to_fix(-q * gz * (float)Kz * a.p.inv_box.z));
 }
 
+// ------------------------------------------------------------------ compile-time FFT
+// The same Stockham autosort algorithm with the line length N a template parameter:
+// radices, strides and twiddle steps are constants, the small DFTs use constant roots.
+__host__ __device__ constexpr int radix_of(int m) { return m % 4 == 0 ? 4 : (m % 2 == 0 ? 2 : (m % 3 == 0 ? 3 : 5)); }
+__host__ __device__ constexpr int radix_at(int n, int s) {
+  int m = n, r = 1;
+  for (int k = 0; k <= s; ++k) {
+    r = radix_of(m);
+    m /= r;
+  }
+  return r;
+}
+__host__ __device__ constexpr int nstages(int n) {
+  int m = n, c = 0;
+  while (m > 1) {
+    m /= radix_of(m);
+    ++c;
+  }
+  return c;
+}
+
+template <int R, bool INV>
+__device__ __forceinline__ void small_dft(float2* v) {
+  const float sg = INV ? 1.f : -1.f;  // exponent sign
+  if constexpr (R == 2) {
+    const float2 a = v[0], b = v[1];
+    v[0] = make_float2(a.x + b.x, a.y + b.y);
+    v[1] = make_float2(a.x - b.x, a.y - b.y);
+  } else if constexpr (R == 4) {
+    const float2 a0 = make_float2(v[0].x + v[2].x, v[0].y + v[2].y);
+    const float2 a1 = make_float2(v[0].x - v[2].x, v[0].y - v[2].y);
+    const float2 b0 = make_float2(v[1].x + v[3].x, v[1].y + v[3].y);
+    const float2 b1 = make_float2(v[1].x - v[3].x, v[1].y - v[3].y);
+    // sg * i * b1 = (-sg b1.y, sg b1.x)
+    v[0] = make_float2(a0.x + b0.x, a0.y + b0.y);
+    v[2] = make_float2(a0.x - b0.x, a0.y - b0.y);
+    v[1] = make_float2(a1.x - sg * b1.y, a1.y + sg * b1.x);
+    v[3] = make_float2(a1.x + sg * b1.y, a1.y - sg * b1.x);
+  } else if constexpr (R == 3) {
+    const float c1 = -0.5f, s1 = sg * 0.86602540378443865f;  // e^{sg 2 pi i/3}
+    const float2 t = make_float2(v[1].x + v[2].x, v[1].y + v[2].y);
+    const float2 d = make_float2(v[1].x - v[2].x, v[1].y - v[2].y);
+    const float2 m = make_float2(v[0].x + c1 * t.x, v[0].y + c1 * t.y);
+    v[0] = make_float2(v[0].x + t.x, v[0].y + t.y);
+    v[1] = make_float2(m.x - s1 * d.y, m.y + s1 * d.x);
+    v[2] = make_float2(m.x + s1 * d.y, m.y - s1 * d.x);
+  } else {  // R == 5
+    const float c1 = 0.30901699437494742f, c2 = -0.80901699437494742f;
+    const float s1 = sg * 0.95105651629515357f, s2 = sg * 0.58778525229247313f;
+    const float2 t1 = make_float2(v[1].x + v[4].x, v[1].y + v[4].y);
+    const float2 d1 = make_float2(v[1].x - v[4].x, v[1].y - v[4].y);
+    const float2 t2 = make_float2(v[2].x + v[3].x, v[2].y + v[3].y);
+    const float2 d2 = make_float2(v[2].x - v[3].x, v[2].y - v[3].y);
+    const float2 m1 = make_float2(v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y);
+    const float2 m2 = make_float2(v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y);
+    const float2 n1 = make_float2(s1 * d1.x + s2 * d2.x, s1 * d1.y + s2 * d2.y);
+    const float2 n2 = make_float2(s2 * d1.x - s1 * d2.x, s2 * d1.y - s1 * d2.y);
+    v[0] = make_float2(v[0].x + t1.x + t2.x, v[0].y + t1.y + t2.y);
+    v[1] = make_float2(m1.x - n1.y, m1.y + n1.x);
+    v[4] = make_float2(m1.x + n1.y, m1.y - n1.x);
+    v[2] = make_float2(m2.x - n2.y, m2.y + n2.x);
+    v[3] = make_float2(m2.x + n2.y, m2.y - n2.x);
+  }
+}
+
+template <int N, int R, int NS, bool INV>
+__device__ __forceinline__ void fft_stage_t(const float2* x, float2* y, const float2* tw, int nl) {
+  constexpr int NB = N / R, STEP = N / (NS * R), LD = N + 1;
+  for (int idx = threadIdx.x; idx < nl * NB; idx += blockDim.x) {
+    const int l = idx / NB, j = idx - l * NB;
+    const int k = j % NS;
+    const float2* xl = x + l * LD;
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = xl[j + r * NB];
+    if constexpr (NS > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        float2 w = tw[r * k * STEP];
+        if (INV) w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+    }
+    small_dft<R, INV>(v);
+    float2* yl = y + l * LD;
+    const int o = (j / NS) * NS * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) yl[o + r * NS] = v[r];
+  }
+}
+
+template <int N, int S, int NS, bool INV>
+__device__ __forceinline__ float2* fft_run_t(float2* a, float2* b, const float2* tw, int nl) {
+  if constexpr (S == nstages(N)) {
+    return a;
+  } else {
+    constexpr int R = radix_at(N, S);
+    fft_stage_t<N, R, NS, INV>(a, b, tw, nl);
+    __syncthreads();
+    return fft_run_t<N, S + 1, NS * R, INV>(b, a, tw, nl);
+  }
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) k_fft_x_r2c_t(PmeArgs a, int nl) {
+  extern __shared__ float2 sm[];
+  constexpr int LD = N + 1, NH = N / 2 + 1;
+  const int nrows = a.K[1] * a.K[2];
+  float2* tw = sm;
+  float2* A = sm + N;
+  float2* B = A + nl * LD;
+  load_tw(tw, a.tw[0], N);
+  const int r0 = blockIdx.x * nl;
+  for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) {
+    const int l = idx / N, x = idx - l * N;
+    const int row = r0 + l;
+    A[l * LD + x] = make_float2(row < nrows ? a.grid[(size_t)row * N + x] : 0.f, 0.f);
+  }
+  __syncthreads();
+  const float2* R = fft_run_t<N, 0, 1, false>(A, B, tw, nl);
+  for (int idx = threadIdx.x; idx < nl * NH; idx += blockDim.x) {
+    const int l = idx / NH, m = idx - l * NH;
+    const int row = r0 + l;
+    if (row < nrows) a.cgrid[(size_t)row * NH + m] = R[l * LD + m];
+  }
+}
+
+template <int N, bool INV>
+__global__ void __launch_bounds__(256) k_fft_y_t(PmeArgs a, int nl) {
+  extern __shared__ float2 sm[];
+  constexpr int LD = N + 1;
+  const int Kxh = a.K[0] / 2 + 1;
+  const int ng = (Kxh + nl - 1) / nl;
+  const int z = blockIdx.x / ng, mx0 = (blockIdx.x % ng) * nl;
+  float2* tw = sm;
+  float2* A = sm + N;
+  float2* B = A + nl * LD;
+  load_tw(tw, a.tw[1], N);
+  for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) {
+    const int y = idx / nl, l = idx - y * nl;
+    const int mx = mx0 + l;
+    A[l * LD + y] = mx < Kxh ? a.cgrid[((size_t)z * N + y) * Kxh + mx] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  const float2* R = fft_run_t<N, 0, 1, INV>(A, B, tw, nl);
+  for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) {
+    const int y = idx / nl, l = idx - y * nl;
+    const int mx = mx0 + l;
+    if (mx < Kxh) a.cgrid[((size_t)z * N + y) * Kxh + mx] = R[l * LD + y];
+  }
+}
+
+template <int N, bool ENERGY>
+__global__ void __launch_bounds__(256) k_fft_z_conv_t(PmeArgs a, int nl) {
+  extern __shared__ float2 sm[];
+  constexpr int LD = N + 1;
+  const int Kx = a.K[0], Ky = a.K[1], Kxh = Kx / 2 + 1;
+  const int ng = (Kxh + nl - 1) / nl;
+  const int y = blockIdx.x / ng, mx0 = (blockIdx.x % ng) * nl;
+  float2* tw = sm;
+  float2* A = sm + N;
+  float2* B = A + nl * LD;
+  load_tw(tw, a.tw[2], N);
+  for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) {
+    const int z = idx / nl, l = idx - z * nl;
+    const int mx = mx0 + l;
+    A[l * LD + z] = mx < Kxh ? a.cgrid[((size_t)z * Ky + y) * Kxh + mx] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  float2* R = fft_run_t<N, 0, 1, false>(A, B, tw, nl);
+  float2* O = (R == A) ? B : A;
+  double e = 0.0;
+  const float gy = a.gfac[1][y], fy2 = a.f2[1][y];
+  for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) {
+    const int l = idx / N, z = idx - l * N;
+    const int mx = mx0 + l;
+    float2 v = R[l * LD + z];
+    float G = 0.f;
+    if (mx < Kxh && (mx | y | z) != 0) G = a.gscale * a.gfac[0][mx] * gy * a.gfac[2][z] / (a.f2[0][mx] + fy2 + a.f2[2][z]);
+    if (ENERGY && mx < Kxh) {
+      const double wmx = (mx == 0 || (2 * mx == Kx)) ? 1.0 : 2.0;
+      e += wmx * 0.5 * (double)G * ((double)v.x * v.x + (double)v.y * v.y);
+    }
+    v.x *= G;
+    v.y *= G;
+    R[l * LD + z] = v;
+  }
+  __syncthreads();
+  const float2* Q = fft_run_t<N, 0, 1, true>(R, O, tw, nl);
+  for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) {
+    const int z = idx / nl, l = idx - z * nl;
+    const int mx = mx0 + l;
+    if (mx < Kxh) a.cgrid[((size_t)z * Ky + y) * Kxh + mx] = Q[l * LD + z];
+  }
+  if (ENERGY) energy_add(a.energy + EN_PME, e);
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) k_fft_x_c2r_t(PmeArgs a, int nl) {
+  extern __shared__ float2 sm[];
+  constexpr int LD = N + 1, NH = N / 2 + 1;
+  const int nrows = a.K[1] * a.K[2];
+  float2* tw = sm;
+  float2* A = sm + N;
+  float2* B = A + nl * LD;
+  load_tw(tw, a.tw[0], N);
+  const int r0 = blockIdx.x * nl;
+  for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) {
+    const int l = idx / N, m = idx - l * N;
+    const int row = r0 + l;
+    float2 v = make_float2(0.f, 0.f);
+    if (row < nrows) {
+      if (m < NH) v = a.cgrid[(size_t)row * NH + m];
+      else {
+        v = a.cgrid[(size_t)row * NH + (N - m)];
+        v.y = -v.y;
+      }
+    }
+    A[l * LD + m] = v;
+  }
+  __syncthreads();
+  const float2* R = fft_run_t<N, 0, 1, true>(A, B, tw, nl);
+  for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) {
+    const int l = idx / N, x = idx - l * N;
+    const int row = r0 + l;
+    if (row < nrows) a.grid[(size_t)row * N + x] = R[l * LD + x].x;
+  }
+}
+
+#define FZ_FFT_SIZES(X) X(16) X(18) X(20) X(24) X(25) X(27) X(30) X(32) X(36) X(40) X(48) X(64) X(80) X(96) X(128)
+
+static bool fft_x_r2c_t(const PmeArgs& a, int nl, dim3 g, size_t sm, cudaStream_t st) {
+  switch (a.K[0]) {
+#define FZ_C(N) case N: k_fft_x_r2c_t<N><<<g, 256, sm, st>>>(a, nl); return true;
+    FZ_FFT_SIZES(FZ_C)
+#undef FZ_C
+  }
+  return false;
+}
+static bool fft_y_t(const PmeArgs& a, int nl, bool inv, dim3 g, size_t sm, cudaStream_t st) {
+  switch (a.K[1]) {
+#define FZ_C(N)                                                   \
+  case N:                                                         \
+    if (inv) k_fft_y_t<N, true><<<g, 256, sm, st>>>(a, nl);        \
+    else k_fft_y_t<N, false><<<g, 256, sm, st>>>(a, nl);           \
+    return true;
+    FZ_FFT_SIZES(FZ_C)
+#undef FZ_C
+  }
+  return false;
+}
+static bool fft_z_t(const PmeArgs& a, int nl, bool energy, dim3 g, size_t sm, cudaStream_t st) {
+  switch (a.K[2]) {
+#define FZ_C(N)                                                      \
+  case N:                                                            \
+    if (energy) k_fft_z_conv_t<N, true><<<g, 256, sm, st>>>(a, nl);   \
+    else k_fft_z_conv_t<N, false><<<g, 256, sm, st>>>(a, nl);         \
+    return true;
+    FZ_FFT_SIZES(FZ_C)
+#undef FZ_C
+  }
+  return false;
+}
+static bool fft_x_c2r_t(const PmeArgs& a, int nl, dim3 g, size_t sm, cudaStream_t st) {
+  switch (a.K[0]) {
+#define FZ_C(N) case N: k_fft_x_c2r_t<N><<<g, 256, sm, st>>>(a, nl); return true;
+    FZ_FFT_SIZES(FZ_C)
+#undef FZ_C
+  }
+  return false;
+}
+
 static FftPlan make_plan(int n) {
   FftPlan p{};
   p.n = n;
@@ -462,7 +731,7 @@ void launch_pme(const PmeArgs& a, bool energy, cudaStream_t st) {
   k_pme_scan<<<1, 1024, 0, st>>>(a, nbr);
   k_pme_scatter<<<(a.n + 255) / 256, 256, 0, st>>>(a);
   const size_t sp = (size_t)a.B[0] * a.B[1] * a.B[2] * sizeof(int);
-  k_pme_spread<<<nbr, 128, sp, st>>>(a);
+  k_pme_spread<<<nbr, 256, sp, st>>>(a);
   const int Kx = a.K[0], Ky = a.K[1], Kz = a.K[2], Kxh = Kx / 2 + 1;
   const FftPlan px = make_plan(Kx), py = make_plan(Ky), pz = make_plan(Kz);
   const int lx = lines_for(Kx), ly = lines_for(Ky), lz = lines_for(Kz);
@@ -470,14 +739,18 @@ void launch_pme(const PmeArgs& a, bool energy, cudaStream_t st) {
   const size_t smx = (size_t)(Kx + 2 * lx * (Kx + 1)) * sizeof(float2);
   const size_t smy = (size_t)(Ky + 2 * ly * (Ky + 1)) * sizeof(float2);
   const size_t smz = (size_t)(Kz + 2 * lz * (Kz + 1)) * sizeof(float2);
-  k_fft_x_r2c<<<(rows + lx - 1) / lx, 256, smx, st>>>(a, px, lx);
-  k_fft_y<<<Kz * ((Kxh + ly - 1) / ly), 256, smy, st>>>(a, py, ly, 0);
-  if (energy)
-    k_fft_z_conv<true><<<Ky * ((Kxh + lz - 1) / lz), 256, smz, st>>>(a, pz, lz);
-  else
-    k_fft_z_conv<false><<<Ky * ((Kxh + lz - 1) / lz), 256, smz, st>>>(a, pz, lz);
-  k_fft_y<<<Kz * ((Kxh + ly - 1) / ly), 256, smy, st>>>(a, py, ly, 1);
-  k_fft_x_c2r<<<(rows + lx - 1) / lx, 256, smx, st>>>(a, px, lx);
+  const dim3 gx((rows + lx - 1) / lx), gy(Kz * ((Kxh + ly - 1) / ly)), gz(Ky * ((Kxh + lz - 1) / lz));
+  // compile-time-sized kernels where available, runtime plans otherwise
+  if (!fft_x_r2c_t(a, lx, gx, smx, st)) k_fft_x_r2c<<<gx, 256, smx, st>>>(a, px, lx);
+  if (!fft_y_t(a, ly, false, gy, smy, st)) k_fft_y<<<gy, 256, smy, st>>>(a, py, ly, 0);
+  if (!fft_z_t(a, lz, energy, gz, smz, st)) {
+    if (energy)
+      k_fft_z_conv<true><<<gz, 256, smz, st>>>(a, pz, lz);
+    else
+      k_fft_z_conv<false><<<gz, 256, smz, st>>>(a, pz, lz);
+  }
+  if (!fft_y_t(a, ly, true, gy, smy, st)) k_fft_y<<<gy, 256, smy, st>>>(a, py, ly, 1);
+  if (!fft_x_c2r_t(a, lx, gx, smx, st)) k_fft_x_c2r<<<gx, 256, smx, st>>>(a, px, lx);
   k_pme_gather<<<(a.n + 255) / 256, 256, 0, st>>>(a);
 }
 

@@ -156,8 +156,8 @@ fz_status fz_get_forces_fixed(fz_system* sys, long long* out3n);
 /* float32 state transfer through caller-pinned host buffers (x,y,z per atom). */
 fz_status fz_set_state_f32(fz_system* sys, const float* pos3n, const float* vel3n);
 fz_status fz_get_state_f32(fz_system* sys, float* pos3n, float* vel3n);
-/* Device-side work counters of the last fz_step: [0] kernel launches issued,
- * [1] neighbour-list rebuilds, [2] tiles in the current list, [3] pair tiles capacity. */
+/* Device-side work counters: [0] kernel launches issued, [1] neighbour-list rebuilds,
+ * [2] 32x32 pair tiles in the current (pruned) list, [3] list prunes. */
 fz_status fz_get_counters(fz_system* sys, long long* out4);
 /* Per-stage device timing (CUDA events on the system stream) for the steps run
  * while enabled.  Stages: 0 neighbour maintenance, 1 real-space pairs, 2 bonded,
