@@ -74,6 +74,7 @@ struct Engine {
   int *brick_of = nullptr, *brick_count = nullptr, *brick_cursor = nullptr, *brick_start = nullptr,
       *brick_atoms = nullptr;
   float* grid = nullptr;
+  int* qgrid = nullptr;
   float2* cgrid = nullptr;
   float2* tw[3] = {nullptr, nullptr, nullptr};
   float *gfac[3] = {nullptr, nullptr, nullptr}, *f2[3] = {nullptr, nullptr, nullptr};
@@ -238,6 +239,7 @@ struct Engine {
     a.brick_start = brick_start;
     a.brick_atoms = brick_atoms;
     a.grid = grid;
+    a.qgrid = qgrid;
     a.cgrid = cgrid;
     a.gscale = gscale;
     a.facc = facc;
@@ -407,13 +409,15 @@ struct Engine {
 void destroy_engine(Engine* e) { delete e; }
 
 static int brick_edge(int K) {
-  int best = K, bd = 1 << 30;
-  for (int d = 3; d <= 16; ++d)
-    if (K % d == 0 && std::abs(d - 8) < bd) {
-      bd = std::abs(d - 8);
-      best = d;
-    }
-  return best;
+  // largest divisor of K in [4, 16] that still gives >= 256 bricks (one CTA each);
+  // else the smallest divisor >= 4 (brick edge >= 3 keeps the stencil halo one brick deep)
+  int best = 0;
+  for (int d = 4; d <= 16; ++d)
+    if (K % d == 0 && (K / d) * (K / d) * (K / d) >= 256) best = d;
+  if (best) return best;
+  for (int d = 4; d <= K; ++d)
+    if (K % d == 0) return d;
+  return K;
 }
 
 static bool fft_size_ok(int n) {
@@ -648,6 +652,7 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
     if ((r = e->alloc(&e->brick_of, n)) || (r = e->alloc(&e->brick_count, nbr)) ||
         (r = e->alloc(&e->brick_cursor, nbr)) || (r = e->alloc(&e->brick_start, nbr + 1)) ||
         (r = e->alloc(&e->brick_atoms, n)) || (r = e->alloc(&e->grid, (size_t)Kx * Ky * Kz)) ||
+        (r = e->alloc(&e->qgrid, (size_t)Kx * Ky * Kz)) ||
         (r = e->alloc(&e->cgrid, (size_t)Kz * Ky * (Kx / 2 + 1))))
       return r;
     const double b2 = c.kappa * c.kappa;

@@ -74,7 +74,8 @@ struct PmeArgs {
   int* brick_cursor;
   int* brick_start;  // [nbricks+1]
   int* brick_atoms;  // [n]
-  float* grid;       // real grid Kz*Ky*Kx (charges, then potential)
+  int* qgrid;        // charge grid Kz*Ky*Kx, int32 fixed point 2^24 (zero between calls)
+  float* grid;       // potential grid Kz*Ky*Kx (real)
   float2* cgrid;     // complex half grid Kz*Ky*(Kx/2+1)
   const float2* tw[3];     // twiddles per dimension (forward, e^{-2 pi i m/K})
   const float* gfac[3];    // per-dim b^2 exp(-pi^2 f^2/beta^2)

@@ -115,69 +115,58 @@ __global__ void k_pme_scatter(PmeArgs a) {
   a.brick_atoms[a.brick_start[b] + k] = i;
 }
 
-// charge-grid accumulation in shared memory: int32 fixed point, 2^24 per e (values
-// stay far below the +-128 e range a grid point could hold), native shared atomics
-constexpr float kFixQ32 = 16777216.0f;
+constexpr float kFixQ32 = 16777216.0f;  // charge grid fixed point, 2^24 per e
 
-// cubic B-spline weight M4(t + j) (j = 0..3, t in [0,1))
-__device__ __forceinline__ float bsp4_w(float t, int j) {
-  const float t2 = t * t, t3 = t2 * t, u = 1.f - t;
-  const float s = 1.f / 6.f;
-  const float w0 = t3 * s;
-  const float w1 = fmaf(-3.f, t3, fmaf(3.f, t2, fmaf(3.f, t, 1.f))) * s;
-  const float w2 = fmaf(3.f, t3, fmaf(-6.f, t2, 4.f)) * s;
-  const float w3 = u * u * u * s;
-  return j == 0 ? w0 : (j == 1 ? w1 : (j == 2 ? w2 : w3));
-}
-
-// One CTA per brick; each warp takes one candidate atom at a time and its 32 lanes
-// cover 32 of the atom's 64 stencil points (two passes), so a warp's shared atomics
-// never collide with each other.
+// One CTA per brick processes the atoms binned to that brick exactly once: their
+// 4x4x4 stencils (grid points k0-3..k0 per dimension) all fall inside the brick grown
+// by 3 points on the low side, accumulated in shared memory with int32 fixed-point
+// atomics (2^24 per e; values stay far below +-128 e); the region is then added to
+// the int32 charge grid with RED atomics.  Integer sums are order independent, so the
+// grid is bit-reproducible.
 __global__ void __launch_bounds__(256) k_pme_spread(PmeArgs a) {
   extern __shared__ int acc[];
   const int Bx = a.B[0], By = a.B[1], Bz = a.B[2];
-  const int nbx = a.nb[0], nby = a.nb[1], nbz = a.nb[2];
+  const int Ex = Bx + 3, Ey = By + 3, Ez = Bz + 3;
+  const int nbx = a.nb[0], nby = a.nb[1];
   const int b = blockIdx.x;
   const int bx = b % nbx, by = (b / nbx) % nby, bz = b / (nbx * nby);
-  const int vol = Bx * By * Bz;
+  const int vol = Ex * Ey * Ez;
   for (int k = threadIdx.x; k < vol; k += blockDim.x) acc[k] = 0;
   __syncthreads();
   const int Kx = a.K[0], Ky = a.K[1], Kz = a.K[2];
-  const int ox = bx * Bx, oy = by * By, oz = bz * Bz;
-  const int sdx = nbx > 1 ? 2 : 1, sdy = nby > 1 ? 2 : 1, sdz = nbz > 1 ? 2 : 1;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int jx = lane & 3, jy = (lane >> 2) & 3, jz0 = lane >> 4;  // jz = jz0 and jz0 + 2
-  for (int dz = 0; dz < sdz; ++dz)
-    for (int dy = 0; dy < sdy; ++dy)
-      for (int dx = 0; dx < sdx; ++dx) {
-        const int sb = (((bz + dz) % nbz) * nby + (by + dy) % nby) * nbx + (bx + dx) % nbx;
-        const int s0 = a.brick_start[sb], s1 = a.brick_start[sb + 1];
-        for (int idx = s0 + warp; idx < s1; idx += nw) {
-          const int i = a.brick_atoms[idx];
-          const float4 r = a.pos4[i];
-          float tx, ty, tz;
-          const int kx = grid_base(r.x, a.p.inv_box.x, Kx, &tx);
-          const int ky = grid_base(r.y, a.p.inv_box.y, Ky, &ty);
-          const int kz = grid_base(r.z, a.p.inv_box.z, Kz, &tz);
-          // local offsets of grid point k0 - j in this brick; k0 - j - o lies in (-K, K)
-          int lx = kx - jx - ox, ly = ky - jy - oy;
-          lx += lx < 0 ? Kx : 0;
-          ly += ly < 0 ? Ky : 0;
-          const float qxy = r.w * bsp4_w(tx, jx) * bsp4_w(ty, jy);
+  // region origin: brick origin - 3
+  const int ox = bx * Bx - 3, oy = by * By - 3, oz = bz * Bz - 3;
+  const int s0 = a.brick_start[b], s1 = a.brick_start[b + 1];
+  for (int idx = s0 + threadIdx.x; idx < s1; idx += blockDim.x) {
+    const float4 r = a.pos4[a.brick_atoms[idx]];
+    float tx, ty, tz, wx[4], wy[4], wz[4];
+    const int kx = grid_base(r.x, a.p.inv_box.x, Kx, &tx) - ox;
+    const int ky = grid_base(r.y, a.p.inv_box.y, Ky, &ty) - oy;
+    const int kz = grid_base(r.z, a.p.inv_box.z, Kz, &tz) - oz;
+    bsp4(tx, wx, nullptr);
+    bsp4(ty, wy, nullptr);
+    bsp4(tz, wz, nullptr);
+    const float q = r.w * kFixQ32;
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int jz = jz0 + 2 * h;
-            int lz = kz - jz - oz;
-            lz += lz < 0 ? Kz : 0;
-            if (lx < Bx && ly < By && lz < Bz)
-              atomicAdd(&acc[(lz * By + ly) * Bx + lx], __float2int_rn(qxy * bsp4_w(tz, jz) * kFixQ32));
-          }
-        }
+    for (int jz = 0; jz < 4; ++jz)
+#pragma unroll
+      for (int jy = 0; jy < 4; ++jy) {
+        const float qzy = q * wz[jz] * wy[jy];
+        int* row = acc + ((kz - jz) * Ey + (ky - jy)) * Ex + kx;
+#pragma unroll
+        for (int jx = 0; jx < 4; ++jx) atomicAdd(row - jx, __float2int_rn(qzy * wx[jx]));
       }
+  }
   __syncthreads();
   for (int k = threadIdx.x; k < vol; k += blockDim.x) {
-    const int lx = k % Bx, ly = (k / Bx) % By, lz = k / (Bx * By);
-    a.grid[((size_t)(oz + lz) * Ky + (oy + ly)) * Kx + (ox + lx)] = (float)acc[k] * (1.0f / kFixQ32);
+    const int v = acc[k];
+    if (v == 0) continue;
+    const int lx = k % Ex, ly = (k / Ex) % Ey, lz = k / (Ex * Ey);
+    int gx = ox + lx, gy = oy + ly, gz = oz + lz;
+    gx += gx < 0 ? Kx : 0;
+    gy += gy < 0 ? Ky : 0;
+    gz += gz < 0 ? Kz : 0;
+    atomicAdd(a.qgrid + ((size_t)gz * Ky + gy) * Kx + gx, v);
   }
 }
 
@@ -276,7 +265,13 @@ __global__ void __launch_bounds__(256) k_fft_x_r2c(PmeArgs a, FftPlan pl, int nl
   for (int idx = threadIdx.x; idx < nl * Kx; idx += blockDim.x) {
     const int l = idx / Kx, x = idx - l * Kx;
     const int row = r0 + l;
-    A[l * ld + x] = make_float2(row < nrows ? a.grid[(size_t)row * Kx + x] : 0.f, 0.f);
+    float qv = 0.f;
+    if (row < nrows) {
+      int* qp = a.qgrid + (size_t)row * Kx + x;
+      qv = (float)*qp * (1.0f / kFixQ32);
+      *qp = 0;  // leaves the charge grid zeroed for the next spread
+    }
+    A[l * ld + x] = make_float2(qv, 0.f);
   }
   __syncthreads();
   const float2* R = fft_lines(A, B, tw, pl, nl, false);
@@ -555,7 +550,13 @@ __global__ void __launch_bounds__(256) k_fft_x_r2c_t(PmeArgs a, int nl) {
   for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) {
     const int l = idx / N, x = idx - l * N;
     const int row = r0 + l;
-    A[l * LD + x] = make_float2(row < nrows ? a.grid[(size_t)row * N + x] : 0.f, 0.f);
+    float qv = 0.f;
+    if (row < nrows) {
+      int* qp = a.qgrid + (size_t)row * N + x;
+      qv = (float)*qp * (1.0f / kFixQ32);
+      *qp = 0;  // leaves the charge grid zeroed for the next spread
+    }
+    A[l * LD + x] = make_float2(qv, 0.f);
   }
   __syncthreads();
   const float2* R = fft_run_t<N, 0, 1, false>(A, B, tw, nl);
@@ -730,7 +731,7 @@ void launch_pme(const PmeArgs& a, bool energy, cudaStream_t st) {
   k_pme_bin<<<(a.n + 255) / 256, 256, 0, st>>>(a);
   k_pme_scan<<<1, 1024, 0, st>>>(a, nbr);
   k_pme_scatter<<<(a.n + 255) / 256, 256, 0, st>>>(a);
-  const size_t sp = (size_t)a.B[0] * a.B[1] * a.B[2] * sizeof(int);
+  const size_t sp = (size_t)(a.B[0] + 3) * (a.B[1] + 3) * (a.B[2] + 3) * sizeof(int);
   k_pme_spread<<<nbr, 256, sp, st>>>(a);
   const int Kx = a.K[0], Ky = a.K[1], Kz = a.K[2], Kxh = Kx / 2 + 1;
   const FftPlan px = make_plan(Kx), py = make_plan(Ky), pz = make_plan(Kz);
