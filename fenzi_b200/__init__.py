@@ -77,7 +77,8 @@ EXPORTS = ["fz_last_error", "fz_version", "fz_read_input", "fz_load_system", "fz
            "fz_free", "fz_upload", "fz_reassign_velocities", "fz_compute_forces", "fz_compute_forces_terms", "fz_step", "fz_eval_props",
            "fz_get_positions", "fz_set_positions", "fz_get_velocities", "fz_set_velocities", "fz_get_forces",
            "fz_get_forces_fixed", "fz_set_state_f32", "fz_get_state_f32", "fz_get_counters", "fz_sync",
-           "fz_stream", "fz_set_stage_timing", "fz_get_stage_times", "fz_measure_fp32_peak"]
+           "fz_stream", "fz_set_stage_timing", "fz_get_stage_times", "fz_measure_fp32_peak",
+           "fz_pme_reciprocal_static"]
 
 STAGES = ["neighbour", "nonbonded", "bonded", "pme", "integrate"]
 
@@ -121,6 +122,8 @@ def lib():
             "fz_set_stage_timing": ([vp, C.c_int], C.c_int),
             "fz_get_stage_times": ([vp, dp], C.c_int),
             "fz_measure_fp32_peak": ([C.c_int, dp], C.c_int),
+            "fz_pme_reciprocal_static": ([C.c_int, vp, vp, C.c_int, dp, C.POINTER(C.c_int), C.c_double, vp, dp],
+                                         C.c_int),
             "fz_stream": ([vp], vp),
         }
         for name, (args, res) in sig.items():
@@ -307,6 +310,17 @@ def fp32_peak_tflops(device: int = 0) -> float:
     out = C.c_double()
     _check(lib().fz_measure_fp32_peak(int(device), C.byref(out)))
     return out.value
+
+
+def pme_reciprocal_static(device, pos4_ptr, n, box, K, beta, facc_ptr, stream=None, energy=True):
+    """PME reciprocal forces with no device allocation (fz_pme_reciprocal_static):
+    pos4_ptr / facc_ptr are caller-owned device pointers (float4[n], int64[3n])."""
+    b = (C.c_double * 3)(*[float(x) for x in box])
+    k = (C.c_int * 3)(*[int(x) for x in K])
+    e = C.c_double()
+    _check(lib().fz_pme_reciprocal_static(int(device), stream, C.c_void_p(pos4_ptr), int(n), b, k, float(beta),
+                                          C.c_void_p(facc_ptr), C.byref(e) if energy else None))
+    return e.value if energy else None
 
 
 def load(in_path: str, device: int | None = None) -> FenZi:

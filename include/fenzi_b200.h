@@ -168,6 +168,18 @@ fz_status fz_get_stage_times(fz_system* sys, double* out6);
 /* Measures this GPU's FP32 FMA throughput (TFLOP/s) with a register-resident FMA
  * kernel; the roof of the pair kernel, which no table of peaks carries. */
 fz_status fz_measure_fp32_peak(int device, double* tflops);
+/* No counterpart in the reference.  PME reciprocal-space forces (and optionally the
+ * reciprocal energy) of n atoms for callers that cannot call cudaMalloc (code living
+ * inside another framework's memory pool or a pre-sized arena).  Allocates nothing:
+ * scratch lives in fixed file-scope device arrays (about 5.4 MB on each GPU that loads
+ * the library, held until exit).  pos4: device float4[n] (x, y, z, q); facc: device
+ * int64[3n] fixed point (scale 2^32, x[n] y[n] z[n]), overwritten; energy_out: host
+ * double or NULL (when given, the call synchronises `stream`).  Limits: n <= 262144,
+ * grid sizes 2^a 3^b 5^c in 4..64.  The first call on a device resolves the scratch
+ * addresses (make it before any stream capture); calls that overlap on the GPU race
+ * on the shared scratch and must be serialised by the caller. */
+fz_status fz_pme_reciprocal_static(int device, void* stream, const float* pos4, int n, const double* box,
+                                   const int* K, double beta, long long* facc, double* energy_out);
 /* Synchronises the system's stream and reports any sticky device error status. */
 fz_status fz_sync(fz_system* sys);
 /* The system's CUDA stream (cudaStream_t), for callers that time or order work. */
