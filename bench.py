@@ -56,6 +56,12 @@ def args_():
                     help="input preparation: MD steps with 300 K velocity reassignment every 100 steps "
                          "(relaxes the seeded lattice start; untimed, before the warm-up)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ensemble", type=int, default=256,
+                    help="batched-ensemble measurement (BASELINE configs[2]) with this many boxes; 0 skips it")
+    ap.add_argument("--served", type=int, default=32,
+                    help="served-job measurement (BASELINE configs[3]) with this many jobs; 0 skips it")
+    ap.add_argument("--precision", type=int, default=100000,
+                    help="precision study (BASELINE configs[4]): NVE steps of the 17,280-atom system; 0 skips it")
     ap.add_argument("--profile", action="store_true",
                     help="only run warm-up + steps (no timing/report): a clean target for ncu")
     return ap.parse_args()
@@ -127,6 +133,214 @@ def traffic_from_profiles(kernel_file):
         return json.load(open(p)).get("dram_bytes_per_launch")
     except Exception:
         return None
+
+
+def bench_ensemble(nsys, device, steps=30):
+    """Aggregate atom-steps/s of nsys independent water boxes advanced together (one
+    graph launch per step) versus the same boxes stepped one at a time; wall clock with
+    a device synchronisation on both sides of each timed region."""
+    import torch
+    import fenzi_b200 as fz
+    from fenzi_b200 import gen_system
+    boxes = gen_system.ensemble(nsys)
+    root = tempfile.mkdtemp(prefix="fzens_")
+    systems = []
+    for i, b in enumerate(boxes):
+        sy = fz.FenZi.ReadInput(gen_system.write(b, os.path.join(root, f"b{i:03d}"))).LoadSystem()
+        sy.InitMem(device)
+        sy.InitVelocity(T=300.0, seed=100 + i)
+        systems.append(sy)
+    natoms = sum(s.n for s in systems)
+    batch = fz.Batch(systems)
+    for k in range(3):  # relax the lattice starts
+        batch.step(100)
+        for i, sy in enumerate(systems):
+            sy.InitVelocity(T=300.0, seed=100 + i, counter=k + 1)
+    batch.step(10)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    batch.step(steps)
+    torch.cuda.synchronize()
+    tb = (time.perf_counter() - t0) / steps
+    seq_steps = max(3, steps // 3)
+    for sy in systems:  # warm each system's own graph
+        sy.SingleStep(1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for sy in systems:
+        sy.SingleStep(seq_steps)
+    torch.cuda.synchronize()
+    ts = (time.perf_counter() - t0) / seq_steps
+    batch.close()
+    for sy in systems:
+        sy.close()
+    return {"metric": "batched aggregate atom-steps/s", "value": natoms / tb, "unit": "atom-steps/s",
+            "systems": nsys, "atoms": natoms, "ms_per_batched_step": tb * 1e3,
+            "sequential_atom_steps_per_s": natoms / ts, "ms_per_sequential_sweep": ts * 1e3,
+            "speedup_vs_one_at_a_time": ts / tb,
+            "workload": f"{nsys} TIP3P boxes, 216-2000 waters each at 0.0334/A^3, grids 16^3-36^3 (smallest "
+                        f"2^a3^b5^c >= L/1.2), rc 9 / ron 7.5, beta 0.34, SHAKE, NVE, 1 fs; seeded",
+            "timing": "wall clock over 30 batched steps vs 10-step sweeps of the boxes one at a time, device "
+                      "synchronised around each; working set > L2"}
+
+
+def served_jobs(njobs, seed):
+    """The served-job stream: sizes U[1,500, 30,000] atoms with 0-40 chains (rest TIP3P),
+    steps log-uniform in [1,000, 20,000], half NVE and half NVT (300 K reassignment
+    every 1,000 steps), Poisson arrivals at 200 jobs/s; all from one seed."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    t = 0.0
+    for i in range(njobs):
+        natom = int(rng.integers(1500, 30001))
+        nch = int(rng.integers(0, 41))
+        nch = min(nch, max(0, (natom - 600) // 30))
+        nw = max(200, (natom - 30 * nch) // 3)
+        steps = int(round(float(np.exp(rng.uniform(np.log(1000), np.log(20000))))))
+        nvt = bool(rng.integers(0, 2))
+        t += float(rng.exponential(1.0 / 200.0))
+        jobs.append(dict(nw=nw, nchains=nch, steps=steps, nvt=nvt, arrival=t, seed=seed + 1 + i))
+    return jobs
+
+
+def bench_served(device, njobs=32, seed=4242, check=4):
+    """Served jobs through the serving loop (fz_server): each job is submitted at its
+    Poisson arrival time, admitted by the 150 GB HBM budget, advanced with the running
+    mix in the batch graph; latency = completion - submission on the server clock.
+    The one-at-a-time comparison times 200 steps of each job alone (its own CUDA graph)
+    and scales to the job's step count."""
+    import torch
+    import fenzi_b200 as fz
+    from fenzi_b200 import gen_system
+    from oracle.oracle import Oracle
+    jobs = served_jobs(njobs, seed)
+    root = tempfile.mkdtemp(prefix="fzserve_")
+    paths = []
+    for i, j in enumerate(jobs):
+        g = gen_system.build(name=f"job{i:02d}", nw=j["nw"], nchains=j["nchains"], chain_len=30, rc=10.0, ron=8.0,
+                             seed=j["seed"])
+        paths.append(gen_system.write(g, os.path.join(root, f"j{i:02d}")))
+
+    def load(i):
+        s = fz.FenZi.ReadInput(paths[i])
+        if jobs[i]["nvt"]:
+            s.cfg.temp_reset_every = 1000
+        return s.LoadSystem()
+
+    # one at a time: 200 steps of each job alone, scaled to its length
+    seq_s, natoms = 0.0, []
+    for i, j in enumerate(jobs):
+        s = load(i)
+        s.InitMem(device)
+        s.InitVelocity(T=300.0, seed=j["seed"])
+        s.SingleStep(20)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.SingleStep(200)
+        torch.cuda.synchronize()
+        seq_s += (time.perf_counter() - t0) / 200 * j["steps"]
+        natoms.append(s.n)
+        s.close()
+    systems = [load(i) for i in range(len(jobs))]
+    total = sum(n * j["steps"] for n, j in zip(natoms, jobs))
+    server = fz.Server(device, hbm_budget_bytes=150e9, chunk_steps=100, max_running=64)
+    ids = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i, j in enumerate(jobs):
+        d = j["arrival"] - (time.perf_counter() - t0)
+        if d > 0:
+            time.sleep(d)
+        ids.append(server.submit(systems[i], j["steps"]))
+    infos = [server.wait(k) for k in ids]
+    wall = time.perf_counter() - t0
+    stats = server.stats()
+    lat = np.array([x["latency_s"] for x in infos])
+    # final-frame force error against the FP64 oracle, on a sample of jobs
+    errs = []
+    for i in sorted(range(len(jobs)), key=lambda k: natoms[k])[:check]:
+        pos = server.positions(ids[i])
+        s = load(i)
+        s.InitMem(device)
+        s.set_positions(pos)
+        s.ComputeAccelGPU()
+        f = s.forces()
+        f0, _ = Oracle(s.topology()).forces(s.positions())
+        errs.append(float(np.sqrt(((f - f0) ** 2).sum() / (f0 ** 2).sum())))
+        s.close()
+    server.close()
+    return {"metric": "served p50/p99 job latency", "p50_s": float(np.percentile(lat, 50)),
+            "p99_s": float(np.percentile(lat, 99)), "unit": "s", "jobs": len(jobs),
+            "aggregate_atom_steps_per_s": total / wall, "makespan_s": wall,
+            "one_at_a_time_atom_steps_per_s": total / seq_s, "speedup_vs_one_at_a_time": seq_s / wall,
+            "peak_running_jobs": stats["peak_running"],
+            "final_frame_force_rel_rms_vs_oracle": {"max": max(errs), "jobs_checked": len(errs)},
+            "workload": f"{len(jobs)} jobs of a Poisson(200/s) stream (seed {seed}): 1.5k-30k atoms, 0-40 30-atom "
+                        f"chains + TIP3P, 1k-20k steps log-uniform, half NVT (reassignment every 1,000), rc 10, "
+                        f"beta 0.34, SHAKE, 1 fs; HBM budget 150 GB, 100-step chunks",
+            "timing": "wall clock from the first submission to the last completion; latency per job on the "
+                      "server's steady clock"}
+
+
+def bench_precision(device, nve_steps=100000, npt_steps=2000):
+    """The 17,280-atom precision study: NVE energy drift per ns per atom over nve_steps
+    (after 2,000 thermalised steps), total-force error against the FP64 oracle, run-to-
+    run bit-equality of the int64 force buffer (SHA-256 of two evaluations), then an
+    Andersen leg of npt_steps at 1 atm (conserved-quantity excursion, volume change)."""
+    import hashlib
+    import fenzi_b200 as fz
+    from fenzi_b200 import gen_system
+    from oracle.oracle import Oracle
+    g = gen_system.build(name="chain17k", seed=2345)
+    path = gen_system.write(g, tempfile.mkdtemp(prefix="fzprec_"))
+    s = fz.FenZi.ReadInput(path).LoadSystem()
+    s.InitMem(device)
+    s.InitVelocity(T=300.0, seed=2345, counter=0)
+    for k in range(20):
+        s.SingleStep(100)
+        s.InitVelocity(T=300.0, seed=2345, counter=k + 1)
+    s.SingleStep(100)
+    chunk = 1000
+    t, tot = [], []
+    t0 = time.perf_counter()
+    for k in range(nve_steps // chunk + 1):
+        if k:
+            s.SingleStep(chunk)
+        e = s.EvalProps()
+        t.append(k * chunk * s.cfg.timestep_ps * 1e-3)  # ns
+        tot.append(e["potential"] + e["kinetic"])
+    wall = time.perf_counter() - t0
+    slope = float(np.polyfit(np.array(t), np.array(tot), 1)[0])  # kcal/mol/ns
+    s.ComputeAccelGPU()
+    a = s.forces_fixed()
+    s.ComputeAccelGPU()
+    b = s.forces_fixed()
+    f = s.forces()
+    f0, _ = Oracle(s.topology()).forces(s.positions())
+    err = float(np.sqrt(((f - f0) ** 2).sum() / (f0 ** 2).sum()))
+    s.set_barostat(True, 1.0, 1e-5)
+    e0 = s.EvalProps()
+    hs, vs = [], []
+    for _ in range(npt_steps // 100):
+        s.SingleStep(100)
+        e = s.EvalProps()
+        hs.append(e["conserved"] - e0["conserved"])
+        vs.append(e["volume"] / e0["volume"] - 1.0)
+    out = {"workload": "chain17k: 5,360 TIP3P + 40 x 30-atom chains = 17,280 atoms, 56 A, 64^3, beta 0.34, rc 10, "
+                       "SHAKE, 1 fs",
+           "nve_steps": nve_steps, "nve_wall_s": wall,
+           "nve_drift_kcal_per_mol_per_ns_per_atom": slope / s.n,
+           "nve_total_energy_std_kcal_per_mol": float(np.std(tot)),
+           "force_rel_rms_vs_fp64_oracle": err,
+           "force_sha256": [hashlib.sha256(a.tobytes()).hexdigest()[:16], hashlib.sha256(b.tobytes()).hexdigest()[:16]],
+           "forces_bit_reproducible": bool(np.array_equal(a, b)),
+           "all_fp64_gpu_variant": None,
+           "npt": {"steps": npt_steps, "pref_atm": 1.0, "pmass": 1e-5,
+                   "conserved_max_excursion_kcal_per_mol": float(np.abs(hs).max()),
+                   "kinetic_kcal_per_mol": e0["kinetic"], "volume_change_max": float(np.abs(vs).max()),
+                   "final_box_A": e["box"][0], "final_pressure_atm": e["pressure_atm"]}}
+    s.close()
+    return out
 
 
 def cpu_baseline(path, nsteps):
@@ -296,6 +510,15 @@ def main():
             per, cores = cpu_baseline(path, 4)
             cpu = {"value": 86.4 * dt_fs / (per * 1e3), "unit": "ns/day", "cores": cores, "kind": "port",
                    "sample": "4 full MD steps of the 230,400-atom system (FP64 oracle, OpenMP, all host threads)"}
+        batched = None
+        if a.ensemble > 0 and world == 1:
+            batched = bench_ensemble(a.ensemble, local)
+        served = None
+        if a.served > 0 and world == 1:
+            served = bench_served(local, a.served)
+        precision = None
+        if a.precision > 0 and world == 1:
+            precision = bench_precision(local, a.precision)
         line = {"metric": "ns/day @230K atoms (MD step, 1 fs)", "value": value, "unit": "ns/day",
                 "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_step,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
@@ -312,11 +535,14 @@ def main():
                 "prunes_total": sysm.counters()["prunes"],
                 "pair_slot_efficiency": pairs / (sysm.counters()["tiles"] * 1024.0),
                 "roofline": roof, "cpu_baseline": cpu,
-                "e2e": {"value": e2e_nsd, "unit": "ns/day", "h2d_bytes_per_step": 24 * natom,
-                        "d2h_bytes_per_step": 24 * natom,
-                        "step": f"one C-ABI call chain per {a.chunk} MD steps: fz_set_state_f32 + fz_step + "
-                                f"fz_get_state_f32 (pinned host buffers, wall clock)"},
-                "gpu_launches": launches, "clocks": clocks}
+                "e2e": {"value": e2e_nsd, "unit": "ns/day", "h2d_bytes_per_step": 24 * natom / a.chunk,
+                        "d2h_bytes_per_step": 24 * natom / a.chunk, "h2d_bytes_per_call": 24 * natom,
+                        "d2h_bytes_per_call": 24 * natom,
+                        "step": f"one C-ABI call chain per {a.chunk} MD steps: fz_set_state_f32 (positions + "
+                                f"velocities from pinned host memory) + fz_step({a.chunk}) + fz_get_state_f32 "
+                                f"(wall clock); bytes per MD step are the per-call copies / {a.chunk}"},
+                "gpu_launches": launches, "clocks": clocks, "batched": batched, "served": served,
+                "precision": precision}
     if dist:
         dist.barrier()
         dist.destroy_process_group()

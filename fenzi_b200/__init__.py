@@ -60,10 +60,20 @@ class Config(C.Structure):
 
 class Energies(C.Structure):
     _fields_ = [(k, C.c_double) for k in E_FIELDS] + [
-        ("virial", C.c_double * 3), ("pressure_atm", C.c_double), ("step", C.c_longlong)]
+        ("virial", C.c_double * 3), ("pressure_atm", C.c_double), ("step", C.c_longlong),
+        ("box", C.c_double * 3), ("volume", C.c_double), ("conserved", C.c_double)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k in E_FIELDS}
+        d = {k: getattr(self, k) for k in E_FIELDS}
+        d.update(virial=list(self.virial), pressure_atm=self.pressure_atm, step=self.step, box=list(self.box),
+                 volume=self.volume, conserved=self.conserved)
+        return d
+
+
+class JobInfo(C.Structure):
+    _fields_ = [("job", C.c_int), ("state", C.c_int), ("status", C.c_int), ("natom", C.c_int),
+                ("nsteps", C.c_longlong), ("steps_done", C.c_longlong), ("submit_s", C.c_double),
+                ("start_s", C.c_double), ("end_s", C.c_double), ("device_bytes", C.c_double), ("final", Energies)]
 
 
 class Info(C.Structure):
@@ -78,7 +88,10 @@ EXPORTS = ["fz_last_error", "fz_version", "fz_read_input", "fz_load_system", "fz
            "fz_get_positions", "fz_set_positions", "fz_get_velocities", "fz_set_velocities", "fz_get_forces",
            "fz_get_forces_fixed", "fz_set_state_f32", "fz_get_state_f32", "fz_get_counters", "fz_sync",
            "fz_stream", "fz_set_stage_timing", "fz_get_stage_times", "fz_measure_fp32_peak",
-           "fz_pme_reciprocal_static"]
+           "fz_pme_reciprocal_static", "fz_batch_create", "fz_batch_add", "fz_batch_step", "fz_batch_free",
+           "fz_set_barostat", "fz_get_virial", "fz_batch_remove", "fz_batch_size", "fz_server_create",
+           "fz_server_submit", "fz_server_info", "fz_server_wait", "fz_server_positions", "fz_server_stats",
+           "fz_server_free", "fz_server_estimate_bytes"]
 
 STAGES = ["neighbour", "nonbonded", "bonded", "pme", "integrate"]
 
@@ -122,9 +135,25 @@ def lib():
             "fz_set_stage_timing": ([vp, C.c_int], C.c_int),
             "fz_get_stage_times": ([vp, dp], C.c_int),
             "fz_measure_fp32_peak": ([C.c_int, dp], C.c_int),
+            "fz_batch_create": ([C.POINTER(vp)], C.c_int),
+            "fz_batch_add": ([vp, vp], C.c_int),
+            "fz_batch_step": ([vp, C.c_int], C.c_int),
+            "fz_batch_free": ([vp], C.c_int),
             "fz_pme_reciprocal_static": ([C.c_int, vp, vp, C.c_int, dp, C.POINTER(C.c_int), C.c_double, vp, dp],
                                          C.c_int),
             "fz_stream": ([vp], vp),
+            "fz_set_barostat": ([vp, C.c_int, C.c_double, C.c_double], C.c_int),
+            "fz_get_virial": ([vp, dp], C.c_int),
+            "fz_batch_remove": ([vp, vp], C.c_int),
+            "fz_batch_size": ([vp, C.POINTER(C.c_int)], C.c_int),
+            "fz_server_create": ([C.c_int, C.c_double, C.c_int, C.c_int, C.POINTER(vp)], C.c_int),
+            "fz_server_submit": ([vp, vp, C.c_longlong, C.POINTER(C.c_int)], C.c_int),
+            "fz_server_info": ([vp, C.c_int, C.POINTER(JobInfo)], C.c_int),
+            "fz_server_wait": ([vp, C.c_int, C.POINTER(JobInfo)], C.c_int),
+            "fz_server_positions": ([vp, C.c_int, dp], C.c_int),
+            "fz_server_stats": ([vp, dp], C.c_int),
+            "fz_server_free": ([vp], C.c_int),
+            "fz_server_estimate_bytes": ([vp, dp], C.c_int),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -237,6 +266,13 @@ class FenZi:
         _check(lib().fz_eval_props(self.h, C.byref(e)))
         return e.as_dict()
 
+    def set_barostat(self, enable: bool = True, pref_atm: float | None = None, pmass: float | None = None):
+        """Andersen constant-pressure dynamics (the reference's PCONSTANT build) for the
+        following SingleStep calls; defaults are the input file's pref / pmass."""
+        pr = self.cfg.pref if pref_atm is None else pref_atm
+        pm = self.cfg.pmass if pmass is None else pmass
+        _check(lib().fz_set_barostat(self.h, 1 if enable else 0, float(pr), float(pm)))
+
     def positions(self):
         out = np.zeros((self.n, 3))
         _check(lib().fz_get_positions(self.h, _dp(out)))
@@ -291,6 +327,12 @@ class FenZi:
     def sync(self):
         _check(lib().fz_sync(self.h))
 
+    def virial(self):
+        """Virial diagonal of the last ComputeAccelGPU(..., energies=True)-style call."""
+        out = np.zeros(3)
+        _check(lib().fz_get_virial(self.h, _dp(out)))
+        return out
+
     def stream(self):
         return lib().fz_stream(self.h)
 
@@ -310,6 +352,106 @@ def fp32_peak_tflops(device: int = 0) -> float:
     out = C.c_double()
     _check(lib().fz_measure_fp32_peak(int(device), C.byref(out)))
     return out.value
+
+
+class Batch:
+    """Independent systems advanced together, one CUDA-graph launch per MD step."""
+
+    def __init__(self, systems=()):
+        self.h = C.c_void_p()
+        _check(lib().fz_batch_create(C.byref(self.h)))
+        self.systems = []
+        for s in systems:
+            self.add(s)
+
+    def add(self, s: FenZi):
+        _check(lib().fz_batch_add(self.h, s.h))
+        self.systems.append(s)
+
+    def remove(self, s: FenZi):
+        _check(lib().fz_batch_remove(self.h, s.h))
+        self.systems.remove(s)
+
+    def step(self, nsteps=1):
+        _check(lib().fz_batch_step(self.h, int(nsteps)))
+
+    def close(self):
+        if self.h:
+            lib().fz_batch_free(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Serving loop (fz_server_*): submitted jobs are admitted by an HBM budget, stay
+    resident and advance together in the batch graph; each job's latency is measured
+    from submission to completion on the server's clock."""
+
+    STATES = ("queued", "running", "done", "failed")
+
+    def __init__(self, device=0, hbm_budget_bytes=150e9, chunk_steps=100, max_running=64):
+        self.h = C.c_void_p()
+        _check(lib().fz_server_create(int(device), float(hbm_budget_bytes), int(chunk_steps), int(max_running),
+                                      C.byref(self.h)))
+        self.natom = {}
+
+    @staticmethod
+    def estimate_bytes(s: FenZi) -> float:
+        """Admission estimate of a loaded system's device memory."""
+        out = C.c_double()
+        _check(lib().fz_server_estimate_bytes(s.h, C.byref(out)))
+        return out.value
+
+    def submit(self, s: FenZi, nsteps: int) -> int:
+        """Hands a loaded (not uploaded) system to the server, which owns it from now on."""
+        jid = C.c_int()
+        _check(lib().fz_server_submit(self.h, s.h, int(nsteps), C.byref(jid)))
+        self.natom[jid.value] = s.n
+        s.h = C.c_void_p()
+        return jid.value
+
+    @staticmethod
+    def _as_dict(j: JobInfo) -> dict:
+        return dict(job=j.job, state=Server.STATES[j.state], status=j.status, natom=j.natom, nsteps=j.nsteps,
+                    steps_done=j.steps_done, submit_s=j.submit_s, start_s=j.start_s, end_s=j.end_s,
+                    latency_s=j.end_s - j.submit_s if j.end_s >= 0 else None, device_bytes=j.device_bytes,
+                    final=j.final.as_dict())
+
+    def info(self, job: int) -> dict:
+        j = JobInfo()
+        _check(lib().fz_server_info(self.h, int(job), C.byref(j)))
+        return self._as_dict(j)
+
+    def wait(self, job: int) -> dict:
+        j = JobInfo()
+        _check(lib().fz_server_wait(self.h, int(job), C.byref(j)))
+        return self._as_dict(j)
+
+    def positions(self, job: int):
+        out = np.zeros((self.natom[job], 3))
+        _check(lib().fz_server_positions(self.h, int(job), _dp(out)))
+        return out
+
+    def stats(self) -> dict:
+        out = np.zeros(4)
+        _check(lib().fz_server_stats(self.h, _dp(out)))
+        return dict(peak_running=int(out[0]), atom_steps=int(out[1]), bytes_in_use=out[2], finished=int(out[3]))
+
+    def close(self):
+        if self.h:
+            _check(lib().fz_server_free(self.h))
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def pme_reciprocal_static(device, pos4_ptr, n, box, K, beta, facc_ptr, stream=None, energy=True):

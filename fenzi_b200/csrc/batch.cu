@@ -1,0 +1,480 @@
+// Batched ensemble and serving loop.
+//
+// fz_batch: many independent uploaded systems advanced together.  One MD step of every
+// system is captured into a single CUDA graph in which each system's step (kick/drift/
+// SHAKE, neighbour maintenance, forces with PME on its second stream, kick/RATTLE) is
+// an independent branch forked from and joined to one master stream, so the GPU runs
+// the small systems' kernels concurrently; each step is one graph launch.  Systems may
+// join and leave between calls (the graph is re-captured on the next step).  Velocity
+// reassignment (NVT by reassignment every temp_reset_every steps, src/fenzi.cu:463-473)
+// splits a call at the reassignment steps of its systems, with the same counter as
+// fz_step, so each system's trajectory is bit-identical alone and in any mix.
+//
+// fz_server: a request loop on a worker thread.  Submitted jobs (a loaded system and a
+// step count) wait in a FIFO queue and are admitted while the estimated device memory
+// of the admitted jobs stays within the HBM budget and a slot is free; admitted jobs
+// are uploaded once, start from Maxwell-Boltzmann velocities at the input's temperature
+// and seed, stay resident (coordinates, velocities, neighbour lists, PME
+// grids) and advance together in the batch graph, in chunks that end when a job
+// finishes; a finished job's final energies and positions are kept on the host, its
+// device memory is freed, and queued jobs are admitted into the running mix.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+
+#include "engine.h"
+
+using namespace fz;
+
+// ====================================================================== batched ensemble
+struct fz_batch {
+  std::vector<fz_system*> systems;
+  int dev = -1;
+  cudaStream_t master = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_master = nullptr;
+  std::vector<cudaEvent_t> ev_done;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int* pinned_status = nullptr;
+  long long steps = 0;
+  void drop_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+    for (auto e : ev_done) cudaEventDestroy(e);
+    ev_done.clear();
+    if (pinned_status) cudaFreeHost(pinned_status);
+    pinned_status = nullptr;
+  }
+  ~fz_batch() {
+    if (master) cudaStreamSynchronize(master);
+    drop_graph();
+    if (ev_start) cudaEventDestroy(ev_start);
+    if (ev_master) cudaEventDestroy(ev_master);
+    if (master) cudaStreamDestroy(master);
+  }
+};
+
+static std::string last_error_text() {
+  char buf[1024];
+  fz_last_error(buf, sizeof buf);
+  return std::string(buf);
+}
+
+extern "C" fz_status fz_batch_create(fz_batch** out) {
+  if (!out) return fail(FZ_ERR_ARG, "null output");
+  *out = new fz_batch();
+  return FZ_OK;
+}
+
+extern "C" fz_status fz_batch_add(fz_batch* b, fz_system* s) {
+  if (!b || !s) return fail(FZ_ERR_ARG, "null argument");
+  if (!s->eng) return fail(FZ_ERR_STATE, "fz_batch_add: system not uploaded (fz_upload)");
+  if (b->dev >= 0 && s->eng->dev != b->dev) return fail(FZ_ERR_ARG, "fz_batch_add: systems must share one device");
+  if (s->eng->npt) return fail(FZ_ERR_STATE, "fz_batch_add: barostat systems synchronise every step; step them alone");
+  if (std::find(b->systems.begin(), b->systems.end(), s) != b->systems.end())
+    return fail(FZ_ERR_ARG, "fz_batch_add: system already in the batch");
+  b->dev = s->eng->dev;
+  b->systems.push_back(s);
+  b->drop_graph();
+  return FZ_OK;
+}
+
+extern "C" fz_status fz_batch_remove(fz_batch* b, fz_system* s) {
+  if (!b || !s) return fail(FZ_ERR_ARG, "null argument");
+  auto it = std::find(b->systems.begin(), b->systems.end(), s);
+  if (it == b->systems.end()) return fail(FZ_ERR_ARG, "fz_batch_remove: system not in the batch");
+  if (b->master) cudaStreamSynchronize(b->master);
+  b->systems.erase(it);
+  b->drop_graph();
+  if (b->systems.empty()) b->dev = -1;
+  return FZ_OK;
+}
+
+static fz_status capture(fz_batch* b) {
+  const int ns = (int)b->systems.size();
+  fz_status r;
+  for (fz_system* s : b->systems) {
+    Engine* e = s->eng;
+    if (!e->forces_valid) {
+      FZ_CUDA(cudaMemsetAsync(e->facc, 0, 3 * sizeof(long long) * e->n, e->st));
+      e->forces(false);
+      e->forces_valid = true;
+    }
+    if ((r = e->check())) return r;
+  }
+  if (!b->master) {
+    FZ_CUDA(cudaStreamCreateWithFlags(&b->master, cudaStreamNonBlocking));
+    FZ_CUDA(cudaEventCreateWithFlags(&b->ev_start, cudaEventDisableTiming));
+    FZ_CUDA(cudaEventCreateWithFlags(&b->ev_master, cudaEventDisableTiming));
+  }
+  b->ev_done.resize(ns, nullptr);
+  for (auto& e : b->ev_done) FZ_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  FZ_CUDA(cudaMallocHost(&b->pinned_status, sizeof(int) * ns));
+  FZ_CUDA(cudaStreamBeginCapture(b->master, cudaStreamCaptureModeThreadLocal));
+  FZ_CUDA(cudaEventRecord(b->ev_start, b->master));
+  for (int i = 0; i < ns; ++i) {
+    Engine* e = b->systems[i]->eng;
+    FZ_CUDA(cudaStreamWaitEvent(e->st, b->ev_start, 0));
+    const long long l0 = e->launches;
+    e->step_body();
+    e->launches = l0;
+    FZ_CUDA(cudaEventRecord(b->ev_done[i], e->st));
+    FZ_CUDA(cudaStreamWaitEvent(b->master, b->ev_done[i], 0));
+  }
+  FZ_CUDA(cudaStreamEndCapture(b->master, &b->graph));
+  FZ_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
+  return FZ_OK;
+}
+
+static long long step_launches(const Engine* e) {
+  return 2 + 11 + 1 + ((e->nbond + e->nangle + e->nub + e->ndihe + e->nimpr + e->nexcl + e->n14 > 0) ? 1 : 0) + 12;
+}
+
+extern "C" fz_status fz_batch_step(fz_batch* b, int nsteps) {
+  if (!b || nsteps < 0) return fail(FZ_ERR_ARG, "bad argument");
+  if (b->systems.empty() || nsteps == 0) return FZ_OK;
+  FZ_CUDA(cudaSetDevice(b->dev));
+  const int ns = (int)b->systems.size();
+  fz_status r;
+  if (!b->exec && (r = capture(b))) return r;
+  // work queued on the systems' own streams precedes the batch
+  for (int i = 0; i < ns; ++i) {
+    FZ_CUDA(cudaEventRecord(b->ev_done[i], b->systems[i]->eng->st));
+    FZ_CUDA(cudaStreamWaitEvent(b->master, b->ev_done[i], 0));
+  }
+  int left = nsteps;
+  while (left > 0) {
+    int k = left;
+    for (fz_system* s : b->systems) {
+      const Engine* e = s->eng;
+      if (e->temp_reset_every > 0) k = std::min<long long>(k, e->temp_reset_every - e->step % e->temp_reset_every);
+    }
+    for (int j = 0; j < k; ++j) FZ_CUDA(cudaGraphLaunch(b->exec, b->master));
+    for (int i = 0; i < ns; ++i) {
+      Engine* e = b->systems[i]->eng;
+      e->step += k;
+      e->launches += (long long)k * step_launches(e);
+      if (e->temp_reset_every > 0 && e->step % e->temp_reset_every == 0) {
+        FZ_CUDA(cudaEventRecord(b->ev_master, b->master));
+        FZ_CUDA(cudaStreamWaitEvent(e->st, b->ev_master, 0));
+        fzk::launch_reassign(e->int_args(), e->temperature, e->seed, (uint32_t)(e->step / e->temp_reset_every),
+                             e->inv_mtot, e->psum, e->st);
+        e->launches += 4;
+        FZ_CUDA(cudaEventRecord(b->ev_done[i], e->st));
+        FZ_CUDA(cudaStreamWaitEvent(b->master, b->ev_done[i], 0));
+      }
+    }
+    left -= k;
+  }
+  for (int i = 0; i < ns; ++i)
+    FZ_CUDA(cudaMemcpyAsync(b->pinned_status + i, b->systems[i]->eng->status, sizeof(int), cudaMemcpyDeviceToHost,
+                            b->master));
+  // later per-system work is ordered after the batch
+  FZ_CUDA(cudaEventRecord(b->ev_master, b->master));
+  for (fz_system* s : b->systems) FZ_CUDA(cudaStreamWaitEvent(s->eng->st, b->ev_master, 0));
+  FZ_CUDA(cudaStreamSynchronize(b->master));
+  for (int i = 0; i < ns; ++i)
+    if (b->pinned_status[i] && (r = b->systems[i]->eng->check()))
+      return fail(r, "system " + std::to_string(i) + " of the batch: " + last_error_text());
+  b->steps += nsteps;
+  return FZ_OK;
+}
+
+extern "C" fz_status fz_batch_size(fz_batch* b, int* out) {
+  if (!b || !out) return fail(FZ_ERR_ARG, "null argument");
+  *out = (int)b->systems.size();
+  return FZ_OK;
+}
+
+extern "C" fz_status fz_batch_free(fz_batch* b) {
+  delete b;
+  return FZ_OK;
+}
+
+// ====================================================================== serving loop
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Job {
+  int id = 0;
+  fz_system* sys = nullptr;
+  long long nsteps = 0, done = 0;
+  int state = 0;  // 0 queued, 1 running, 2 done, 3 failed
+  fz_status status = FZ_OK;
+  std::string err;
+  double t_submit = 0, t_start = -1, t_end = -1;
+  size_t est_bytes = 0;
+  fz_energies final{};
+  std::vector<double> pos;
+};
+
+// Device bytes of one uploaded system, an upper estimate of build_engine's allocations:
+// ~140 B per atom of atom, slot and PME-binning arrays, the per-block pair lists, masks
+// and work items (~0.5 B per atom per unit of list capacity, the capacity estimated as
+// build_engine does), the PME grids and charge staging (~24 B per grid point), and 8 MiB
+// of fixed overhead.
+size_t engine_bytes_estimate(const fz_system* s) {
+  const double n = (double)s->top.n;
+  const double V = s->cfg.box[0] * s->cfg.box[1] * s->cfg.box[2];
+  const double rho = n / V;
+  const double K3 = (double)s->cfg.pme_grid[0] * s->cfg.pme_grid[1] * s->cfg.pme_grid[2];
+  const double R = std::max(s->cfg.pairlistdist, s->cfg.cutoff);
+  const double a = 1.4 * std::cbrt(32.0 / rho);
+  const double vm = a * a * a + 6 * a * a * R + 3 * M_PI * a * R * R + 4.0 / 3.0 * M_PI * R * R * R;
+  const double ocap = std::max(256.0, 1.25 * rho * vm);
+  return (size_t)(n * (140.0 + 0.5 * ocap) + 24.0 * K3) + ((size_t)8 << 20);
+}
+
+}  // namespace
+
+struct fz_server {
+  int dev = 0;
+  size_t budget = 0;
+  int chunk = 100, max_running = 64;
+  Clock::time_point t0 = Clock::now();
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<int> queue;
+  std::unordered_map<int, std::unique_ptr<Job>> jobs;
+  int next_id = 1;
+  bool stop = false;
+  std::thread worker;
+  size_t in_use = 0;
+  int running_now = 0, peak_running = 0;
+  long long atom_steps = 0, finished = 0;
+  double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
+  void run();
+};
+
+void fz_server::run() {
+  cudaSetDevice(dev);
+  fz_batch* batch = nullptr;
+  fz_batch_create(&batch);
+  std::vector<Job*> running;
+  auto finish = [&](Job* j, fz_status st, const std::string& msg) {
+    if (j->sys->eng) {
+      fz_batch_remove(batch, j->sys);
+      destroy_engine(j->sys->eng);
+      j->sys->eng = nullptr;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    j->status = st;
+    j->err = msg;
+    j->state = st == FZ_OK ? 2 : 3;
+    j->t_end = now();
+    in_use -= j->est_bytes;
+    finished++;
+    cv_done.notify_all();
+  };
+  for (;;) {
+    std::vector<Job*> admit;
+    {
+      std::unique_lock<std::mutex> lock(mu);
+      for (;;) {
+        while (!queue.empty() && (int)(running.size() + admit.size()) < max_running) {
+          Job* j = jobs[queue.front()].get();
+          if (j->est_bytes > budget) {  // can never fit: fail it
+            queue.pop_front();
+            j->status = FZ_ERR_CAPACITY;
+            j->err = "job needs ~" + std::to_string(j->est_bytes >> 20) + " MiB, above the HBM budget";
+            j->state = 3;
+            j->t_end = now();
+            finished++;
+            cv_done.notify_all();
+            continue;
+          }
+          if (in_use + j->est_bytes > budget) break;  // FIFO: wait for memory
+          queue.pop_front();
+          in_use += j->est_bytes;
+          j->state = 1;
+          j->t_start = now();
+          admit.push_back(j);
+        }
+        if (!running.empty() || !admit.empty()) break;
+        if (stop) {
+          lock.unlock();
+          fz_batch_free(batch);
+          return;
+        }
+        cv_work.wait(lock);
+      }
+    }
+    for (Job* j : admit) {
+      // InitMem + InitVelocity of the reference's main (src/fenzi.cu:212-232): Maxwell-
+      // Boltzmann velocities at the input's temperature and seed
+      fz_status r = fz_upload(j->sys, dev, nullptr);
+      if (!r) r = fz_reassign_velocities(j->sys, j->sys->cfg.temperature, (uint64_t)j->sys->cfg.seed, 0);
+      if (!r) r = fz_batch_add(batch, j->sys);
+      if (r) {
+        finish(j, r, last_error_text());
+        continue;
+      }
+      running.push_back(j);
+    }
+    {
+      std::lock_guard<std::mutex> lock(mu);
+      running_now = (int)running.size();
+      peak_running = std::max(peak_running, running_now);
+    }
+    if (running.empty()) continue;
+    long long k = chunk;
+    for (Job* j : running) k = std::min(k, j->nsteps - j->done);
+    fz_status r = fz_batch_step(batch, (int)k);
+    if (r) {
+      // find the failing systems; the others continue
+      const std::string msg = last_error_text();
+      std::vector<Job*> keep;
+      for (Job* j : running) {
+        if (fz_sync(j->sys) != FZ_OK)
+          finish(j, FZ_ERR_CUDA, last_error_text());
+        else
+          keep.push_back(j);
+      }
+      if (keep.size() == running.size()) {  // not attributable: fail the whole mix
+        for (Job* j : running) finish(j, r, msg);
+        keep.clear();
+      }
+      running.swap(keep);
+      continue;
+    }
+    std::vector<Job*> keep;
+    for (Job* j : running) {
+      j->done += k;
+      {
+        std::lock_guard<std::mutex> lock(mu);
+        atom_steps += (long long)j->sys->top.n * k;
+      }
+      if (j->done < j->nsteps) {
+        keep.push_back(j);
+        continue;
+      }
+      fz_status st = fz_eval_props(j->sys, &j->final);
+      if (!st) {
+        j->pos.resize(3 * (size_t)j->sys->top.n);
+        st = fz_get_positions(j->sys, j->pos.data());
+      }
+      finish(j, st, st ? last_error_text() : std::string());
+    }
+    running.swap(keep);
+  }
+}
+
+extern "C" fz_status fz_server_estimate_bytes(const fz_system* sys, double* out) {
+  if (!sys || !out) return fail(FZ_ERR_ARG, "null argument");
+  *out = (double)engine_bytes_estimate(sys);
+  return FZ_OK;
+}
+
+extern "C" fz_status fz_server_create(int device, double hbm_budget_bytes, int chunk_steps, int max_running,
+                                      fz_server** out) {
+  if (!out) return fail(FZ_ERR_ARG, "null output");
+  if (!(hbm_budget_bytes > 0) || chunk_steps <= 0 || max_running <= 0)
+    return fail(FZ_ERR_ARG, "fz_server_create: budget, chunk and slots must be positive");
+  int ndev = 0;
+  cudaError_t ce = cudaGetDeviceCount(&ndev);
+  if (ce != cudaSuccess) return fail(FZ_ERR_CUDA, std::string("cudaGetDeviceCount: ") + cudaGetErrorString(ce));
+  if (device < 0 || device >= ndev) return fail(FZ_ERR_ARG, "fz_server_create: no such device");
+  fz_server* sv = new fz_server();
+  sv->dev = device;
+  sv->budget = (size_t)hbm_budget_bytes;
+  sv->chunk = chunk_steps;
+  sv->max_running = max_running;
+  sv->worker = std::thread([sv] { sv->run(); });
+  *out = sv;
+  return FZ_OK;
+}
+
+extern "C" fz_status fz_server_submit(fz_server* sv, fz_system* sys, long long nsteps, int* job_id) {
+  if (!sv || !sys || !job_id) return fail(FZ_ERR_ARG, "null argument");
+  if (nsteps <= 0) return fail(FZ_ERR_ARG, "fz_server_submit: nsteps must be positive");
+  if (sys->eng) return fail(FZ_ERR_STATE, "fz_server_submit: the server uploads the system itself");
+  std::unique_ptr<Job> j(new Job());
+  j->sys = sys;
+  j->nsteps = nsteps;
+  j->est_bytes = engine_bytes_estimate(sys);
+  std::lock_guard<std::mutex> lock(sv->mu);
+  if (sv->stop) return fail(FZ_ERR_STATE, "fz_server_submit: server is stopping");
+  j->id = sv->next_id++;
+  j->t_submit = sv->now();
+  *job_id = j->id;
+  sv->queue.push_back(j->id);
+  sv->jobs[j->id] = std::move(j);
+  sv->cv_work.notify_all();
+  return FZ_OK;
+}
+
+static void fill_info(const Job& j, fz_job_info* o) {
+  o->job = j.id;
+  o->state = j.state;
+  o->status = j.status;
+  o->nsteps = j.nsteps;
+  o->steps_done = j.done;
+  o->natom = j.sys->top.n;
+  o->submit_s = j.t_submit;
+  o->start_s = j.t_start;
+  o->end_s = j.t_end;
+  o->device_bytes = (double)j.est_bytes;
+  o->final = j.final;
+}
+
+extern "C" fz_status fz_server_info(fz_server* sv, int job_id, fz_job_info* out) {
+  if (!sv || !out) return fail(FZ_ERR_ARG, "null argument");
+  std::lock_guard<std::mutex> lock(sv->mu);
+  auto it = sv->jobs.find(job_id);
+  if (it == sv->jobs.end()) return fail(FZ_ERR_ARG, "fz_server_info: unknown job");
+  fill_info(*it->second, out);
+  return FZ_OK;
+}
+
+extern "C" fz_status fz_server_wait(fz_server* sv, int job_id, fz_job_info* out) {
+  if (!sv) return fail(FZ_ERR_ARG, "null argument");
+  std::unique_lock<std::mutex> lock(sv->mu);
+  auto it = sv->jobs.find(job_id);
+  if (it == sv->jobs.end()) return fail(FZ_ERR_ARG, "fz_server_wait: unknown job");
+  Job* j = it->second.get();
+  sv->cv_done.wait(lock, [j] { return j->state >= 2; });
+  if (out) fill_info(*j, out);
+  if (j->status) return fail(j->status, "job " + std::to_string(j->id) + ": " + j->err);
+  return FZ_OK;
+}
+
+extern "C" fz_status fz_server_positions(fz_server* sv, int job_id, double* out) {
+  if (!sv || !out) return fail(FZ_ERR_ARG, "null argument");
+  std::lock_guard<std::mutex> lock(sv->mu);
+  auto it = sv->jobs.find(job_id);
+  if (it == sv->jobs.end()) return fail(FZ_ERR_ARG, "fz_server_positions: unknown job");
+  if (it->second->state != 2) return fail(FZ_ERR_STATE, "fz_server_positions: job has not finished");
+  std::copy(it->second->pos.begin(), it->second->pos.end(), out);
+  return FZ_OK;
+}
+
+extern "C" fz_status fz_server_stats(fz_server* sv, double* out4) {
+  if (!sv || !out4) return fail(FZ_ERR_ARG, "null argument");
+  std::lock_guard<std::mutex> lock(sv->mu);
+  out4[0] = (double)sv->peak_running;
+  out4[1] = (double)sv->atom_steps;
+  out4[2] = (double)sv->in_use;
+  out4[3] = (double)sv->finished;
+  return FZ_OK;
+}
+
+extern "C" fz_status fz_server_free(fz_server* sv) {
+  if (!sv) return FZ_OK;
+  {
+    std::lock_guard<std::mutex> lock(sv->mu);
+    sv->stop = true;
+    sv->cv_work.notify_all();
+  }
+  if (sv->worker.joinable()) sv->worker.join();  // queued and running jobs finish first
+  for (auto& kv : sv->jobs) fz_free(kv.second->sys);
+  delete sv;
+  return FZ_OK;
+}

@@ -13,398 +13,9 @@
 //   grid float[K^3], cgrid float2[Kz*Ky*(Kx/2+1)] PME
 // A step is ~20 launches and no host synchronisation; fz_step checks the sticky
 // device status word once per call.
-#include <cmath>
-#include <cstdio>
-#include <cstdlib>
-#include <cstring>
-#include <string>
-#include <vector>
-
-#include "host/host.h"
-#include "kernels/kernels.h"
+#include "engine.h"
 
 namespace fz {
-
-#define FZ_CUDA(call)                                                                                  \
-  do {                                                                                                 \
-    cudaError_t e_ = (call);                                                                           \
-    if (e_ != cudaSuccess) return fail(FZ_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-  } while (0)
-
-struct Engine {
-  int dev = 0;
-  cudaStream_t st = nullptr;
-  bool own_stream = false;
-  fzk::SysParams p{};
-  int n = 0, nunits = 0, ncol = 0, nslots = 0, mask_cap = 0, all_images = 0;
-  int ocap = 0;            // per-block pair-list capacity (multiple of 32)
-  float rp2 = 0.f, prune_half2 = 0.f;
-  int nb_grid = 0;
-  int dcx = 1, dcy = 1;
-  int* blk_col = nullptr;
-  std::vector<void*> allocs;
-  // atoms
-  float4 *pos4 = nullptr, *vel4 = nullptr, *pos_build = nullptr;
-  long long *facc = nullptr, *energy = nullptr, *psum = nullptr;
-  int* type = nullptr;
-  // sorted slots / neighbour tiles
-  float4 *xyzq_s = nullptr, *bb_lo = nullptr, *bb_hi = nullptr;
-  int *typ_s = nullptr, *perm = nullptr, *inv_perm = nullptr, *col_of = nullptr, *col_count = nullptr,
-      *col_cursor = nullptr, *col_start = nullptr, *col_tmp = nullptr;
-  uint32_t *outer = nullptr, *inner = nullptr, *masks = nullptr, *dmask = nullptr;
-  int *outer_n = nullptr, *inner_nt = nullptr, *inner_m = nullptr, *flag_prune = nullptr;
-  float4* pos_prune = nullptr;
-  int2* items = nullptr;
-  int chunk = 16;
-  int *excl_off = nullptr, *excl_idx = nullptr;
-  int *flag = nullptr, *counters = nullptr, *status = nullptr;
-  float2 *ljtab = nullptr, *lj14 = nullptr;
-  // bonded
-  int nbond = 0, nangle = 0, nub = 0, ndihe = 0, nimpr = 0, nexcl = 0, n14 = 0;
-  int2 *bond = nullptr, *ub = nullptr, *excl = nullptr, *p14 = nullptr;
-  int4 *angle = nullptr, *dihe = nullptr, *impr = nullptr;
-  float2 *bond_prm = nullptr, *angle_prm = nullptr, *ub_prm = nullptr, *impr_prm = nullptr;
-  float4* dihe_prm = nullptr;
-  // integration units
-  int4* unit_atoms = nullptr;
-  int* unit_meta = nullptr;
-  float4* unit_d = nullptr;
-  // PME
-  int K[3] = {0, 0, 0}, B[3] = {0, 0, 0}, nbk[3] = {0, 0, 0};
-  int *brick_of = nullptr, *brick_count = nullptr, *brick_cursor = nullptr, *brick_start = nullptr,
-      *brick_atoms = nullptr;
-  float* grid = nullptr;
-  int* qgrid = nullptr;
-  float2* cgrid = nullptr;
-  float2* tw[3] = {nullptr, nullptr, nullptr};
-  float *gfac[3] = {nullptr, nullptr, nullptr}, *f2[3] = {nullptr, nullptr, nullptr};
-  float gscale = 0.f;
-  // run state
-  bool forces_valid = false;
-  long long step = 0;
-  double self_energy = 0, inv_mtot = 0, dtu = 0, shake_tol = 1e-10;
-  double box_d[3] = {0, 0, 0};
-  int ncons = 0;
-  int temp_reset_every = 0;
-  double temperature = 300.0;
-  unsigned long long seed = 0;
-  long long launches = 0;
-  // per-stage timing
-  bool timing = false;
-  cudaEvent_t ev[12] = {};
-  double stage_ms[5] = {0, 0, 0, 0, 0};
-  long long timed_steps = 0;
-  // CUDA graph of one MD step (kick/drift/SHAKE, neighbour maintenance, forces,
-  // kick/RATTLE); captured on first use, replayed with one launch per step
-  cudaGraph_t step_graph = nullptr;
-  cudaGraphExec_t step_exec = nullptr;
-  bool use_graph = true;
-  // PME runs on a second stream concurrently with the pair and bonded kernels
-  cudaStream_t st2 = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-  // pinned staging
-  void* pinned = nullptr;
-  size_t pinned_bytes = 0;
-
-  template <class T>
-  fz_status alloc(T** ptr, size_t count) {
-    *ptr = nullptr;
-    if (count == 0) count = 1;
-    void* p = nullptr;
-    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
-    if (e != cudaSuccess) return fail(FZ_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-    allocs.push_back(p);
-    e = cudaMemsetAsync(p, 0, count * sizeof(T), st);
-    if (e != cudaSuccess) return fail(FZ_ERR_CUDA, std::string("cudaMemset: ") + cudaGetErrorString(e));
-    *ptr = static_cast<T*>(p);
-    return FZ_OK;
-  }
-  template <class T>
-  fz_status upload(T** ptr, const std::vector<T>& v) {
-    fz_status s = alloc(ptr, v.size());
-    if (s) return s;
-    if (!v.empty()) FZ_CUDA(cudaMemcpyAsync(*ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
-    return FZ_OK;
-  }
-  void release(void* ptr) {
-    for (auto& a : allocs)
-      if (a == ptr) {
-        cudaFree(a);
-        a = allocs.back();
-        allocs.pop_back();
-        return;
-      }
-  }
-  fz_status staging(size_t bytes) {
-    if (pinned_bytes >= bytes) return FZ_OK;
-    if (pinned) cudaFreeHost(pinned);
-    pinned = nullptr;
-    FZ_CUDA(cudaMallocHost(&pinned, bytes));
-    pinned_bytes = bytes;
-    return FZ_OK;
-  }
-  ~Engine() {
-    if (st) cudaStreamSynchronize(st);
-    if (step_exec) cudaGraphExecDestroy(step_exec);
-    if (step_graph) cudaGraphDestroy(step_graph);
-    if (ev_fork) cudaEventDestroy(ev_fork);
-    if (ev_join) cudaEventDestroy(ev_join);
-    if (st2) cudaStreamDestroy(st2);
-    for (auto& x : ev)
-      if (x) cudaEventDestroy(x);
-    for (void* p : allocs) cudaFree(p);
-    if (pinned) cudaFreeHost(pinned);
-    if (own_stream && st) cudaStreamDestroy(st);
-  }
-
-  fzk::RebuildArgs rebuild_args() const {
-    fzk::RebuildArgs a{};
-    a.p = p;
-    a.flag = flag;
-    a.counters = counters;
-    a.status = status;
-    a.pos4 = pos4;
-    a.pos_build = pos_build;
-    a.type = type;
-    a.col_of = col_of;
-    a.col_count = col_count;
-    a.col_cursor = col_cursor;
-    a.col_start = col_start;
-    a.col_tmp = col_tmp;
-    a.perm = perm;
-    a.inv_perm = inv_perm;
-    a.xyzq_s = xyzq_s;
-    a.typ_s = typ_s;
-    a.bb_lo = bb_lo;
-    a.bb_hi = bb_hi;
-    a.excl_off = excl_off;
-    a.excl_idx = excl_idx;
-    a.masks = masks;
-    a.mask_cap = mask_cap;
-    a.all_images = all_images;
-    a.outer = outer;
-    a.outer_n = outer_n;
-    a.inner = inner;
-    a.inner_nt = inner_nt;
-    a.inner_m = inner_m;
-    a.dmask = dmask;
-    a.ocap = ocap;
-    a.flag_prune = flag_prune;
-    a.rp2 = rp2;
-    a.pos_prune = pos_prune;
-    a.items = items;
-    a.chunk = chunk;
-    a.blk_col = blk_col;
-    a.dcx = dcx;
-    a.dcy = dcy;
-    return a;
-  }
-  fzk::NonbondedArgs nb_args() const {
-    fzk::NonbondedArgs a{};
-    a.p = p;
-    a.xyzq_s = xyzq_s;
-    a.typ_s = typ_s;
-    a.perm = perm;
-    a.inner = inner;
-    a.inner_nt = inner_nt;
-    a.inner_m = inner_m;
-    a.dmask = dmask;
-    a.masks = masks;
-    a.counters = counters;
-    a.ljtab = ljtab;
-    a.facc = facc;
-    a.energy = energy;
-    a.ocap = ocap;
-    a.items = items;
-    a.chunk = chunk;
-    a.grid = nb_grid;
-    return a;
-  }
-  fzk::PmeArgs pme_args() const {
-    fzk::PmeArgs a{};
-    a.p = p;
-    a.pos4 = pos4;
-    a.n = n;
-    for (int d = 0; d < 3; ++d) {
-      a.K[d] = K[d];
-      a.B[d] = B[d];
-      a.nb[d] = nbk[d];
-      a.tw[d] = tw[d];
-      a.gfac[d] = gfac[d];
-      a.f2[d] = f2[d];
-    }
-    a.brick_of = brick_of;
-    a.brick_count = brick_count;
-    a.brick_cursor = brick_cursor;
-    a.brick_start = brick_start;
-    a.brick_atoms = brick_atoms;
-    a.grid = grid;
-    a.qgrid = qgrid;
-    a.cgrid = cgrid;
-    a.gscale = gscale;
-    a.facc = facc;
-    a.energy = energy;
-    a.status = status;
-    return a;
-  }
-  fzk::BondedArgs bonded_args() const {
-    fzk::BondedArgs a{};
-    a.p = p;
-    a.pos4 = pos4;
-    a.nbond = nbond;
-    a.nangle = nangle;
-    a.nub = nub;
-    a.ndihe = ndihe;
-    a.nimpr = nimpr;
-    a.nexcl = nexcl;
-    a.n14 = n14;
-    a.bond = bond;
-    a.bond_prm = bond_prm;
-    a.angle = angle;
-    a.angle_prm = angle_prm;
-    a.ub = ub;
-    a.ub_prm = ub_prm;
-    a.dihe = dihe;
-    a.dihe_prm = dihe_prm;
-    a.impr = impr;
-    a.impr_prm = impr_prm;
-    a.excl = excl;
-    a.p14 = p14;
-    a.type = type;
-    a.lj14 = lj14;
-    a.facc = facc;
-    a.energy = energy;
-    return a;
-  }
-  fzk::IntegrateArgs int_args() const {
-    fzk::IntegrateArgs a{};
-    a.p = p;
-    a.nunits = nunits;
-    a.unit_atoms = unit_atoms;
-    a.unit_meta = unit_meta;
-    a.unit_d = unit_d;
-    a.pos4 = pos4;
-    a.vel4 = vel4;
-    a.facc = facc;
-    a.xyzq_s = xyzq_s;
-    a.inv_perm = inv_perm;
-    a.pos_build = pos_build;
-    a.pos_prune = pos_prune;
-    a.flag = flag;
-    a.flag_prune = flag_prune;
-    a.prune_half2 = prune_half2;
-    a.status = status;
-    a.energy = energy;
-    a.dtu = dtu;
-    for (int d = 0; d < 3; ++d) {
-      a.box_d[d] = box_d[d];
-      a.inv_box_d[d] = 1.0 / box_d[d];
-    }
-    a.shake_tol = shake_tol;
-    a.shake_maxit = 500;
-    return a;
-  }
-
-  // ---------------------------------------------------------------- step pieces
-  void mark(int k) {
-    if (timing) cudaEventRecord(ev[k], st);
-  }
-  void forces(bool energies, int terms = FZ_TERM_ALL) {
-    mark(1);
-    fzk::launch_rebuild(rebuild_args(), st);
-    launches += 11;
-    mark(2);
-    if (terms & FZ_TERM_NONBONDED) {
-      fzk::launch_nonbonded(nb_args(), energies, st);
-      launches += 1;
-    }
-    mark(3);
-    if (terms & FZ_TERM_BONDED) {
-      fzk::launch_bonded(bonded_args(), energies, st);
-      launches += (nbond + nangle + nub + ndihe + nimpr + nexcl + n14 > 0) ? 1 : 0;
-    }
-    mark(4);
-    if (terms & FZ_TERM_PME) {
-      fzk::launch_pme(pme_args(), energies, st);
-      launches += 11;
-    }
-    mark(5);
-  }
-  // accumulates the events of one timed step: 0 start, 1..5 forces, 6 end
-  void collect_step() {
-    cudaEventSynchronize(ev[6]);
-    float ms = 0.f;
-    auto el = [&](int a, int b) {
-      cudaEventElapsedTime(&ms, ev[a], ev[b]);
-      return (double)ms;
-    };
-    stage_ms[0] += el(1, 2);
-    stage_ms[1] += el(2, 3);
-    stage_ms[2] += el(3, 4);
-    stage_ms[3] += el(4, 5);
-    stage_ms[4] += el(0, 1) + el(5, 6);
-    timed_steps++;
-  }
-  // forces with PME on st2, overlapping the pair and bonded kernels on st
-  void forces_overlapped() {
-    fzk::launch_rebuild(rebuild_args(), st);
-    cudaEventRecord(ev_fork, st);
-    cudaStreamWaitEvent(st2, ev_fork, 0);
-    fzk::launch_pme(pme_args(), false, st2);
-    fzk::launch_nonbonded(nb_args(), false, st);
-    fzk::launch_bonded(bonded_args(), false, st);
-    cudaEventRecord(ev_join, st2);
-    cudaStreamWaitEvent(st, ev_join, 0);
-  }
-  void step_body() {
-    const fzk::IntegrateArgs ia = int_args();
-    fzk::launch_kick_drift(ia, st);
-    if (st2)
-      forces_overlapped();
-    else
-      forces(false);
-    fzk::launch_kick_rattle(ia, false, true, st);
-  }
-  fz_status graph_step() {
-    if (!step_exec) {
-      FZ_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-      const long long l0 = launches;
-      step_body();
-      launches = l0;
-      cudaGraph_t g = nullptr;
-      FZ_CUDA(cudaStreamEndCapture(st, &g));
-      step_graph = g;
-      FZ_CUDA(cudaGraphInstantiate(&step_exec, step_graph, 0));
-    }
-    FZ_CUDA(cudaGraphLaunch(step_exec, st));
-    launches += 2 + 11 + 1 + ((nbond + nangle + nub + ndihe + nimpr + nexcl + n14 > 0) ? 1 : 0) + 11;
-    return FZ_OK;
-  }
-  void drop_graph() {
-    if (step_exec) cudaGraphExecDestroy(step_exec);
-    if (step_graph) cudaGraphDestroy(step_graph);
-    step_exec = nullptr;
-    step_graph = nullptr;
-  }
-  fz_status check() {
-    int h = 0;
-    FZ_CUDA(cudaMemcpyAsync(&h, status, sizeof(int), cudaMemcpyDeviceToHost, st));
-    FZ_CUDA(cudaStreamSynchronize(st));
-    FZ_CUDA(cudaGetLastError());
-    if (h) {
-      std::string m = "device status:";
-      if (h & fzk::ST_TILE_OVERFLOW) m += " pair-tile capacity exceeded;";
-      if (h & fzk::ST_MASK_OVERFLOW) m += " exclusion-mask capacity exceeded;";
-      if (h & fzk::ST_SLOT_OVERFLOW) m += " sorted-slot capacity exceeded;";
-      if (h & fzk::ST_COLUMN_OVERFLOW) m += " column occupancy exceeded;";
-      if (h & fzk::ST_SHAKE_NOCONV) m += " SHAKE did not converge within its iteration cap;";
-      if (h & fzk::ST_BAD_COORD) m += " non-finite or runaway coordinates;";
-      const int code = (h & fzk::ST_SHAKE_NOCONV) ? FZ_ERR_SHAKE : FZ_ERR_CAPACITY;
-      return fail(code, m);
-    }
-    return FZ_OK;
-  }
-};
 
 void destroy_engine(Engine* e) { delete e; }
 
@@ -491,6 +102,15 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
   // column offsets whose x-y rectangles can lie within the pair-list radius
   e->dcx = std::min(ncx, (int)std::ceil(plist / (c.box[0] / ncx)));
   e->dcy = std::min(ncy, (int)std::ceil(plist / (c.box[1] / ncy)));
+  e->ncx = ncx;
+  e->ncy = ncy;
+  e->col_a = a;
+  e->plist = plist;
+  e->cutoff = rc;
+  for (int d = 0; d < 3; ++d) e->ratio[d] = c.box[d] / c.box[0];
+  e->L_build = e->L_prune = c.box[0];
+  e->pmass = c.pmass;
+  e->pref_atm = c.pref;
   e->nslots = ((n + 32 * e->ncol + 64 + 31) / 32) * 32;
   p.nslots = e->nslots;
   for (int d = 0; d < 3; ++d) {
@@ -510,6 +130,9 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
     const double delta = std::min(0.3, plist - c.cutoff);
     e->rp2 = (float)((c.cutoff + delta) * (c.cutoff + delta));
     e->prune_half2 = (float)(0.25 * delta * delta);
+    e->prune_delta = delta;
+    e->prune_half2_nve = e->prune_half2;
+    e->skin_half2_nve = p.skin_half2;
   }
   e->dtu = c.timestep_ps * kTU;
   e->shake_tol = c.shake_tol > 0 ? c.shake_tol : 1e-10;
@@ -652,7 +275,7 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
     if ((r = e->alloc(&e->brick_of, n)) || (r = e->alloc(&e->brick_count, nbr)) ||
         (r = e->alloc(&e->brick_cursor, nbr)) || (r = e->alloc(&e->brick_start, nbr + 1)) ||
         (r = e->alloc(&e->brick_atoms, n)) || (r = e->alloc(&e->grid, (size_t)Kx * Ky * Kz)) ||
-        (r = e->alloc(&e->qgrid, (size_t)Kx * Ky * Kz)) ||
+        (r = e->alloc(&e->stage, (size_t)nbr * (e->B[0] + 3) * (e->B[1] + 3) * (e->B[2] + 3))) ||
         (r = e->alloc(&e->cgrid, (size_t)Kz * Ky * (Kx / 2 + 1))))
       return r;
     const double b2 = c.kappa * c.kappa;
@@ -718,6 +341,138 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
   return e->check();
 }
 
+// ---------------------------------------------------------------- barostat
+constexpr double kPatm = 68558.64100846418;     // kcal/mol/A^3 -> atm (src/cell_based_kernels.cu:584)
+
+// Moves the engine to a new box (x edge L, aspect ratios kept): parameters passed by
+// value to the kernels, the column search reach, and the PME influence tables.
+static fz_status set_box(Engine* e, double L) {
+  fzk::SysParams& p = e->p;
+  for (int d = 0; d < 3; ++d) e->box_d[d] = L * e->ratio[d];
+  const double lmin = std::min(e->box_d[0], std::min(e->box_d[1], e->box_d[2]));
+  if (e->cutoff >= 0.5 * lmin) return fail(FZ_ERR_STATE, "barostat: box shrank below twice the cutoff");
+  p.box = make_float3((float)e->box_d[0], (float)e->box_d[1], (float)e->box_d[2]);
+  p.inv_box = make_float3((float)(1.0 / e->box_d[0]), (float)(1.0 / e->box_d[1]), (float)(1.0 / e->box_d[2]));
+  const double V = e->box_d[0] * e->box_d[1] * e->box_d[2];
+  e->gscale = (float)(kCC / (M_PI * V));
+  e->dcx = std::min(e->ncx, (int)std::ceil(e->plist / (e->box_d[0] / e->ncx)));
+  e->dcy = std::min(e->ncy, (int)std::ceil(e->plist / (e->box_d[1] / e->ncy)));
+  const double colw = std::max(e->box_d[0] / e->ncx, e->box_d[1] / e->ncy);
+  e->all_images = (0.5 * lmin < e->plist + 3.0 * std::max(colw, e->col_a)) ? 1 : 0;
+  const int ktot = e->K[0] + e->K[1] + e->K[2];
+  if (!e->pme_tab_host) FZ_CUDA(cudaMallocHost(&e->pme_tab_host, sizeof(float) * 2 * ktot));
+  // the previous step's table copies have completed: barostat steps synchronise each step
+  const double b2 = (double)p.beta * (double)p.beta;
+  float* h = e->pme_tab_host;
+  for (int d = 0; d < 3; ++d) {
+    const int Kd = e->K[d];
+    float* g = h;
+    float* ff = h + Kd;
+    for (int m = 0; m < Kd; ++m) {
+      const double f = (m <= Kd / 2 ? m : m - Kd) / e->box_d[d];
+      ff[m] = (float)(f * f);
+      g[m] = (float)(bmod2(m, Kd) * std::exp(-M_PI * M_PI * f * f / b2));
+    }
+    FZ_CUDA(cudaMemcpyAsync(e->gfac[d], g, sizeof(float) * Kd, cudaMemcpyHostToDevice, e->st));
+    FZ_CUDA(cudaMemcpyAsync(e->f2[d], ff, sizeof(float) * Kd, cudaMemcpyHostToDevice, e->st));
+    h += 2 * Kd;
+  }
+  return FZ_OK;
+}
+
+// host copy of the energy slots and the cumulative list counters (synchronises)
+static fz_status read_slots(Engine* e, long long* en, int* cnt) {
+  FZ_CUDA(cudaMemcpyAsync(en, e->energy, sizeof(long long) * fzk::EN_COUNT, cudaMemcpyDeviceToHost, e->st));
+  if (cnt) FZ_CUDA(cudaMemcpyAsync(cnt, e->counters, sizeof(int) * fzk::CNT_COUNT, cudaMemcpyDeviceToHost, e->st));
+  return e->check();
+}
+
+static double volume(const Engine* e) { return e->box_d[0] * e->box_d[1] * e->box_d[2]; }
+
+// piston acceleration for the instantaneous pressure P (kcal/mol/A^3)
+static double piston_accel(const Engine* e, double P) {
+  const double L = e->box_d[0];
+  return (P - e->pref_atm * kPU) / (3.0 * e->pmass * L * L) - 2.0 * e->Ldot * e->Ldot / L;
+}
+
+// Forces + energies + virial of the current state and its instantaneous pressure
+// (kcal/mol/A^3).  Atomic form (fz_eval_props): all kinetic energy, the force virial and
+// the instantaneous constraint virial.  Group form (barostat): the kinetic energy of the
+// unit centres and the virial of the unit centres.
+static fz_status state_pressure(Engine* e, long long* en, double* P, bool group) {
+  FZ_CUDA(cudaMemsetAsync(e->facc, 0, 3 * sizeof(long long) * e->n, e->st));
+  FZ_CUDA(cudaMemsetAsync(e->energy, 0, fzk::EN_COUNT * sizeof(long long), e->st));
+  e->forces(true);
+  e->forces_valid = true;
+  const fzk::IntegrateArgs ia = e->int_args();
+  fzk::launch_kinetic(ia, e->st);
+  if (group)
+    fzk::launch_unit_virial(ia, e->st);
+  else if (e->ncons)
+    fzk::launch_constraint_virial(ia, e->st);
+  fz_status r;
+  if ((r = read_slots(e, en, nullptr))) return r;
+  const double s = 1.0 / fzk::kFixE;
+  const double W = (en[fzk::EN_VIR_X] + en[fzk::EN_VIR_Y] + en[fzk::EN_VIR_Z]) * s;
+  const double K = (group ? en[fzk::EN_KIN_HALF] : en[fzk::EN_KIN]) * s;
+  *P = (2.0 * K + W) / (3.0 * volume(e));
+  return FZ_OK;
+}
+
+// One barostat step: piston half kick, box drift with rigid scaling of every
+// integration unit's mass centre, kick/drift/SHAKE, forces at the new box, pressure of
+// the unit centres from the half-step velocities (the reference's ScanVirial placement,
+// src/dynamics.cu:773-776), piston half kick, kick/RATTLE.  Peculiar centre-of-mass
+// velocities feel the friction exp(-L'/L dt/2) in each half kick (Andersen, J. Chem.
+// Phys. 72, 2384 (1980), with the units as scaling groups; constraint forces act
+// inside a unit and do not enter the group virial).
+static fz_status npt_step(Engine* e) {
+  const double dt = e->dtu;
+  const double L = e->box_d[0];
+  e->Ldot += 0.5 * dt * e->Lacc;
+  const double Ln = L + dt * e->Ldot;
+  if (!(Ln > 0.0) || !std::isfinite(Ln)) return fail(FZ_ERR_STATE, "barostat: box length diverged");
+  fz_status r;
+  if ((r = set_box(e, Ln))) return r;
+  // list validity: periodic image shifts move with the box, by up to sqrt(3) dL
+  const double rmax = std::max(e->ratio[0], std::max(e->ratio[1], e->ratio[2]));
+  const double mb = 0.05 * (e->plist - e->cutoff), mp = 0.1 * e->prune_delta;
+  const int one = 1;
+  if (std::sqrt(3.0) * std::fabs(Ln - e->L_build) * rmax > 2.0 * mb)
+    FZ_CUDA(cudaMemcpyAsync(e->flag, &one, sizeof(int), cudaMemcpyHostToDevice, e->st));
+  else if (std::sqrt(3.0) * std::fabs(Ln - e->L_prune) * rmax > 2.0 * mp)
+    FZ_CUDA(cudaMemcpyAsync(e->flag_prune, &one, sizeof(int), cudaMemcpyHostToDevice, e->st));
+  FZ_CUDA(cudaMemsetAsync(e->energy, 0, fzk::EN_COUNT * sizeof(long long), e->st));
+  fzk::IntegrateArgs ia = e->int_args();
+  ia.lam = Ln / L;
+  ia.vfric = std::exp(-0.5 * dt * e->Ldot / L);
+  fzk::launch_kick_drift_npt(ia, e->st);
+  e->forces(true);
+  fzk::launch_unit_virial(ia, e->st);
+  long long en[fzk::EN_COUNT];
+  int cnt[fzk::CNT_COUNT];
+  if ((r = read_slots(e, en, cnt))) return r;
+  if (cnt[fzk::CNT_REBUILDS] != e->seen_rebuilds) {
+    e->seen_rebuilds = cnt[fzk::CNT_REBUILDS];
+    e->L_build = e->L_prune = Ln;
+  }
+  if (cnt[fzk::CNT_PRUNES] != e->seen_prunes) {
+    e->seen_prunes = cnt[fzk::CNT_PRUNES];
+    e->L_prune = Ln;
+  }
+  const double s = 1.0 / fzk::kFixE;
+  const double W = (en[fzk::EN_VIR_X] + en[fzk::EN_VIR_Y] + en[fzk::EN_VIR_Z]) * s;
+  const double P = (2.0 * en[fzk::EN_KIN_HALF] * s + W) / (3.0 * volume(e));
+  e->last_pressure = P * kPatm;
+  e->Lacc = piston_accel(e, P);
+  e->Ldot += 0.5 * dt * e->Lacc;
+  ia = e->int_args();
+  ia.vfric = std::exp(-0.5 * dt * e->Ldot / Ln);
+  fzk::launch_kick_rattle(ia, false, true, e->st);
+  e->launches += 4 + 11 + 1 + ((e->nbond + e->nangle + e->nub + e->ndihe + e->nimpr + e->nexcl + e->n14 > 0) ? 1 : 0) + 12;
+  return FZ_OK;
+}
+
 }  // namespace fz
 
 using namespace fz;
@@ -772,7 +527,9 @@ extern "C" fz_status fz_step(fz_system* s, int nsteps) {
   }
   const fzk::IntegrateArgs ia = e->int_args();
   for (int k = 0; k < nsteps; ++k) {
-    if (e->use_graph && !e->timing) {
+    if (e->npt) {
+      if ((r = npt_step(e))) return r;
+    } else if (e->use_graph && !e->timing) {
       if ((r = e->graph_step())) return r;
     } else {
       e->mark(0);
@@ -785,7 +542,7 @@ extern "C" fz_status fz_step(fz_system* s, int nsteps) {
     }
     e->step++;
     if (e->temp_reset_every > 0 && e->step % e->temp_reset_every == 0) {
-      fzk::launch_reassign(ia, e->temperature, e->seed, (uint32_t)(e->step / e->temp_reset_every), e->inv_mtot,
+      fzk::launch_reassign(e->npt ? e->int_args() : ia, e->temperature, e->seed, (uint32_t)(e->step / e->temp_reset_every), e->inv_mtot,
                            e->psum, e->st);
       e->launches += 4;
     }
@@ -806,14 +563,9 @@ extern "C" fz_status fz_eval_props(fz_system* s, fz_energies* out) {
   if (!out) return fail(FZ_ERR_ARG, "null output");
   if ((r = need_engine(s))) return r;
   Engine* e = s->eng;
-  FZ_CUDA(cudaMemsetAsync(e->facc, 0, 3 * sizeof(long long) * e->n, e->st));
-  FZ_CUDA(cudaMemsetAsync(e->energy, 0, fzk::EN_COUNT * sizeof(long long), e->st));
-  e->forces(true);
-  e->forces_valid = true;
-  fzk::launch_kinetic(e->int_args(), e->st);
   long long en[fzk::EN_COUNT];
-  FZ_CUDA(cudaMemcpyAsync(en, e->energy, sizeof(en), cudaMemcpyDeviceToHost, e->st));
-  if ((r = e->check())) return r;
+  double P = 0.0;
+  if ((r = state_pressure(e, en, &P, false))) return r;
   const double s_ = 1.0 / fzk::kFixE;
   std::memset(out, 0, sizeof(*out));
   out->bond = en[fzk::EN_BOND] * s_;
@@ -831,7 +583,55 @@ extern "C" fz_status fz_eval_props(fz_system* s, fz_energies* out) {
   out->kinetic = en[fzk::EN_KIN] * s_;
   const double dof = 3.0 * e->n - 6.0 - e->ncons;  // src/evalprops.cu:225
   out->temperature = dof > 0 ? 2.0 * out->kinetic / (kRC * dof) : 0.0;
+  out->virial[0] = en[fzk::EN_VIR_X] * s_;
+  out->virial[1] = en[fzk::EN_VIR_Y] * s_;
+  out->virial[2] = en[fzk::EN_VIR_Z] * s_;
+  out->pressure_atm = P * kPatm;
   out->step = e->step;
+  for (int d = 0; d < 3; ++d) out->box[d] = e->box_d[d];
+  out->volume = volume(e);
+  out->conserved = out->potential + out->kinetic;
+  if (e->npt) {
+    const double rho = e->ratio[1] * e->ratio[2], L = e->box_d[0];
+    const double vdot = 3.0 * L * L * e->Ldot;
+    out->conserved += e->pref_atm * kPU * out->volume + 0.5 * e->pmass * rho * vdot * vdot;
+  }
+  return FZ_OK;
+}
+
+extern "C" fz_status fz_set_barostat(fz_system* s, int enable, double pref_atm, double pmass) {
+  fz_status r;
+  if ((r = need_engine(s))) return r;
+  Engine* e = s->eng;
+  if (enable && !(pmass > 0.0)) return fail(FZ_ERR_ARG, "fz_set_barostat: piston mass must be positive");
+  e->drop_graph();
+  if (!enable) {
+    e->npt = false;
+    e->p.skin_half2 = e->skin_half2_nve;
+    e->prune_half2 = e->prune_half2_nve;
+    e->Ldot = e->Lacc = 0.0;
+    return FZ_OK;
+  }
+  e->pref_atm = pref_atm;
+  e->pmass = pmass;
+  // tighter displacement triggers leave room for the image shifts of a moving box
+  const double skin = e->plist - e->cutoff;
+  e->p.skin_half2 = (float)std::pow(0.5 * skin - 0.05 * skin, 2);
+  e->prune_half2 = (float)std::pow(0.5 * e->prune_delta - 0.1 * e->prune_delta, 2);
+  const int one = 1;
+  FZ_CUDA(cudaMemcpyAsync(e->flag, &one, sizeof(int), cudaMemcpyHostToDevice, e->st));
+  long long en[fzk::EN_COUNT];
+  double P = 0.0;
+  if ((r = state_pressure(e, en, &P, true))) return r;
+  int cnt[fzk::CNT_COUNT];
+  if ((r = read_slots(e, en, cnt))) return r;
+  e->seen_rebuilds = cnt[fzk::CNT_REBUILDS];
+  e->seen_prunes = cnt[fzk::CNT_PRUNES];
+  e->L_build = e->L_prune = e->box_d[0];
+  if (!e->npt) e->Ldot = 0.0;
+  e->npt = true;
+  e->last_pressure = P * kPatm;
+  e->Lacc = piston_accel(e, P);
   return FZ_OK;
 }
 
@@ -949,6 +749,17 @@ extern "C" fz_status fz_get_state_f32(fz_system* s, float* pos, float* vel) {
     FZ_CUDA(cudaMemcpy2DAsync(vel, 3 * sizeof(float), e->vel4, sizeof(float4), 3 * sizeof(float), e->n,
                               cudaMemcpyDeviceToHost, e->st));
   FZ_CUDA(cudaStreamSynchronize(e->st));
+  return FZ_OK;
+}
+
+extern "C" fz_status fz_get_virial(fz_system* s, double* out3) {
+  fz_status r;
+  if ((r = need_engine(s))) return r;
+  if (!out3) return fail(FZ_ERR_ARG, "null output");
+  Engine* e = s->eng;
+  long long en[fzk::EN_COUNT];
+  if ((r = read_slots(e, en, nullptr))) return r;
+  for (int d = 0; d < 3; ++d) out3[d] = en[fzk::EN_VIR_X + d] / fzk::kFixE;
   return FZ_OK;
 }
 

@@ -1,0 +1,416 @@
+// Device engine of one system: its HBM state, kernel argument builders and the step
+// pieces queued on its stream.  Shared by the single-system C ABI (engine.cu) and the
+// batched ensemble / serving loop (batch.cu).
+#pragma once
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "host/host.h"
+#include "kernels/kernels.h"
+
+namespace fz {
+
+#define FZ_CUDA(call)                                                                                  \
+  do {                                                                                                 \
+    cudaError_t e_ = (call);                                                                           \
+    if (e_ != cudaSuccess) return fail(FZ_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+struct Engine {
+  int dev = 0;
+  cudaStream_t st = nullptr;
+  bool own_stream = false;
+  fzk::SysParams p{};
+  int n = 0, nunits = 0, ncol = 0, nslots = 0, mask_cap = 0, all_images = 0;
+  int ocap = 0;            // per-block pair-list capacity (multiple of 32)
+  float rp2 = 0.f, prune_half2 = 0.f;
+  int nb_grid = 0;
+  int dcx = 1, dcy = 1;
+  int* blk_col = nullptr;
+  std::vector<void*> allocs;
+  // atoms
+  float4 *pos4 = nullptr, *vel4 = nullptr, *pos_build = nullptr;
+  long long *facc = nullptr, *energy = nullptr, *psum = nullptr;
+  int* type = nullptr;
+  // sorted slots / neighbour tiles
+  float4 *xyzq_s = nullptr, *bb_lo = nullptr, *bb_hi = nullptr;
+  int *typ_s = nullptr, *perm = nullptr, *inv_perm = nullptr, *col_of = nullptr, *col_count = nullptr,
+      *col_cursor = nullptr, *col_start = nullptr, *col_tmp = nullptr;
+  uint32_t *outer = nullptr, *inner = nullptr, *masks = nullptr, *dmask = nullptr;
+  int *outer_n = nullptr, *inner_nt = nullptr, *inner_m = nullptr, *flag_prune = nullptr;
+  float4* pos_prune = nullptr;
+  int2* items = nullptr;
+  int chunk = 16;
+  int *excl_off = nullptr, *excl_idx = nullptr;
+  int *flag = nullptr, *counters = nullptr, *status = nullptr;
+  float2 *ljtab = nullptr, *lj14 = nullptr;
+  // bonded
+  int nbond = 0, nangle = 0, nub = 0, ndihe = 0, nimpr = 0, nexcl = 0, n14 = 0;
+  int2 *bond = nullptr, *ub = nullptr, *excl = nullptr, *p14 = nullptr;
+  int4 *angle = nullptr, *dihe = nullptr, *impr = nullptr;
+  float2 *bond_prm = nullptr, *angle_prm = nullptr, *ub_prm = nullptr, *impr_prm = nullptr;
+  float4* dihe_prm = nullptr;
+  // integration units
+  int4* unit_atoms = nullptr;
+  int* unit_meta = nullptr;
+  float4* unit_d = nullptr;
+  // PME
+  int K[3] = {0, 0, 0}, B[3] = {0, 0, 0}, nbk[3] = {0, 0, 0};
+  int *brick_of = nullptr, *brick_count = nullptr, *brick_cursor = nullptr, *brick_start = nullptr,
+      *brick_atoms = nullptr;
+  float* grid = nullptr;
+  int* stage = nullptr;
+  float2* cgrid = nullptr;
+  float2* tw[3] = {nullptr, nullptr, nullptr};
+  float *gfac[3] = {nullptr, nullptr, nullptr}, *f2[3] = {nullptr, nullptr, nullptr};
+  float gscale = 0.f;
+  // run state
+  bool forces_valid = false;
+  long long step = 0;
+  double self_energy = 0, inv_mtot = 0, dtu = 0, shake_tol = 1e-10;
+  double box_d[3] = {0, 0, 0};
+  int ncons = 0;
+  int temp_reset_every = 0;
+  double temperature = 300.0;
+  unsigned long long seed = 0;
+  long long launches = 0;
+  // per-stage timing
+  bool timing = false;
+  cudaEvent_t ev[12] = {};
+  double stage_ms[5] = {0, 0, 0, 0, 0};
+  long long timed_steps = 0;
+  // CUDA graph of one MD step (kick/drift/SHAKE, neighbour maintenance, forces,
+  // kick/RATTLE); captured on first use, replayed with one launch per step
+  cudaGraph_t step_graph = nullptr;
+  cudaGraphExec_t step_exec = nullptr;
+  bool use_graph = true;
+  // PME runs on a second stream concurrently with the pair and bonded kernels
+  cudaStream_t st2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // pinned staging
+  void* pinned = nullptr;
+  size_t pinned_bytes = 0;
+  // Andersen barostat (isotropic; the box keeps its aspect ratios).  L is the x edge;
+  // the piston obeys L'' = (P - Pref) / (3 M L^2) - 2 L'^2 / L, P = (2 KE + W) / (3 V)
+  // (src/cell_based_kernels.cu:569-579).
+  bool npt = false;
+  double pmass = 1e-5, pref_atm = 1.0;
+  double ratio[3] = {1.0, 1.0, 1.0};
+  double Ldot = 0.0, Lacc = 0.0;
+  double L_build = 0.0, L_prune = 0.0;  // box x edge at the last list build / prune
+  long long seen_rebuilds = 0, seen_prunes = 0;
+  double last_pressure = 0.0;
+  double plist = 0.0, cutoff = 0.0, col_a = 0.0;
+  float skin_half2_nve = 0.f, prune_half2_nve = 0.f;
+  double prune_delta = 0.0;
+  float* pme_tab_host = nullptr;  // pinned: gfac|f2 per dimension
+  int ncx = 1, ncy = 1;
+
+  template <class T>
+  fz_status alloc(T** ptr, size_t count) {
+    *ptr = nullptr;
+    if (count == 0) count = 1;
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e != cudaSuccess) return fail(FZ_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    allocs.push_back(p);
+    e = cudaMemsetAsync(p, 0, count * sizeof(T), st);
+    if (e != cudaSuccess) return fail(FZ_ERR_CUDA, std::string("cudaMemset: ") + cudaGetErrorString(e));
+    *ptr = static_cast<T*>(p);
+    return FZ_OK;
+  }
+  template <class T>
+  fz_status upload(T** ptr, const std::vector<T>& v) {
+    fz_status s = alloc(ptr, v.size());
+    if (s) return s;
+    if (!v.empty()) FZ_CUDA(cudaMemcpyAsync(*ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+    return FZ_OK;
+  }
+  void release(void* ptr) {
+    for (auto& a : allocs)
+      if (a == ptr) {
+        cudaFree(a);
+        a = allocs.back();
+        allocs.pop_back();
+        return;
+      }
+  }
+  fz_status staging(size_t bytes) {
+    if (pinned_bytes >= bytes) return FZ_OK;
+    if (pinned) cudaFreeHost(pinned);
+    pinned = nullptr;
+    FZ_CUDA(cudaMallocHost(&pinned, bytes));
+    pinned_bytes = bytes;
+    return FZ_OK;
+  }
+  ~Engine() {
+    if (st) cudaStreamSynchronize(st);
+    if (step_exec) cudaGraphExecDestroy(step_exec);
+    if (step_graph) cudaGraphDestroy(step_graph);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (st2) cudaStreamDestroy(st2);
+    for (auto& x : ev)
+      if (x) cudaEventDestroy(x);
+    for (void* p : allocs) cudaFree(p);
+    if (pinned) cudaFreeHost(pinned);
+    if (pme_tab_host) cudaFreeHost(pme_tab_host);
+    if (own_stream && st) cudaStreamDestroy(st);
+  }
+
+  fzk::RebuildArgs rebuild_args() const {
+    fzk::RebuildArgs a{};
+    a.p = p;
+    a.flag = flag;
+    a.counters = counters;
+    a.status = status;
+    a.pos4 = pos4;
+    a.pos_build = pos_build;
+    a.type = type;
+    a.col_of = col_of;
+    a.col_count = col_count;
+    a.col_cursor = col_cursor;
+    a.col_start = col_start;
+    a.col_tmp = col_tmp;
+    a.perm = perm;
+    a.inv_perm = inv_perm;
+    a.xyzq_s = xyzq_s;
+    a.typ_s = typ_s;
+    a.bb_lo = bb_lo;
+    a.bb_hi = bb_hi;
+    a.excl_off = excl_off;
+    a.excl_idx = excl_idx;
+    a.masks = masks;
+    a.mask_cap = mask_cap;
+    a.all_images = all_images;
+    a.outer = outer;
+    a.outer_n = outer_n;
+    a.inner = inner;
+    a.inner_nt = inner_nt;
+    a.inner_m = inner_m;
+    a.dmask = dmask;
+    a.ocap = ocap;
+    a.flag_prune = flag_prune;
+    a.rp2 = rp2;
+    a.pos_prune = pos_prune;
+    a.items = items;
+    a.chunk = chunk;
+    a.blk_col = blk_col;
+    a.dcx = dcx;
+    a.dcy = dcy;
+    return a;
+  }
+  fzk::NonbondedArgs nb_args() const {
+    fzk::NonbondedArgs a{};
+    a.p = p;
+    a.xyzq_s = xyzq_s;
+    a.typ_s = typ_s;
+    a.perm = perm;
+    a.inner = inner;
+    a.inner_nt = inner_nt;
+    a.inner_m = inner_m;
+    a.dmask = dmask;
+    a.masks = masks;
+    a.counters = counters;
+    a.ljtab = ljtab;
+    a.facc = facc;
+    a.energy = energy;
+    a.ocap = ocap;
+    a.items = items;
+    a.chunk = chunk;
+    a.grid = nb_grid;
+    return a;
+  }
+  fzk::PmeArgs pme_args() const {
+    fzk::PmeArgs a{};
+    a.p = p;
+    a.pos4 = pos4;
+    a.n = n;
+    for (int d = 0; d < 3; ++d) {
+      a.K[d] = K[d];
+      a.B[d] = B[d];
+      a.nb[d] = nbk[d];
+      a.tw[d] = tw[d];
+      a.gfac[d] = gfac[d];
+      a.f2[d] = f2[d];
+    }
+    a.brick_of = brick_of;
+    a.brick_count = brick_count;
+    a.brick_cursor = brick_cursor;
+    a.brick_start = brick_start;
+    a.brick_atoms = brick_atoms;
+    a.grid = grid;
+    a.stage = stage;
+    a.cgrid = cgrid;
+    a.gscale = gscale;
+    a.facc = facc;
+    a.energy = energy;
+    a.status = status;
+    return a;
+  }
+  fzk::BondedArgs bonded_args() const {
+    fzk::BondedArgs a{};
+    a.p = p;
+    a.pos4 = pos4;
+    a.nbond = nbond;
+    a.nangle = nangle;
+    a.nub = nub;
+    a.ndihe = ndihe;
+    a.nimpr = nimpr;
+    a.nexcl = nexcl;
+    a.n14 = n14;
+    a.bond = bond;
+    a.bond_prm = bond_prm;
+    a.angle = angle;
+    a.angle_prm = angle_prm;
+    a.ub = ub;
+    a.ub_prm = ub_prm;
+    a.dihe = dihe;
+    a.dihe_prm = dihe_prm;
+    a.impr = impr;
+    a.impr_prm = impr_prm;
+    a.excl = excl;
+    a.p14 = p14;
+    a.type = type;
+    a.lj14 = lj14;
+    a.facc = facc;
+    a.energy = energy;
+    return a;
+  }
+  fzk::IntegrateArgs int_args() const {
+    fzk::IntegrateArgs a{};
+    a.p = p;
+    a.nunits = nunits;
+    a.unit_atoms = unit_atoms;
+    a.unit_meta = unit_meta;
+    a.unit_d = unit_d;
+    a.pos4 = pos4;
+    a.vel4 = vel4;
+    a.facc = facc;
+    a.xyzq_s = xyzq_s;
+    a.inv_perm = inv_perm;
+    a.pos_build = pos_build;
+    a.pos_prune = pos_prune;
+    a.flag = flag;
+    a.flag_prune = flag_prune;
+    a.prune_half2 = prune_half2;
+    a.status = status;
+    a.energy = energy;
+    a.dtu = dtu;
+    for (int d = 0; d < 3; ++d) {
+      a.box_d[d] = box_d[d];
+      a.inv_box_d[d] = 1.0 / box_d[d];
+    }
+    a.shake_tol = shake_tol;
+    a.shake_maxit = 500;
+    a.lam = 1.0;
+    a.vfric = 1.0;
+    return a;
+  }
+
+  // ---------------------------------------------------------------- step pieces
+  void mark(int k) {
+    if (timing) cudaEventRecord(ev[k], st);
+  }
+  void forces(bool energies, int terms = FZ_TERM_ALL) {
+    mark(1);
+    fzk::launch_rebuild(rebuild_args(), st);
+    launches += 11;
+    mark(2);
+    if (terms & FZ_TERM_NONBONDED) {
+      fzk::launch_nonbonded(nb_args(), energies, st);
+      launches += 1;
+    }
+    mark(3);
+    if (terms & FZ_TERM_BONDED) {
+      fzk::launch_bonded(bonded_args(), energies, st);
+      launches += (nbond + nangle + nub + ndihe + nimpr + nexcl + n14 > 0) ? 1 : 0;
+    }
+    mark(4);
+    if (terms & FZ_TERM_PME) {
+      fzk::launch_pme(pme_args(), energies, st);
+      launches += 12;
+    }
+    mark(5);
+  }
+  // accumulates the events of one timed step: 0 start, 1..5 forces, 6 end
+  void collect_step() {
+    cudaEventSynchronize(ev[6]);
+    float ms = 0.f;
+    auto el = [&](int a, int b) {
+      cudaEventElapsedTime(&ms, ev[a], ev[b]);
+      return (double)ms;
+    };
+    stage_ms[0] += el(1, 2);
+    stage_ms[1] += el(2, 3);
+    stage_ms[2] += el(3, 4);
+    stage_ms[3] += el(4, 5);
+    stage_ms[4] += el(0, 1) + el(5, 6);
+    timed_steps++;
+  }
+  // forces with PME on st2, overlapping the pair and bonded kernels on st
+  void forces_overlapped() {
+    fzk::launch_rebuild(rebuild_args(), st);
+    cudaEventRecord(ev_fork, st);
+    cudaStreamWaitEvent(st2, ev_fork, 0);
+    fzk::launch_pme(pme_args(), false, st2);
+    fzk::launch_nonbonded(nb_args(), false, st);
+    fzk::launch_bonded(bonded_args(), false, st);
+    cudaEventRecord(ev_join, st2);
+    cudaStreamWaitEvent(st, ev_join, 0);
+  }
+  void step_body() {
+    const fzk::IntegrateArgs ia = int_args();
+    fzk::launch_kick_drift(ia, st);
+    if (st2)
+      forces_overlapped();
+    else
+      forces(false);
+    fzk::launch_kick_rattle(ia, false, true, st);
+  }
+  fz_status graph_step() {
+    if (!step_exec) {
+      FZ_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      const long long l0 = launches;
+      step_body();
+      launches = l0;
+      cudaGraph_t g = nullptr;
+      FZ_CUDA(cudaStreamEndCapture(st, &g));
+      step_graph = g;
+      FZ_CUDA(cudaGraphInstantiate(&step_exec, step_graph, 0));
+    }
+    FZ_CUDA(cudaGraphLaunch(step_exec, st));
+    launches += 2 + 11 + 1 + ((nbond + nangle + nub + ndihe + nimpr + nexcl + n14 > 0) ? 1 : 0) + 12;
+    return FZ_OK;
+  }
+  void drop_graph() {
+    if (step_exec) cudaGraphExecDestroy(step_exec);
+    if (step_graph) cudaGraphDestroy(step_graph);
+    step_exec = nullptr;
+    step_graph = nullptr;
+  }
+  fz_status check() {
+    int h = 0;
+    FZ_CUDA(cudaMemcpyAsync(&h, status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    FZ_CUDA(cudaStreamSynchronize(st));
+    FZ_CUDA(cudaGetLastError());
+    if (h) {
+      std::string m = "device status:";
+      if (h & fzk::ST_TILE_OVERFLOW) m += " pair-tile capacity exceeded;";
+      if (h & fzk::ST_MASK_OVERFLOW) m += " exclusion-mask capacity exceeded;";
+      if (h & fzk::ST_SLOT_OVERFLOW) m += " sorted-slot capacity exceeded;";
+      if (h & fzk::ST_COLUMN_OVERFLOW) m += " column occupancy exceeded;";
+      if (h & fzk::ST_SHAKE_NOCONV) m += " SHAKE did not converge within its iteration cap;";
+      if (h & fzk::ST_BAD_COORD) m += " non-finite or runaway coordinates;";
+      const int code = (h & fzk::ST_SHAKE_NOCONV) ? FZ_ERR_SHAKE : FZ_ERR_CAPACITY;
+      return fail(code, m);
+    }
+    return FZ_OK;
+  }
+};
+
+}  // namespace fz

@@ -73,7 +73,7 @@ extern "C" fz_status fz_read_input(const char* in_path, fz_config* c) {
   c->steepdesfac = 1e-4;
   c->conjgradrate = 0.1;
   c->steepdesrate = 0.01;
-  c->pmass = 2000.0;  // PMASS, src/defs.in.h
+  c->pmass = 1.0e-5;  // the pmass keyword sets pmass_cubic (src/prmread.cu:663-666), PMASS_CUBIC src/defs.in.h:104
   c->pref = 1.0;      // PREF (atm)
   c->printtostdout = 1;
   c->seed = 0;

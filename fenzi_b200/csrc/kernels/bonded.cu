@@ -30,10 +30,14 @@ __device__ __forceinline__ void addf(long long* facc, int n, int i, float3 f) {
 // J. Comput. Chem. 17, 1132 (1996)); returns false for a degenerate (collinear) geometry
 __device__ __forceinline__ bool dihedral_geom(float4 ri, float4 rj, float4 rk, float4 rl, const SysParams& p,
                                               float* cphi, float* sphi, float3* gi, float3* gj, float3* gk,
-                                              float3* gl) {
+                                              float3* gl, float3* rel) {
   const float3 F = min_image(sub3(ri, rj), p);
   const float3 G = min_image(sub3(rj, rk), p);
   const float3 H = min_image(sub3(rl, rk), p);
+  // positions relative to atom j: i - j = F, k - j = -G, l - j = H - G
+  rel[0] = F;
+  rel[1] = make_float3(-G.x, -G.y, -G.z);
+  rel[2] = make_float3(H.x - G.x, H.y - G.y, H.z - G.z);
   const float3 A = cross(F, G), B = cross(H, G);
   const float A2 = dot(A, A), B2 = dot(B, B), G2 = dot(G, G);
   if (A2 < 1e-12f || B2 < 1e-12f || G2 < 1e-12f) return false;
@@ -57,6 +61,7 @@ __global__ void __launch_bounds__(256) k_bonded(BondedArgs a) {
   const SysParams& p = a.p;
   double e[7] = {0, 0, 0, 0, 0, 0, 0};  // bond angle ub dihed impr ewexcl (vdw14, elec14 below)
   double e14v = 0, e14e = 0;
+  double w[3] = {0, 0, 0};  // virial diagonal sum over atoms of r_a F_a (relative vectors)
   int r = t;
   if (r < a.nbond) {
     const int2 b = a.bond[r];
@@ -67,7 +72,12 @@ __global__ void __launch_bounds__(256) k_bonded(BondedArgs a) {
     const float f = rr > 0.f ? -2.f * pr.x * dr / rr : 0.f;
     addf(a.facc, n, b.x, make_float3(f * d.x, f * d.y, f * d.z));
     addf(a.facc, n, b.y, make_float3(-f * d.x, -f * d.y, -f * d.z));
-    if (ENERGY) e[0] = (double)pr.x * dr * dr;
+    if (ENERGY) {
+      e[0] = (double)pr.x * dr * dr;
+      w[0] = f * d.x * d.x;
+      w[1] = f * d.y * d.y;
+      w[2] = f * d.z * d.z;
+    }
   } else if ((r -= a.nbond) < a.nangle) {
     const int4 q = a.angle[r];
     const float2 pr = a.angle_prm[r];
@@ -75,10 +85,10 @@ __global__ void __launch_bounds__(256) k_bonded(BondedArgs a) {
     const float3 u = min_image(sub3(a.pos4[q.x], rj), p);
     const float3 v = min_image(sub3(a.pos4[q.z], rj), p);
     const float uu = dot(u, u), vv = dot(v, v), uv = dot(u, v);
-    const float3 w = cross(u, v);
+    const float3 uxv = cross(u, v);
     const float ruv = rsqrtf(uu * vv);
     const float c = uv * ruv;
-    const float s = sqrtf(dot(w, w)) * ruv;
+    const float s = sqrtf(dot(uxv, uxv)) * ruv;
     const float th = atan2f(s, c);
     const float dth = th - pr.y;
     const float dE = 2.f * pr.x * dth;
@@ -92,7 +102,12 @@ __global__ void __launch_bounds__(256) k_bonded(BondedArgs a) {
     addf(a.facc, n, q.x, fi);
     addf(a.facc, n, q.z, fk);
     addf(a.facc, n, q.y, make_float3(-fi.x - fk.x, -fi.y - fk.y, -fi.z - fk.z));
-    if (ENERGY) e[1] = (double)pr.x * dth * dth;
+    if (ENERGY) {
+      e[1] = (double)pr.x * dth * dth;
+      w[0] = fi.x * u.x + fk.x * v.x;
+      w[1] = fi.y * u.y + fk.y * v.y;
+      w[2] = fi.z * u.z + fk.z * v.z;
+    }
   } else if ((r -= a.nangle) < a.nub) {
     const int2 b = a.ub[r];
     const float2 pr = a.ub_prm[r];
@@ -102,13 +117,18 @@ __global__ void __launch_bounds__(256) k_bonded(BondedArgs a) {
     const float f = rr > 0.f ? -2.f * pr.x * dr / rr : 0.f;
     addf(a.facc, n, b.x, make_float3(f * d.x, f * d.y, f * d.z));
     addf(a.facc, n, b.y, make_float3(-f * d.x, -f * d.y, -f * d.z));
-    if (ENERGY) e[2] = (double)pr.x * dr * dr;
+    if (ENERGY) {
+      e[2] = (double)pr.x * dr * dr;
+      w[0] = f * d.x * d.x;
+      w[1] = f * d.y * d.y;
+      w[2] = f * d.z * d.z;
+    }
   } else if ((r -= a.nub) < a.ndihe) {
     const int4 q = a.dihe[r];
     const float4 pr = a.dihe_prm[r];  // K, n, cos d, sin d
     float c, s;
-    float3 gi, gj, gk, gl;
-    if (dihedral_geom(a.pos4[q.x], a.pos4[q.y], a.pos4[q.z], a.pos4[q.w], p, &c, &s, &gi, &gj, &gk, &gl)) {
+    float3 gi, gj, gk, gl, rel[3];
+    if (dihedral_geom(a.pos4[q.x], a.pos4[q.y], a.pos4[q.z], a.pos4[q.w], p, &c, &s, &gi, &gj, &gk, &gl, rel)) {
       const int nn = (int)pr.y;
       float cn = 1.f, sn = 0.f;
       for (int m = 0; m < nn; ++m) {
@@ -123,14 +143,19 @@ __global__ void __launch_bounds__(256) k_bonded(BondedArgs a) {
       addf(a.facc, n, q.y, make_float3(-dE * gj.x, -dE * gj.y, -dE * gj.z));
       addf(a.facc, n, q.z, make_float3(-dE * gk.x, -dE * gk.y, -dE * gk.z));
       addf(a.facc, n, q.w, make_float3(-dE * gl.x, -dE * gl.y, -dE * gl.z));
-      if (ENERGY) e[3] = (double)pr.x * (1.0 + (double)cosd);
+      if (ENERGY) {
+        e[3] = (double)pr.x * (1.0 + (double)cosd);
+        w[0] = -dE * (gi.x * rel[0].x + gk.x * rel[1].x + gl.x * rel[2].x);
+        w[1] = -dE * (gi.y * rel[0].y + gk.y * rel[1].y + gl.y * rel[2].y);
+        w[2] = -dE * (gi.z * rel[0].z + gk.z * rel[1].z + gl.z * rel[2].z);
+      }
     }
   } else if ((r -= a.ndihe) < a.nimpr) {
     const int4 q = a.impr[r];
     const float2 pr = a.impr_prm[r];
     float c, s;
-    float3 gi, gj, gk, gl;
-    if (dihedral_geom(a.pos4[q.x], a.pos4[q.y], a.pos4[q.z], a.pos4[q.w], p, &c, &s, &gi, &gj, &gk, &gl)) {
+    float3 gi, gj, gk, gl, rel[3];
+    if (dihedral_geom(a.pos4[q.x], a.pos4[q.y], a.pos4[q.z], a.pos4[q.w], p, &c, &s, &gi, &gj, &gk, &gl, rel)) {
       float dp = atan2f(s, c) - pr.y;
       dp -= 6.283185307179586f * rintf(dp * 0.15915494309189535f);
       const float dE = 2.f * pr.x * dp;
@@ -138,7 +163,12 @@ __global__ void __launch_bounds__(256) k_bonded(BondedArgs a) {
       addf(a.facc, n, q.y, make_float3(-dE * gj.x, -dE * gj.y, -dE * gj.z));
       addf(a.facc, n, q.z, make_float3(-dE * gk.x, -dE * gk.y, -dE * gk.z));
       addf(a.facc, n, q.w, make_float3(-dE * gl.x, -dE * gl.y, -dE * gl.z));
-      if (ENERGY) e[4] = (double)pr.x * dp * dp;
+      if (ENERGY) {
+        e[4] = (double)pr.x * dp * dp;
+        w[0] = -dE * (gi.x * rel[0].x + gk.x * rel[1].x + gl.x * rel[2].x);
+        w[1] = -dE * (gi.y * rel[0].y + gk.y * rel[1].y + gl.y * rel[2].y);
+        w[2] = -dE * (gi.z * rel[0].z + gk.z * rel[1].z + gl.z * rel[2].z);
+      }
     }
   } else if ((r -= a.nimpr) < a.nexcl) {
     // Ewald exclusion correction, FP64: E = -CC qq erf(beta r)/r
@@ -159,7 +189,12 @@ __global__ void __launch_bounds__(256) k_bonded(BondedArgs a) {
     red_add(a.facc + b.y, -fx);
     red_add(a.facc + n + b.y, -fy);
     red_add(a.facc + 2 * n + b.y, -fz);
-    if (ENERGY) e[5] = -kCC * qq * erfv / rr;
+    if (ENERGY) {
+      e[5] = -kCC * qq * erfv / rr;
+      w[0] = f * d[0] * d[0];
+      w[1] = f * d[1] * d[1];
+      w[2] = f * d[2] * d[2];
+    }
   } else if ((r -= a.nexcl) < a.n14) {
     // 1-4: 1-4 LJ (switched) + erfc Coulomb, no cutoff test (src/bonded_forces.cu:1155-1268)
     const int2 b = a.p14[r];
@@ -188,6 +223,9 @@ __global__ void __launch_bounds__(256) k_bonded(BondedArgs a) {
     if (ENERGY) {
       e14v = (double)(elj * sw);
       e14e = (double)ec;
+      w[0] = fr * d.x * d.x;
+      w[1] = fr * d.y * d.y;
+      w[2] = fr * d.z * d.z;
     }
   }
   if (ENERGY) {
@@ -199,6 +237,9 @@ __global__ void __launch_bounds__(256) k_bonded(BondedArgs a) {
     energy_add(a.energy + EN_EWEXCL, e[5]);
     energy_add(a.energy + EN_VDW, e14v);
     energy_add(a.energy + EN_ELEC, e14e);
+    energy_add(a.energy + EN_VIR_X, w[0]);
+    energy_add(a.energy + EN_VIR_Y, w[1]);
+    energy_add(a.energy + EN_VIR_Z, w[2]);
   }
 }
 

@@ -31,7 +31,9 @@ enum : int {
 // energy slots (same order as fz_energies)
 enum : int {
   EN_BOND = 0, EN_ANGLE, EN_UREYB, EN_DIHED, EN_IMPR, EN_VDW, EN_ELEC, EN_PME, EN_EWEXCL, EN_EWSELF,
-  EN_KIN, EN_VIR_X, EN_VIR_Y, EN_VIR_Z, EN_COUNT = 16
+  EN_KIN, EN_VIR_X, EN_VIR_Y, EN_VIR_Z,
+  EN_KIN_HALF,  // half-step kinetic energy of a barostat step
+  EN_COUNT = 16
 };
 
 // tile-list j entry: bits 0..26 slot, bits 27..31 periodic image code (0..26, 13 = none)

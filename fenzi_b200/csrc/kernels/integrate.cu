@@ -197,6 +197,47 @@ __device__ void rattle_unit(const Unit& U, const double r[4][3], double v[4][3],
     }
 }
 
+// mass centre offset of a unit relative to its atom 0 (min-imaged) and total mass
+__device__ __forceinline__ double unit_centre(const Unit& U, const double r[4][3], const double* im, double* cm,
+                                              const IntegrateArgs& a) {
+  double mt = 0.0;
+  cm[0] = cm[1] = cm[2] = 0.0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (k >= U.na) continue;
+    const double m = im[k] > 0.0 ? 1.0 / im[k] : 0.0;
+    double d[3] = {r[k][0] - r[0][0], r[k][1] - r[0][1], r[k][2] - r[0][2]};
+    minimg3(d, a);
+    for (int c = 0; c < 3; ++c) cm[c] += m * d[c];
+    mt += m;
+  }
+  if (mt > 0.0)
+    for (int c = 0; c < 3; ++c) cm[c] /= mt;
+  return mt;
+}
+
+// scales the unit's centre-of-mass velocity by f (barostat friction on the peculiar
+// centre-of-mass motion; internal motion is untouched)
+__device__ __forceinline__ void scale_com_velocity(const Unit& U, double v[4][3], const double* im, double f) {
+  double p[3] = {0.0, 0.0, 0.0}, mt = 0.0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (k >= U.na) continue;
+    const double m = im[k] > 0.0 ? 1.0 / im[k] : 0.0;
+    for (int c = 0; c < 3; ++c) p[c] += m * v[k][c];
+    mt += m;
+  }
+  if (mt <= 0.0) return;
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (k < U.na)
+      for (int c = 0; c < 3; ++c) v[k][c] += (f - 1.0) * p[c] / mt;
+}
+
+// NPT (Andersen barostat step with the integration units as scaling groups): the unit
+// moves rigidly with its mass centre scaled by a.lam about the origin (the box changed
+// by a.lam), and its centre-of-mass velocity is scaled by a.vfric before the kick.
+template <bool NPT>
 __global__ void __launch_bounds__(128) k_kick_drift(IntegrateArgs a) {
   const int u = blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= a.nunits) return;
@@ -212,23 +253,61 @@ __global__ void __launch_bounds__(128) k_kick_drift(IntegrateArgs a) {
     if (k < U.na) {
       const int i = U.atom[k];
       const float4 pr = a.pos4[i], vl = a.vel4[i];
-      const double3 F = force_of(a.facc, n, i);
-      a.facc[i] = 0;
-      a.facc[n + i] = 0;
-      a.facc[2 * n + i] = 0;
       im[k] = vl.w;
       q[k] = pr.w;
-      const double h = 0.5 * a.dtu * im[k];
-      v[k][0] = vl.x + h * F.x;
-      v[k][1] = vl.y + h * F.y;
-      v[k][2] = vl.z + h * F.z;
+      v[k][0] = vl.x;
+      v[k][1] = vl.y;
+      v[k][2] = vl.z;
       r0[k][0] = pr.x;
       r0[k][1] = pr.y;
       r0[k][2] = pr.z;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) rn[k][c] = r0[k][c] + a.dtu * v[k][c];
     }
   }
+  if (NPT) scale_com_velocity(U, v, im, a.vfric);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (k >= U.na) continue;
+    const int i = U.atom[k];
+    const double3 F = force_of(a.facc, n, i);
+    a.facc[i] = 0;
+    a.facc[n + i] = 0;
+    a.facc[2 * n + i] = 0;
+    const double h = 0.5 * a.dtu * im[k];
+    v[k][0] += h * F.x;
+    v[k][1] += h * F.y;
+    v[k][2] += h * F.z;
+  }
+  if (NPT) {
+    // Each atom moves by (lam - 1) x the unit's mass centre taken in the atom's own
+    // periodic image (atoms of a unit can sit on opposite sides of the box after the
+    // rebuild wraps them), so every min-imaged intra-unit vector is unchanged in the
+    // new box and the unit moves rigidly.  Offsets are min-imaged in the old box
+    // (a.box_d / a.lam), the frame the positions are in.
+    double d[4][3], cm[3] = {0.0, 0.0, 0.0}, mt = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      for (int c = 0; c < 3; ++c) {
+        const double L0 = a.box_d[c] / a.lam;
+        const double x = r0[k][c] - r0[0][c];
+        d[k][c] = x - L0 * rint(x / L0);
+      }
+      if (k < U.na && im[k] > 0.0) {
+        for (int c = 0; c < 3; ++c) cm[c] += d[k][c] / im[k];
+        mt += 1.0 / im[k];
+      }
+    }
+    if (mt > 0.0)
+      for (int c = 0; c < 3; ++c) cm[c] /= mt;
+    const double s = a.lam - 1.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (k < U.na)
+        for (int c = 0; c < 3; ++c) r0[k][c] += s * (r0[k][c] - d[k][c] + cm[c]);
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) rn[k][c] = r0[k][c] + a.dtu * v[k][c];
   if (U.nc > 0) {
     const int st = shake_unit(U, r0, rn, im, a);
     if (st) atomicOr(a.status, ST_SHAKE_NOCONV);
@@ -256,6 +335,57 @@ __global__ void __launch_bounds__(128) k_kick_drift(IntegrateArgs a) {
   }
   if (far) *a.flag = 1;
   if (moved) *a.flag_prune = 1;
+}
+
+// Group (unit) virial terms of a barostat step, after the forces: the centre-of-mass
+// kinetic energy of the half-step velocities into EN_KIN_HALF and, into the virial
+// slots, minus the intra-unit part sum_a (r_a - R_unit) . F_a, which turns the atomic
+// force virial into the virial of the unit centres (constraint forces are internal to
+// a unit and drop out).
+__global__ void __launch_bounds__(128) k_unit_virial(IntegrateArgs a) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  double ke = 0.0, vir[3] = {0.0, 0.0, 0.0};
+  if (u < a.nunits) {
+    const Unit U = load_unit(a, u);
+    const int n = a.p.n;
+    double r[4][3], im[4], p[3] = {0.0, 0.0, 0.0}, mt = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      im[k] = 0.0;
+      for (int c = 0; c < 3; ++c) r[k][c] = 0.0;
+      if (k >= U.na) continue;
+      const int i = U.atom[k];
+      const float4 pr = a.pos4[i], vl = a.vel4[i];
+      im[k] = vl.w;
+      r[k][0] = pr.x;
+      r[k][1] = pr.y;
+      r[k][2] = pr.z;
+      const double m = im[k] > 0.0 ? 1.0 / im[k] : 0.0;
+      p[0] += m * vl.x;
+      p[1] += m * vl.y;
+      p[2] += m * vl.z;
+      mt += m;
+    }
+    if (mt > 0.0) ke = 0.5 * (p[0] * p[0] + p[1] * p[1] + p[2] * p[2]) / mt;
+    if (U.na > 1) {
+      double cm[3];
+      unit_centre(U, r, im, cm, a);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if (k >= U.na) continue;
+        const double3 F = force_of(a.facc, n, U.atom[k]);
+        double d[3] = {r[k][0] - r[0][0], r[k][1] - r[0][1], r[k][2] - r[0][2]};
+        minimg3(d, a);
+        vir[0] -= (d[0] - cm[0]) * F.x;
+        vir[1] -= (d[1] - cm[1]) * F.y;
+        vir[2] -= (d[2] - cm[2]) * F.z;
+      }
+    }
+  }
+  energy_add(a.energy + EN_KIN_HALF, ke);
+  energy_add(a.energy + EN_VIR_X, vir[0]);
+  energy_add(a.energy + EN_VIR_Y, vir[1]);
+  energy_add(a.energy + EN_VIR_Z, vir[2]);
 }
 
 template <bool KIN>
@@ -288,6 +418,7 @@ __global__ void __launch_bounds__(128) k_kick_rattle(IntegrateArgs a, int kick) 
       r[k][1] = pr.y;
       r[k][2] = pr.z;
     }
+    if (kick && a.vfric != 1.0) scale_com_velocity(U, v, im, a.vfric);
     if (U.nc > 0) rattle_unit(U, r, v, im, a);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -311,6 +442,74 @@ __global__ void __launch_bounds__(256) k_kinetic(IntegrateArgs a) {
     if (v.w > 0.f) ke = 0.5 / (double)v.w * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
   }
   energy_add(a.energy + EN_KIN, ke);
+}
+
+// Instantaneous constraint virial of the current state: the multipliers that keep the
+// second time derivative of every constraint length at zero given the forces F and the
+// velocities v, sum_l c_kl (r_k . r_l) lambda_l = -|v_k|^2 - r_k . (sum_a sgn_ka F_a / m_a),
+// give constraint forces G_a = sum_l sgn_la lambda_l r_l and the virial
+// sum_l lambda_l r_l (x) r_l (diagonal), added to the virial slots.
+__global__ void __launch_bounds__(128) k_constraint_virial(IntegrateArgs a) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  double vir[3] = {0.0, 0.0, 0.0};
+  if (u < a.nunits) {
+    const Unit U = load_unit(a, u);
+    if (U.nc > 0) {
+      const int n = a.p.n;
+      double r[4][3], v[4][3], f[4][3], im[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        im[k] = 0.0;
+        for (int c = 0; c < 3; ++c) r[k][c] = v[k][c] = f[k][c] = 0.0;
+        if (k >= U.na) continue;
+        const int i = U.atom[k];
+        const float4 pr = a.pos4[i], vl = a.vel4[i];
+        const double3 F = force_of(a.facc, n, i);
+        im[k] = vl.w;
+        r[k][0] = pr.x;
+        r[k][1] = pr.y;
+        r[k][2] = pr.z;
+        v[k][0] = vl.x;
+        v[k][1] = vl.y;
+        v[k][2] = vl.z;
+        f[k][0] = F.x * im[k];
+        f[k][1] = F.y * im[k];
+        f[k][2] = F.z * im[k];
+      }
+      double rd[3][3], vd[3][3], ad[3][3], cf[3][3], J[3][3], rhs[3], lam[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        bond_vec(U, k, r, rd[k], a);
+        for (int c = 0; c < 3; ++c) vd[k][c] = ad[k][c] = 0.0;
+#pragma unroll
+        for (int at = 0; at < 4; ++at) {
+          const double sg = sgn(U, k, at);
+          for (int c = 0; c < 3; ++c) {
+            vd[k][c] += sg * v[at][c];
+            ad[k][c] += sg * f[at][c];
+          }
+        }
+      }
+      coef_matrix(U, im, cf);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        rhs[k] = -(vd[k][0] * vd[k][0] + vd[k][1] * vd[k][1] + vd[k][2] * vd[k][2]) -
+                 (rd[k][0] * ad[k][0] + rd[k][1] * ad[k][1] + rd[k][2] * ad[k][2]);
+#pragma unroll
+        for (int l = 0; l < 3; ++l)
+          J[k][l] = cf[k][l] * (rd[l][0] * rd[k][0] + rd[l][1] * rd[k][1] + rd[l][2] * rd[k][2]);
+      }
+      if (solve3(U.nc, J, rhs, lam)) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+          if (k < U.nc)
+            for (int c = 0; c < 3; ++c) vir[c] += lam[k] * rd[k][c] * rd[k][c];
+      }
+    }
+  }
+  energy_add(a.energy + EN_VIR_X, vir[0]);
+  energy_add(a.energy + EN_VIR_Y, vir[1]);
+  energy_add(a.energy + EN_VIR_Z, vir[2]);
 }
 
 // ---------------------------------------------------------------- velocity reassignment
@@ -375,7 +574,19 @@ __global__ void k_zero_ll(long long* p, int n) {
 }
 
 void launch_kick_drift(const IntegrateArgs& a, cudaStream_t st) {
-  k_kick_drift<<<(a.nunits + 127) / 128, 128, 0, st>>>(a);
+  k_kick_drift<false><<<(a.nunits + 127) / 128, 128, 0, st>>>(a);
+}
+
+void launch_kick_drift_npt(const IntegrateArgs& a, cudaStream_t st) {
+  k_kick_drift<true><<<(a.nunits + 127) / 128, 128, 0, st>>>(a);
+}
+
+void launch_unit_virial(const IntegrateArgs& a, cudaStream_t st) {
+  k_unit_virial<<<(a.nunits + 127) / 128, 128, 0, st>>>(a);
+}
+
+void launch_constraint_virial(const IntegrateArgs& a, cudaStream_t st) {
+  k_constraint_virial<<<(a.nunits + 127) / 128, 128, 0, st>>>(a);
 }
 
 void launch_kick_rattle(const IntegrateArgs& a, bool kinetic, bool kick, cudaStream_t st) {

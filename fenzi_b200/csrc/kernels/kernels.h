@@ -74,8 +74,8 @@ struct PmeArgs {
   int* brick_cursor;
   int* brick_start;  // [nbricks+1]
   int* brick_atoms;  // [n]
-  int* qgrid;        // charge grid Kz*Ky*Kx, int32 fixed point 2^24 (zero between calls)
-  float* grid;       // potential grid Kz*Ky*Kx (real)
+  int* stage;        // per-brick charge regions (B+3)^3, int32 fixed point 2^24
+  float* grid;       // real grid Kz*Ky*Kx (charges, then potential)
   float2* cgrid;     // complex half grid Kz*Ky*(Kx/2+1)
   const float2* tw[3];     // twiddles per dimension (forward, e^{-2 pi i m/K})
   const float* gfac[3];    // per-dim b^2 exp(-pi^2 f^2/beta^2)
@@ -127,9 +127,18 @@ struct IntegrateArgs {
   double box_d[3], inv_box_d[3];
   double shake_tol;
   int shake_maxit;
+  double lam;    // barostat step: centre-of-mass scale of every unit (1 = none)
+  double vfric;  // barostat step: centre-of-mass velocity scale of the half kicks (1 = none)
 };
 // kick (F/2) + drift + SHAKE, zeroes the force accumulator, scatters sorted positions
 void launch_kick_drift(const IntegrateArgs& a, cudaStream_t st);
+// the same for a barostat step (rigid unit scaling by lam, centre-of-mass velocity
+// scale vfric)
+void launch_kick_drift_npt(const IntegrateArgs& a, cudaStream_t st);
+// barostat step: unit centre-of-mass kinetic energy and intra-unit virial correction
+void launch_unit_virial(const IntegrateArgs& a, cudaStream_t st);
+// adds the instantaneous constraint virial of the current positions/velocities/forces
+void launch_constraint_virial(const IntegrateArgs& a, cudaStream_t st);
 // kick (F/2) + RATTLE (+ kinetic energy)
 void launch_kick_rattle(const IntegrateArgs& a, bool kinetic, bool kick, cudaStream_t st);
 void launch_kinetic(const IntegrateArgs& a, cudaStream_t st);

@@ -96,7 +96,8 @@ __device__ __forceinline__ void run_tile(const PairConst& c, const SysParams& p,
                                          const float2* ljrow, uint32_t je, uint32_t excl, float4* jx, int* jt,
                                          const float4* __restrict__ xyzq, const int* __restrict__ typ,
                                          const int* __restrict__ perm, long long* __restrict__ facc, int lane,
-                                         int src, float& fix, float& fiy, float& fiz, float& ev, float& ee) {
+                                         int src, float& fix, float& fiy, float& fiz, float& ev, float& ee,
+                                         float* vir) {
   const int jslot = (int)(je & kSlotMask);
   const int code = (int)(je >> kSlotBits);
   float4 xj = xyzq[jslot];
@@ -126,6 +127,11 @@ __device__ __forceinline__ void run_tile(const PairConst& c, const SysParams& p,
       const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
       const bool ok = (r2 < c.rc2) && !((mrot >> k) & 1u);
       const float fr = pair_force<ENERGY>(c, r2, qi * b.w, ljrow[jtl[k]], ok, ev, ee);
+      if (ENERGY) {
+        vir[0] = fmaf(fr * dx, dx, vir[0]);
+        vir[1] = fmaf(fr * dy, dy, vir[1]);
+        vir[2] = fmaf(fr * dz, dz, vir[2]);
+      }
       fix = fmaf(fr, dx, fix);
       fiy = fmaf(fr, dy, fiy);
       fiz = fmaf(fr, dz, fiz);
@@ -140,6 +146,11 @@ __device__ __forceinline__ void run_tile(const PairConst& c, const SysParams& p,
       const float dx = xi.x - b.x, dy = xi.y - b.y, dz = xi.z - b.z;
       const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
       const float fr = pair_force<ENERGY>(c, r2, qi * b.w, ljrow[jtl[k]], r2 < c.rc2, ev, ee);
+      if (ENERGY) {
+        vir[0] = fmaf(fr * dx, dx, vir[0]);
+        vir[1] = fmaf(fr * dy, dy, vir[1]);
+        vir[2] = fmaf(fr * dz, dz, vir[2]);
+      }
       fix = fmaf(fr, dx, fix);
       fiy = fmaf(fr, dy, fiy);
       fiz = fmaf(fr, dz, fiz);
@@ -179,7 +190,7 @@ __global__ void __launch_bounds__(256, 3)
   int* jt = jt_all[warp];
   const int n = p.n;
   const int src = (lane + 1) & 31;
-  double e_vdw = 0.0, e_el = 0.0;
+  double e_vdw = 0.0, e_el = 0.0, w_acc[3] = {0.0, 0.0, 0.0};
   for (;;) {
     int it = 0;
     if (lane == 0) it = atomicAdd(&counters[CNT_WORK], 1);
@@ -192,14 +203,15 @@ __global__ void __launch_bounds__(256, 3)
     const float2* ljrow = lj + typ[islot] * nt1;
     const float qi = xi.w * p.cc;
     float fix = 0.f, fiy = 0.f, fiz = 0.f;
-    float ev = 0.f, ee = 0.f;
+    float ev = 0.f, ee = 0.f, vir[3] = {0.f, 0.f, 0.f};
     // tile 0 of a block is the diagonal (the block with itself, upper triangle j > i)
     int t = item.y;
     const int tend = min(inner_nt[I] + 1, t + chunk);
     if (t == 0) {
       const uint32_t tri = (lane == 31) ? 0xffffffffu : ((2u << lane) - 1u);
       run_tile<ENERGY>(c, p, xi, qi, ljrow, (uint32_t)islot | ((uint32_t)kNoShift << kSlotBits),
-                       dmask[islot] | tri, jx, jt, xyzq, typ, perm, facc, lane, src, fix, fiy, fiz, ev, ee);
+                       dmask[islot] | tri, jx, jt, xyzq, typ, perm, facc, lane, src, fix, fiy, fiz, ev, ee,
+                       vir);
       t = 1;
     }
     const uint32_t* jl = inner + (size_t)I * ocap - 32;  // inner tile t-1
@@ -208,7 +220,7 @@ __global__ void __launch_bounds__(256, 3)
       const int m = ml[t];
       const uint32_t excl = m >= 0 ? masks[(size_t)m * 32 + lane] : 0u;
       run_tile<ENERGY>(c, p, xi, qi, ljrow, jl[t * 32 + lane], excl, jx, jt, xyzq, typ, perm, facc, lane, src, fix,
-                       fiy, fiz, ev, ee);
+                       fiy, fiz, ev, ee, vir);
     }
     const int ai = perm[islot];
     if (ai >= 0) {
@@ -219,11 +231,15 @@ __global__ void __launch_bounds__(256, 3)
     if (ENERGY) {
       e_vdw += (double)ev;
       e_el += (double)ee;
+      for (int d = 0; d < 3; ++d) w_acc[d] += (double)vir[d];
     }
   }
   if (ENERGY) {
     energy_add(energy + EN_VDW, e_vdw);
     energy_add(energy + EN_ELEC, e_el);
+    energy_add(energy + EN_VIR_X, w_acc[0]);
+    energy_add(energy + EN_VIR_Y, w_acc[1]);
+    energy_add(energy + EN_VIR_Z, w_acc[2]);
   }
 }
 

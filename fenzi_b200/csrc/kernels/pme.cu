@@ -4,13 +4,14 @@
 // pair and BCMultiply (src/mdcuda.cu:748,780, src/cell_based_kernels.cu:1770-1826)
 // and PMEForce_medium/_large (src/pme_kernels.cu:381-770).
 //
-// Spreading is owner-computes: the grid is cut into bricks, atoms are binned by the
-// brick of their base grid point every step, and one CTA per brick accumulates the
-// order-4 B-spline weights of the atoms of that brick and of the next brick in each
-// dimension into shared memory with int64 fixed-point atomics (order independent, so
-// the grid is bit-reproducible), then writes its brick with plain stores.  No global
-// atomics, no per-grid-point lists.  B-splines are evaluated analytically (the
-// reference samples a 1001-point table with a truncating index).
+// Spreading in two phases: the grid is cut into bricks and atoms are binned by the
+// brick of their base grid point every step; one CTA per brick spreads each of its
+// atoms once into a shared-memory region (the brick grown by the 3-point stencil
+// reach on its low side) with int32 fixed-point atomics and stores the region to its
+// staging slot; k_pme_reduce then sums, per grid point, the <= 8 regions covering it.
+// Integer sums are order independent, so the grid is bit-reproducible; there are no
+// global atomics and no per-grid-point lists.  B-splines are evaluated analytically
+// (the reference samples a 1001-point table with a truncating index).
 #include "common.cuh"
 #include "kernels.h"
 
@@ -120,9 +121,10 @@ constexpr float kFixQ32 = 16777216.0f;  // charge grid fixed point, 2^24 per e
 // One CTA per brick processes the atoms binned to that brick exactly once: their
 // 4x4x4 stencils (grid points k0-3..k0 per dimension) all fall inside the brick grown
 // by 3 points on the low side, accumulated in shared memory with int32 fixed-point
-// atomics (2^24 per e; values stay far below +-128 e); the region is then added to
-// the int32 charge grid with RED atomics.  Integer sums are order independent, so the
-// grid is bit-reproducible.
+// atomics (2^24 per e; values stay far below +-128 e).  The region is stored to the
+// brick's staging slot with plain stores; k_pme_reduce then sums, for every grid point,
+// the <= 8 regions that cover it.  No global atomics, integer sums are exact, so the
+// charge grid is bit-reproducible.
 __global__ void __launch_bounds__(256) k_pme_spread(PmeArgs a) {
   extern __shared__ int acc[];
   const int Bx = a.B[0], By = a.B[1], Bz = a.B[2];
@@ -158,16 +160,42 @@ __global__ void __launch_bounds__(256) k_pme_spread(PmeArgs a) {
       }
   }
   __syncthreads();
-  for (int k = threadIdx.x; k < vol; k += blockDim.x) {
-    const int v = acc[k];
-    if (v == 0) continue;
-    const int lx = k % Ex, ly = (k / Ex) % Ey, lz = k / (Ex * Ey);
-    int gx = ox + lx, gy = oy + ly, gz = oz + lz;
-    gx += gx < 0 ? Kx : 0;
-    gy += gy < 0 ? Ky : 0;
-    gz += gz < 0 ? Kz : 0;
-    atomicAdd(a.qgrid + ((size_t)gz * Ky + gy) * Kx + gx, v);
+  int* stage = a.stage + (size_t)b * vol;
+  for (int k = threadIdx.x; k < vol; k += blockDim.x) stage[k] = acc[k];
+}
+
+// charge grid point (x, y, z) = sum over the bricks whose grown region covers it: its
+// own brick and, within 3 points of the brick's upper faces, the next brick(s)
+__global__ void __launch_bounds__(256) k_pme_reduce(PmeArgs a) {
+  const int Kx = a.K[0], Ky = a.K[1], Kz = a.K[2];
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= Kx * Ky * Kz) return;
+  const int x = g % Kx, y = (g / Kx) % Ky, z = g / (Kx * Ky);
+  const int Bx = a.B[0], By = a.B[1], Bz = a.B[2];
+  const int Ex = Bx + 3, Ey = By + 3, Ez = Bz + 3;
+  const int nbx = a.nb[0], nby = a.nb[1], nbz = a.nb[2];
+  const int bx = x / Bx, by = y / By, bz = z / Bz;
+  const int lx = x - bx * Bx, ly = y - by * By, lz = z - bz * Bz;
+  const int vol = Ex * Ey * Ez;
+  int sum = 0;
+#pragma unroll
+  for (int dz = 0; dz < 2; ++dz) {
+    if (dz && lz < Bz - 3) continue;
+    const int cz = dz ? (bz + 1) % nbz : bz, rz = dz ? lz - Bz + 3 : lz + 3;
+#pragma unroll
+    for (int dy = 0; dy < 2; ++dy) {
+      if (dy && ly < By - 3) continue;
+      const int cy = dy ? (by + 1) % nby : by, ry = dy ? ly - By + 3 : ly + 3;
+#pragma unroll
+      for (int dx = 0; dx < 2; ++dx) {
+        if (dx && lx < Bx - 3) continue;
+        const int cx = dx ? (bx + 1) % nbx : bx, rx = dx ? lx - Bx + 3 : lx + 3;
+        const int brick = (cz * nby + cy) * nbx + cx;
+        sum += a.stage[(size_t)brick * vol + (rz * Ey + ry) * Ex + rx];
+      }
+    }
   }
+  a.grid[g] = (float)sum * (1.0f / kFixQ32);
 }
 
 // ------------------------------------------------------------------ FFT
@@ -265,13 +293,7 @@ __global__ void __launch_bounds__(256) k_fft_x_r2c(PmeArgs a, FftPlan pl, int nl
   for (int idx = threadIdx.x; idx < nl * Kx; idx += blockDim.x) {
     const int l = idx / Kx, x = idx - l * Kx;
     const int row = r0 + l;
-    float qv = 0.f;
-    if (row < nrows) {
-      int* qp = a.qgrid + (size_t)row * Kx + x;
-      qv = (float)*qp * (1.0f / kFixQ32);
-      *qp = 0;  // leaves the charge grid zeroed for the next spread
-    }
-    A[l * ld + x] = make_float2(qv, 0.f);
+    A[l * ld + x] = make_float2(row < nrows ? a.grid[(size_t)row * Kx + x] : 0.f, 0.f);
   }
   __syncthreads();
   const float2* R = fft_lines(A, B, tw, pl, nl, false);
@@ -327,7 +349,7 @@ __global__ void __launch_bounds__(256) k_fft_z_conv(PmeArgs a, FftPlan pl, int n
   __syncthreads();
   float2* R = fft_lines(A, B, tw, pl, nl, false);
   float2* O = (R == A) ? B : A;
-  double e = 0.0;
+  double e = 0.0, w0 = 0.0, w1 = 0.0, w2 = 0.0;
   const float gy = a.gfac[1][y], fy2 = a.f2[1][y];
   for (int idx = threadIdx.x; idx < nl * Kz; idx += blockDim.x) {
     const int l = idx / Kz, z = idx - l * Kz;
@@ -338,9 +360,17 @@ __global__ void __launch_bounds__(256) k_fft_z_conv(PmeArgs a, FftPlan pl, int n
       const float den = a.f2[0][mx] + fy2 + a.f2[2][z];
       G = a.gscale * a.gfac[0][mx] * gy * a.gfac[2][z] / den;
     }
-    if (ENERGY && mx < Kxh) {
+    if (ENERGY && mx < Kxh && G != 0.f) {
+      // energy of this mode and its virial diagonal E (1 - 2 (1 + pi^2 m^2/beta^2) m_a^2 / m^2)
       const double wmx = (mx == 0 || (2 * mx == Kx)) ? 1.0 : 2.0;
-      e += wmx * 0.5 * (double)G * ((double)v.x * v.x + (double)v.y * v.y);
+      const double em = wmx * 0.5 * (double)G * ((double)v.x * v.x + (double)v.y * v.y);
+      const double fx2 = a.f2[0][mx], fz2 = a.f2[2][z];
+      const double m2 = fx2 + fy2 + fz2;
+      const double k = 2.0 * (1.0 + kPi * kPi * m2 / ((double)a.p.beta * a.p.beta)) / m2;
+      e += em;
+      w0 += em * (1.0 - k * fx2);
+      w1 += em * (1.0 - k * fy2);
+      w2 += em * (1.0 - k * fz2);
     }
     v.x *= G;
     v.y *= G;
@@ -353,7 +383,12 @@ __global__ void __launch_bounds__(256) k_fft_z_conv(PmeArgs a, FftPlan pl, int n
     const int mx = mx0 + l;
     if (mx < Kxh) a.cgrid[((size_t)z * Ky + y) * Kxh + mx] = Q[l * ld + z];
   }
-  if (ENERGY) energy_add(a.energy + EN_PME, e);
+  if (ENERGY) {
+    energy_add(a.energy + EN_PME, e);
+    energy_add(a.energy + EN_VIR_X, w0);
+    energy_add(a.energy + EN_VIR_Y, w1);
+    energy_add(a.energy + EN_VIR_Z, w2);
+  }
 }
 
 // x pass inverse: Hermitian half rows -> real potential rows
@@ -550,13 +585,7 @@ __global__ void __launch_bounds__(256) k_fft_x_r2c_t(PmeArgs a, int nl) {
   for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) {
     const int l = idx / N, x = idx - l * N;
     const int row = r0 + l;
-    float qv = 0.f;
-    if (row < nrows) {
-      int* qp = a.qgrid + (size_t)row * N + x;
-      qv = (float)*qp * (1.0f / kFixQ32);
-      *qp = 0;  // leaves the charge grid zeroed for the next spread
-    }
-    A[l * LD + x] = make_float2(qv, 0.f);
+    A[l * LD + x] = make_float2(row < nrows ? a.grid[(size_t)row * N + x] : 0.f, 0.f);
   }
   __syncthreads();
   const float2* R = fft_run_t<N, 0, 1, false>(A, B, tw, nl);
@@ -611,7 +640,7 @@ __global__ void __launch_bounds__(256) k_fft_z_conv_t(PmeArgs a, int nl) {
   __syncthreads();
   float2* R = fft_run_t<N, 0, 1, false>(A, B, tw, nl);
   float2* O = (R == A) ? B : A;
-  double e = 0.0;
+  double e = 0.0, w0 = 0.0, w1 = 0.0, w2 = 0.0;
   const float gy = a.gfac[1][y], fy2 = a.f2[1][y];
   for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) {
     const int l = idx / N, z = idx - l * N;
@@ -619,9 +648,17 @@ __global__ void __launch_bounds__(256) k_fft_z_conv_t(PmeArgs a, int nl) {
     float2 v = R[l * LD + z];
     float G = 0.f;
     if (mx < Kxh && (mx | y | z) != 0) G = a.gscale * a.gfac[0][mx] * gy * a.gfac[2][z] / (a.f2[0][mx] + fy2 + a.f2[2][z]);
-    if (ENERGY && mx < Kxh) {
+    if (ENERGY && mx < Kxh && G != 0.f) {
+      // energy of this mode and its virial diagonal E (1 - 2 (1 + pi^2 m^2/beta^2) m_a^2 / m^2)
       const double wmx = (mx == 0 || (2 * mx == Kx)) ? 1.0 : 2.0;
-      e += wmx * 0.5 * (double)G * ((double)v.x * v.x + (double)v.y * v.y);
+      const double em = wmx * 0.5 * (double)G * ((double)v.x * v.x + (double)v.y * v.y);
+      const double fx2 = a.f2[0][mx], fz2 = a.f2[2][z];
+      const double m2 = fx2 + fy2 + fz2;
+      const double k = 2.0 * (1.0 + kPi * kPi * m2 / ((double)a.p.beta * a.p.beta)) / m2;
+      e += em;
+      w0 += em * (1.0 - k * fx2);
+      w1 += em * (1.0 - k * fy2);
+      w2 += em * (1.0 - k * fz2);
     }
     v.x *= G;
     v.y *= G;
@@ -634,7 +671,12 @@ __global__ void __launch_bounds__(256) k_fft_z_conv_t(PmeArgs a, int nl) {
     const int mx = mx0 + l;
     if (mx < Kxh) a.cgrid[((size_t)z * Ky + y) * Kxh + mx] = Q[l * LD + z];
   }
-  if (ENERGY) energy_add(a.energy + EN_PME, e);
+  if (ENERGY) {
+    energy_add(a.energy + EN_PME, e);
+    energy_add(a.energy + EN_VIR_X, w0);
+    energy_add(a.energy + EN_VIR_Y, w1);
+    energy_add(a.energy + EN_VIR_Z, w2);
+  }
 }
 
 template <int N>
@@ -733,6 +775,7 @@ void launch_pme(const PmeArgs& a, bool energy, cudaStream_t st) {
   k_pme_scatter<<<(a.n + 255) / 256, 256, 0, st>>>(a);
   const size_t sp = (size_t)(a.B[0] + 3) * (a.B[1] + 3) * (a.B[2] + 3) * sizeof(int);
   k_pme_spread<<<nbr, 256, sp, st>>>(a);
+  k_pme_reduce<<<(a.K[0] * a.K[1] * a.K[2] + 255) / 256, 256, 0, st>>>(a);
   const int Kx = a.K[0], Ky = a.K[1], Kz = a.K[2], Kxh = Kx / 2 + 1;
   const FftPlan px = make_plan(Kx), py = make_plan(Ky), pz = make_plan(Kz);
   const int lx = lines_for(Kx), ly = lines_for(Ky), lz = lines_for(Kz);

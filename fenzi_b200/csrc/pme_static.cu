@@ -5,7 +5,7 @@
 // device memory after start-up.  fz_pme_reciprocal_static() serves them: it runs the
 // same spread / R2C-FFT + influence function / C2R / gather kernels as the system
 // path, but every scratch buffer lives in the fixed-size file-scope __device__ arrays
-// below (about 5.4 MB on every GPU that loads the library, held until the process
+// below (about 11 MB on every GPU that loads the library, held until the process
 // exits).  The caller passes its own device input (float4 x, y, z, q per atom) and
 // output (int64 fixed-point forces) buffers.
 //
@@ -31,7 +31,8 @@ constexpr int kSMaxBricks = 22 * 22 * 22;
 constexpr int kSMaxDev = 64;
 
 __device__ __align__(256) float s_grid[kSMaxK * kSMaxK * kSMaxK];
-__device__ __align__(256) int s_qgrid[kSMaxK * kSMaxK * kSMaxK];
+constexpr int kSMaxStage = 1536 * 1024;  // per-brick charge regions, (K/B)^3 (B+3)^3 ints
+__device__ __align__(256) int s_stage[kSMaxStage];
 __device__ __align__(256) float2 s_cgrid[kSMaxK * kSMaxK * (kSMaxK / 2 + 1)];
 __device__ __align__(256) int s_brick_of[kSMaxAtoms];
 __device__ __align__(256) int s_brick_atoms[kSMaxAtoms];
@@ -46,7 +47,7 @@ __device__ __align__(256) int s_status[1];
 
 struct Scratch {
   float* grid;
-  int* qgrid;
+  int* stage;
   float2* cgrid;
   int *brick_of, *brick_atoms, *brick_count, *brick_cursor, *brick_start, *status;
   float2* tw;
@@ -66,7 +67,7 @@ fz_status setup(int device, Scratch** out) {
     float2* tw = nullptr;
     float *gf = nullptr, *f2 = nullptr;
     if ((e = cudaGetSymbolAddress((void**)&s.grid, s_grid)) != cudaSuccess ||
-        (e = cudaGetSymbolAddress((void**)&s.qgrid, s_qgrid)) != cudaSuccess ||
+        (e = cudaGetSymbolAddress((void**)&s.stage, s_stage)) != cudaSuccess ||
         (e = cudaGetSymbolAddress((void**)&s.cgrid, s_cgrid)) != cudaSuccess ||
         (e = cudaGetSymbolAddress((void**)&s.brick_of, s_brick_of)) != cudaSuccess ||
         (e = cudaGetSymbolAddress((void**)&s.brick_atoms, s_brick_atoms)) != cudaSuccess ||
@@ -153,9 +154,13 @@ extern "C" fz_status fz_pme_reciprocal_static(int device, void* stream, const fl
       (ce = cudaMemcpyAsync(s->gfac, gfac, sizeof(gfac), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
       (ce = cudaMemcpyAsync(s->f2, f2, sizeof(f2), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
       (ce = cudaMemsetAsync(s->energy, 0, sizeof(long long) * fzk::EN_COUNT, st)) != cudaSuccess ||
-      (ce = cudaMemsetAsync(s->qgrid, 0, sizeof(int) * (size_t)K[0] * K[1] * K[2], st)) != cudaSuccess ||
       (ce = cudaMemsetAsync(facc, 0, sizeof(long long) * 3 * (size_t)n, st)) != cudaSuccess)
     return fail(FZ_ERR_CUDA, std::string("fz_pme_reciprocal_static: ") + cudaGetErrorString(ce));
+  {
+    long long need = 1;
+    for (int d = 0; d < 3; ++d) need *= (long long)(K[d] / brick_edge(K[d])) * (brick_edge(K[d]) + 3);
+    if (need > kSMaxStage) return fail(FZ_ERR_ARG, "fz_pme_reciprocal_static: grid too large for the static scratch");
+  }
   fzk::PmeArgs a{};
   a.p.box = make_float3((float)box[0], (float)box[1], (float)box[2]);
   a.p.inv_box = make_float3((float)(1.0 / box[0]), (float)(1.0 / box[1]), (float)(1.0 / box[2]));
@@ -178,7 +183,7 @@ extern "C" fz_status fz_pme_reciprocal_static(int device, void* stream, const fl
   a.brick_start = s->brick_start;
   a.brick_atoms = s->brick_atoms;
   a.grid = s->grid;
-  a.qgrid = s->qgrid;
+  a.stage = s->stage;
   a.cgrid = s->cgrid;
   a.gscale = (float)(kCC / (M_PI * box[0] * box[1] * box[2]));
   a.facc = facc;

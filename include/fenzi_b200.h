@@ -79,9 +79,12 @@ typedef struct fz_energies {
   double potential;          /* sum of the above */
   double kinetic;            /* 1/2 sum m v^2 */
   double temperature;        /* 2 KE / (k_B (3N - 6 - Ncons)) */
-  double virial[3];          /* diagonal of the virial (kcal/mol) */
-  double pressure_atm;
+  double virial[3];          /* diagonal of the virial sum r (x) F, constraint forces included (kcal/mol) */
+  double pressure_atm;       /* (2 KE + W) / (3 V), src/cell_based_kernels.cu:582-587 */
   long long step;
+  double box[3];             /* current box edges (A); they change under the barostat */
+  double volume;             /* A^3 */
+  double conserved;          /* KE + U, plus Pref V + piston kinetic energy under the barostat */
 } fz_energies;
 
 /* Sizes of a loaded system. */
@@ -142,8 +145,18 @@ fz_status fz_compute_forces_terms(fz_system* sys, int terms, int energies);
  * device-side neighbour maintenance, velocity reassignment every temp_reset_every
  * steps when set.  Returns after the work is queued and checked. */
 fz_status fz_step(fz_system* sys, int nsteps);
-/* EvalProps (src/evalprops.cu:17-308): energies of the current state. */
+/* EvalProps (src/evalprops.cu:17-308): energies of the current state, with the
+ * virial (force terms, PME reciprocal term and the instantaneous constraint forces)
+ * and the pressure (src/evalprops.cu:214-218). */
 fz_status fz_eval_props(fz_system* sys, fz_energies* out);
+/* Andersen constant-pressure dynamics for the following fz_step calls (the reference's
+ * PCONSTANT build: src/cell_based_kernels.cu:566-579 piston acceleration,
+ * src/mdcuda.cu:58-88 half kicks; keywords pref/pmass, src/prmread.cu:663-670).
+ * The box keeps its aspect ratios; its x edge L follows
+ * L'' = (P - pref) / (3 pmass L^2) - 2 L'^2 / L with P in kcal/mol/A^3.  Each
+ * barostat step synchronises with the host once (the pressure steers the next box).
+ * enable = 0 returns to constant volume at the current box. */
+fz_status fz_set_barostat(fz_system* sys, int enable, double pref_atm, double pmass);
 /* Host <-> device state (original atom order). */
 fz_status fz_get_positions(fz_system* sys, double* out3n);
 fz_status fz_set_positions(fz_system* sys, const double* in3n);
@@ -159,6 +172,9 @@ fz_status fz_get_state_f32(fz_system* sys, float* pos3n, float* vel3n);
 /* Device-side work counters: [0] kernel launches issued, [1] neighbour-list rebuilds,
  * [2] 32x32 pair tiles in the current (pruned) list, [3] list prunes. */
 fz_status fz_get_counters(fz_system* sys, long long* out4);
+/* Virial diagonal accumulated by the last fz_compute_forces_terms(..., energies = 1)
+ * (force terms only: no constraint or kinetic part). */
+fz_status fz_get_virial(fz_system* sys, double* out3);
 /* Per-stage device timing (CUDA events on the system stream) for the steps run
  * while enabled.  Stages: 0 neighbour maintenance, 1 real-space pairs, 2 bonded,
  * 3 PME, 4 integrate (kick/drift/SHAKE + kick/RATTLE).  fz_get_stage_times returns
@@ -171,7 +187,7 @@ fz_status fz_measure_fp32_peak(int device, double* tflops);
 /* No counterpart in the reference.  PME reciprocal-space forces (and optionally the
  * reciprocal energy) of n atoms for callers that cannot call cudaMalloc (code living
  * inside another framework's memory pool or a pre-sized arena).  Allocates nothing:
- * scratch lives in fixed file-scope device arrays (about 5.4 MB on each GPU that loads
+ * scratch lives in fixed file-scope device arrays (about 11 MB on each GPU that loads
  * the library, held until exit).  pos4: device float4[n] (x, y, z, q); facc: device
  * int64[3n] fixed point (scale 2^32, x[n] y[n] z[n]), overwritten; energy_out: host
  * double or NULL (when given, the call synchronises `stream`).  Limits: n <= 262144,
@@ -180,6 +196,52 @@ fz_status fz_measure_fp32_peak(int device, double* tflops);
  * on the shared scratch and must be serialised by the caller. */
 fz_status fz_pme_reciprocal_static(int device, void* stream, const float* pos4, int n, const double* box,
                                    const int* K, double beta, long long* facc, double* energy_out);
+/* ---- batched ensemble --------------------------- */
+/* Independent uploaded systems (same device) advanced together: one MD step of every
+ * system is one CUDA-graph launch whose branches are the systems' steps, so small
+ * systems run concurrently on the GPU.  The batch does not own the systems; positions,
+ * velocities and energies are read per system with the single-system calls. */
+typedef struct fz_batch fz_batch;
+fz_status fz_batch_create(fz_batch** out);
+fz_status fz_batch_add(fz_batch* batch, fz_system* sys);
+fz_status fz_batch_step(fz_batch* batch, int nsteps);
+fz_status fz_batch_free(fz_batch* batch);
+/* Removes a system (it keeps its device state and can be stepped alone or added again). */
+fz_status fz_batch_remove(fz_batch* batch, fz_system* sys);
+fz_status fz_batch_size(fz_batch* batch, int* out);
+
+/* Serving loop (no counterpart in the reference, which runs one system per process):
+ * a worker thread admits submitted jobs in FIFO order while the estimated device
+ * memory of the running jobs stays within hbm_budget_bytes and fewer than max_running
+ * run, keeps their state resident, advances the running mix together in the batch
+ * graph in chunks of at most chunk_steps (a chunk ends when a job finishes), and
+ * frees a job's device memory when it finishes, keeping its final energies and
+ * positions.  Times are seconds since fz_server_create. */
+typedef struct fz_server fz_server;
+typedef struct fz_job_info {
+  int job;
+  int state;                 /* 0 queued, 1 running, 2 done, 3 failed */
+  int status;                /* fz_status of a failed job */
+  int natom;
+  long long nsteps, steps_done;
+  double submit_s, start_s, end_s;
+  double device_bytes;       /* admission estimate */
+  fz_energies final;         /* energies of the last frame (done jobs) */
+} fz_job_info;
+fz_status fz_server_create(int device, double hbm_budget_bytes, int chunk_steps, int max_running, fz_server** out);
+/* Takes ownership of a loaded (not uploaded) system; it is freed by fz_server_free. */
+fz_status fz_server_submit(fz_server* server, fz_system* sys, long long nsteps, int* job_id);
+fz_status fz_server_info(fz_server* server, int job_id, fz_job_info* out);
+/* Blocks until the job is done or failed; returns the job's status. */
+fz_status fz_server_wait(fz_server* server, int job_id, fz_job_info* out);
+/* Final positions (natom x 3, PSF order) of a done job. */
+fz_status fz_server_positions(fz_server* server, int job_id, double* out);
+/* [0] peak running jobs, [1] atom-steps done, [2] estimated bytes in use, [3] jobs finished. */
+fz_status fz_server_stats(fz_server* server, double* out4);
+/* The admission estimate of a loaded system's device memory (bytes). */
+fz_status fz_server_estimate_bytes(const fz_system* sys, double* out);
+/* Lets queued and running jobs finish, stops the worker, frees every job's system. */
+fz_status fz_server_free(fz_server* server);
 /* Synchronises the system's stream and reports any sticky device error status. */
 fz_status fz_sync(fz_system* sys);
 /* The system's CUDA stream (cudaStream_t), for callers that time or order work. */

@@ -1017,3 +1017,223 @@ void orc_reassign_velocities(void* h, const double* pos, double T, uint64_t seed
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- virial, pressure, Andersen barostat
+namespace {
+
+// integration units: SHAKE clusters and free atoms (the barostat's scaling groups)
+std::vector<std::vector<int>> units_of(const Orc& o) {
+  std::vector<std::vector<int>> u;
+  std::vector<int> in_cl(o.s.n, 0);
+  for (const Cluster& cl : o.clusters) {
+    u.emplace_back(cl.atom, cl.atom + cl.na);
+    for (int a = 0; a < cl.na; ++a) in_cl[cl.atom[a]] = 1;
+  }
+  for (int i = 0; i < o.s.n; ++i)
+    if (!in_cl[i]) u.push_back({i});
+  return u;
+}
+
+// mass centre of a unit (min-imaged about its first atom)
+void centre(const Orc& o, const std::vector<int>& u, const double* pos, double* R) {
+  double cm[3] = {0, 0, 0}, mt = 0;
+  for (int i : u) {
+    double d[3] = {pos[3 * i] - pos[3 * u[0]], pos[3 * i + 1] - pos[3 * u[0] + 1], pos[3 * i + 2] - pos[3 * u[0] + 2]};
+    minimg(d, o.s.box);
+    for (int c = 0; c < 3; ++c) cm[c] += o.mass[i] * d[c];
+    mt += o.mass[i];
+  }
+  for (int c = 0; c < 3; ++c) R[c] = pos[3 * u[0] + c] + cm[c] / mt;
+}
+
+// W_aa = -L_a dU/dL_a by central differences of the energy at fixed fractional
+// coordinates: of every atom (group = 0, the atomic virial) or of every unit's mass
+// centre with the units moved rigidly (group = 1, the group virial).
+void virial_fd(const Orc& o, const double* pos, double h, int terms, double* vir, int group) {
+  const int n = o.s.n;
+  std::vector<double> ps(3 * (size_t)n), f(3 * (size_t)n), R;
+  std::vector<std::vector<int>> units;
+  if (group) {
+    units = units_of(o);
+    R.resize(3 * units.size());
+    for (size_t k = 0; k < units.size(); ++k) centre(o, units[k], pos, &R[3 * k]);
+  }
+  double e[ORC_NE];
+  for (int a = 0; a < 3; ++a) {
+    double u[2];
+    for (int sgn = 0; sgn < 2; ++sgn) {
+      const double sc = sgn ? 1.0 - h : 1.0 + h;
+      Orc w = o;
+      w.s.box[a] = o.s.box[a] * sc;
+      for (int i = 0; i < 3 * n; ++i) ps[i] = pos[i];
+      if (group) {  // the centre's image next to each atom, so wrapped units move rigidly
+        for (size_t k = 0; k < units.size(); ++k)
+          for (int i : units[k]) {
+            const int a0 = units[k][0];
+            double d[3] = {pos[3 * i] - pos[3 * a0], pos[3 * i + 1] - pos[3 * a0 + 1], pos[3 * i + 2] - pos[3 * a0 + 2]};
+            double dm[3] = {d[0], d[1], d[2]};
+            minimg(dm, o.s.box);
+            ps[3 * i + a] += (sc - 1.0) * (R[3 * k + a] + d[a] - dm[a]);
+          }
+      } else {
+        for (int i = 0; i < n; ++i) ps[3 * i + a] *= sc;
+      }
+      std::fill(f.begin(), f.end(), 0.0);
+      orc_forces(&w, ps.data(), f.data(), e, terms);
+      double t = 0;
+      for (int k = 0; k < ORC_NE; ++k) t += e[k];
+      u[sgn] = t;
+    }
+    vir[a] = -(u[0] - u[1]) / (2.0 * h);
+  }
+}
+
+// kinetic energy of the unit centres
+double com_kinetic(const Orc& o, const std::vector<std::vector<int>>& units, const double* vel) {
+  double k = 0;
+  for (const auto& u : units) {
+    double p[3] = {0, 0, 0}, mt = 0;
+    for (int i : u) {
+      for (int c = 0; c < 3; ++c) p[c] += o.mass[i] * vel[3 * i + c];
+      mt += o.mass[i];
+    }
+    k += 0.5 * dot3(p, p) / mt;
+  }
+  return k;
+}
+
+// scales every unit's centre-of-mass velocity by f
+void scale_com(const Orc& o, const std::vector<std::vector<int>>& units, double* vel, double f) {
+  for (const auto& u : units) {
+    double p[3] = {0, 0, 0}, mt = 0;
+    for (int i : u) {
+      for (int c = 0; c < 3; ++c) p[c] += o.mass[i] * vel[3 * i + c];
+      mt += o.mass[i];
+    }
+    for (int i : u)
+      for (int c = 0; c < 3; ++c) vel[3 * i + c] += (f - 1.0) * p[c] / mt;
+  }
+}
+
+// instantaneous constraint virial: multipliers keeping d2/dt2 |r_k|^2 = 0 given F and v
+void constraint_virial(const Orc& o, const double* pos, const double* vel, const double* f, double* vir) {
+  for (const Cluster& cl : o.clusters) {
+    double rd[3][3], im[4];
+    for (int a = 0; a < cl.na; ++a) im[a] = 1.0 / o.mass[cl.atom[a]];
+    double J[3][3] = {}, rhs[3] = {}, lam[3];
+    for (int k = 0; k < cl.nc; ++k) {
+      const int ga = cl.atom[cl.ca[k]], gb = cl.atom[cl.cb[k]];
+      for (int c = 0; c < 3; ++c) rd[k][c] = pos[3 * ga + c] - pos[3 * gb + c];
+      minimg(rd[k], o.s.box);
+    }
+    for (int k = 0; k < cl.nc; ++k) {
+      const int a = cl.ca[k], b = cl.cb[k];
+      const int ga = cl.atom[a], gb = cl.atom[b];
+      double vab[3], aab[3];
+      for (int c = 0; c < 3; ++c) {
+        vab[c] = vel[3 * ga + c] - vel[3 * gb + c];
+        aab[c] = f[3 * ga + c] * im[a] - f[3 * gb + c] * im[b];
+      }
+      rhs[k] = -dot3(vab, vab) - dot3(rd[k], aab);
+      for (int l = 0; l < cl.nc; ++l) {
+        double coef = 0;
+        if (cl.ca[l] == a) coef += im[a];
+        if (cl.cb[l] == a) coef -= im[a];
+        if (cl.ca[l] == b) coef -= im[b];
+        if (cl.cb[l] == b) coef += im[b];
+        J[k][l] = coef * dot3(rd[l], rd[k]);
+      }
+    }
+    if (!gauss_solve(cl.nc, J, rhs, lam)) continue;
+    for (int k = 0; k < cl.nc; ++k)
+      for (int c = 0; c < 3; ++c) vir[c] += lam[k] * rd[k][c] * rd[k][c];
+  }
+}
+
+const double kPUo = 1.4586e-5;             // atm -> kcal/mol/A^3 (src/defs.in.h:105)
+const double kPatmO = 68558.64100846418;   // kcal/mol/A^3 -> atm (src/cell_based_kernels.cu:584)
+
+}  // namespace
+
+extern "C" {
+
+int orc_virial_fd(void* h, const double* pos, double hrel, int terms, int group, double* vir3) {
+  virial_fd(*(Orc*)h, pos, hrel, terms, vir3, group);
+  return 0;
+}
+
+int orc_constraint_virial(void* h, const double* pos, const double* vel, const double* f, double* vir3) {
+  vir3[0] = vir3[1] = vir3[2] = 0.0;
+  constraint_virial(*(Orc*)h, pos, vel, f, vir3);
+  return 0;
+}
+
+double orc_group_pressure(void* h, const double* pos, const double* vel, double hrel) {
+  const Orc& o = *(Orc*)h;
+  double w[3];
+  virial_fd(o, pos, hrel, ORC_T_ALL, w, 1);
+  const double V = o.s.box[0] * o.s.box[1] * o.s.box[2];
+  return (2.0 * com_kinetic(o, units_of(o), vel) + w[0] + w[1] + w[2]) / (3.0 * V) * kPatmO;
+}
+
+int orc_npt(void* h, double* pos, double* vel, double* box3, double* lstate, int nsteps, double dt_ps, double tol,
+            double pref_atm, double pmass, double hrel, double* Ltrace, double* Ptrace) {
+  Orc w = *(Orc*)h;  // works on a copy whose box follows the piston
+  const int n = w.s.n;
+  const double dt = dt_ps * ORC_TU;
+  for (int d = 0; d < 3; ++d) w.s.box[d] = box3[d];
+  const double ratio[3] = {1.0, box3[1] / box3[0], box3[2] / box3[0]};
+  double Ldot = lstate[0], Lacc = lstate[1];
+  const std::vector<std::vector<int>> units = units_of(w);
+  std::vector<double> f(3 * (size_t)n, 0.0), ref(3 * (size_t)n), R(3 * units.size());
+  double e[ORC_NE];
+  orc_forces(&w, pos, f.data(), e, ORC_T_ALL);
+  int bad = 0;
+  for (int s = 0; s < nsteps; ++s) {
+    const double L = w.s.box[0];
+    Ldot += 0.5 * dt * Lacc;
+    const double Ln = L + dt * Ldot, lam = Ln / L;
+    scale_com(w, units, vel, std::exp(-0.5 * dt * Ldot / L));
+    // each atom moves by (lam - 1) x its unit's mass centre taken in the atom's own
+    // periodic image, so the unit moves rigidly even when its atoms are wrapped apart
+    for (size_t k = 0; k < units.size(); ++k) {
+      centre(w, units[k], pos, &R[3 * k]);
+      const int a0 = units[k][0];
+      for (int i : units[k]) {
+        double d[3] = {pos[3 * i] - pos[3 * a0], pos[3 * i + 1] - pos[3 * a0 + 1], pos[3 * i + 2] - pos[3 * a0 + 2]};
+        double dm[3] = {d[0], d[1], d[2]};
+        minimg(dm, w.s.box);
+        for (int c = 0; c < 3; ++c)  // R + (d - dm): the centre's image next to atom i
+          ref[3 * i + c] = pos[3 * i + c] + (lam - 1.0) * (R[3 * k + c] + d[c] - dm[c]);
+      }
+    }
+    for (int d = 0; d < 3; ++d) w.s.box[d] = Ln * ratio[d];
+    for (int i = 0; i < n; ++i)
+      for (int c = 0; c < 3; ++c) {
+        vel[3 * i + c] += 0.5 * dt * f[3 * i + c] / w.mass[i];
+        pos[3 * i + c] = ref[3 * i + c] + dt * vel[3 * i + c];
+      }
+    for (const Cluster& cl : w.clusters) bad += shake_cluster(w, cl, ref.data(), pos, vel, dt, tol, 1000) != 0;
+    const double kc = com_kinetic(w, units, vel);
+    std::fill(f.begin(), f.end(), 0.0);
+    orc_forces(&w, pos, f.data(), e, ORC_T_ALL);
+    double wf[3];
+    virial_fd(w, pos, hrel, ORC_T_ALL, wf, 1);
+    const double V = w.s.box[0] * w.s.box[1] * w.s.box[2];
+    const double P = (2.0 * kc + wf[0] + wf[1] + wf[2]) / (3.0 * V);
+    Lacc = (P - pref_atm * kPUo) / (3.0 * pmass * Ln * Ln) - 2.0 * Ldot * Ldot / Ln;
+    Ldot += 0.5 * dt * Lacc;
+    for (int i = 0; i < n; ++i)
+      for (int c = 0; c < 3; ++c) vel[3 * i + c] += 0.5 * dt * f[3 * i + c] / w.mass[i];
+    scale_com(w, units, vel, std::exp(-0.5 * dt * Ldot / Ln));
+    for (const Cluster& cl : w.clusters) rattle_cluster(w, cl, pos, vel);
+    if (Ltrace) Ltrace[s] = Ln;
+    if (Ptrace) Ptrace[s] = P * kPatmO;
+  }
+  for (int d = 0; d < 3; ++d) box3[d] = w.s.box[d];
+  lstate[0] = Ldot;
+  lstate[1] = Lacc;
+  return bad;
+}
+
+}  // extern "C"

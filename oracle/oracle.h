@@ -111,6 +111,23 @@ void orc_reassign_velocities(void* h, const double* pos, double T, uint64_t seed
 /* the raw counter-based normal deviates used above: out[3n] */
 void orc_normals(int n, uint64_t seed, uint32_t counter, double* out);
 
+/* virial diagonal W_aa = -L_a dU/dL_a (central differences, relative step hrel) of the
+ * selected terms at the oracle's box: atoms scaled (group = 0, the atomic virial) or the
+ * mass centres of the integration units (SHAKE clusters and free atoms) scaled with the
+ * units moved rigidly (group = 1, the group virial) */
+int orc_virial_fd(void* h, const double* pos, double hrel, int terms, int group, double* vir3);
+/* instantaneous constraint virial for positions, velocities and forces f[3n] */
+int orc_constraint_virial(void* h, const double* pos, const double* vel, const double* f, double* vir3);
+/* pressure (atm) of the unit centres: (2 KE_centres + W_group) / (3 V) */
+double orc_group_pressure(void* h, const double* pos, const double* vel, double hrel);
+/* Andersen barostat steps with the integration units as scaling groups (the product's
+ * splitting: piston half kick, centre-of-mass friction, rigid unit scaling,
+ * kick/drift/SHAKE, group pressure from the half-step velocities, piston half kick,
+ * kick, friction, RATTLE).  box3 and lstate = {L', L''} in/out; traces of L (x edge)
+ * and P (atm) per step (may be NULL). */
+int orc_npt(void* h, double* pos, double* vel, double* box3, double* lstate, int nsteps, double dt_ps, double tol,
+            double pref_atm, double pmass, double hrel, double* Ltrace, double* Ptrace);
+
 #ifdef __cplusplus
 }
 #endif

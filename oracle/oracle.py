@@ -46,6 +46,12 @@ def _lib():
     lib.orc_md.argtypes = [C.c_void_p, dp, dp, C.c_int, C.c_double, C.c_double, dp, dp, dp]
     lib.orc_reassign_velocities.argtypes = [C.c_void_p, dp, C.c_double, C.c_uint64, C.c_uint32, dp]
     lib.orc_normals.argtypes = [C.c_int, C.c_uint64, C.c_uint32, dp]
+    lib.orc_virial_fd.argtypes = [C.c_void_p, dp, C.c_double, C.c_int, C.c_int, dp]
+    lib.orc_group_pressure.restype = C.c_double
+    lib.orc_group_pressure.argtypes = [C.c_void_p, dp, dp, C.c_double]
+    lib.orc_constraint_virial.argtypes = [C.c_void_p, dp, dp, dp, dp]
+    lib.orc_npt.argtypes = [C.c_void_p, dp, dp, dp, dp, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                            C.c_double, dp, dp]
     return lib
 
 
@@ -176,6 +182,47 @@ class Oracle:
         bad = lib().orc_md(self.h, _dp(p), _dp(v), int(nsteps), float(dt_ps), float(tol), _dp(f),
                            _dp(ep) if traces else None, _dp(ek) if traces else None)
         return dict(pos=p, vel=v, f=f, epot=ep[:nsteps], ekin=ek[:nsteps], bad=bad)
+
+    def virial_fd(self, pos, hrel=1e-6, terms=T_ALL, group=False):
+        """Diagonal virial -L_a dU/dL_a by central differences: atomic scaling, or the
+        integration units' mass centres scaled with rigid units (group=True)."""
+        p = np.ascontiguousarray(pos, np.float64)
+        out = np.zeros(3)
+        lib().orc_virial_fd(self.h, _dp(p), float(hrel), int(terms), 1 if group else 0, _dp(out))
+        return out
+
+    def group_pressure(self, pos, vel, hrel=1e-6):
+        p = np.ascontiguousarray(pos, np.float64)
+        v = np.ascontiguousarray(vel, np.float64)
+        return float(lib().orc_group_pressure(self.h, _dp(p), _dp(v), float(hrel)))
+
+    def constraint_virial(self, pos, vel, f):
+        p = np.ascontiguousarray(pos, np.float64)
+        v = np.ascontiguousarray(vel, np.float64)
+        ff = np.ascontiguousarray(f, np.float64)
+        out = np.zeros(3)
+        lib().orc_constraint_virial(self.h, _dp(p), _dp(v), _dp(ff), _dp(out))
+        return out
+
+    def pressure(self, pos, vel, hrel=1e-6):
+        """Instantaneous pressure (atm) and virial: (2 KE + W_forces + W_constraints) / (3 V)."""
+        f, _ = self.forces(pos)
+        w = self.virial_fd(pos, hrel) + self.constraint_virial(pos, vel, f)
+        box = np.asarray(self.topo["box"], np.float64)
+        V = float(np.prod(box))
+        return (2.0 * self.kinetic(vel) + w.sum()) / (3.0 * V) * 68558.64100846418, w
+
+    def npt(self, pos, vel, box, lstate, nsteps, dt_ps=0.001, tol=1e-10, pref_atm=1.0, pmass=1e-5, hrel=1e-6):
+        """Andersen barostat steps; returns the final state and per-step L and P traces."""
+        p = np.ascontiguousarray(pos, np.float64).copy()
+        v = np.ascontiguousarray(vel, np.float64).copy()
+        b = np.ascontiguousarray(box, np.float64).copy()
+        ls = np.ascontiguousarray(lstate, np.float64).copy()
+        Lt = np.zeros(max(1, nsteps))
+        Pt = np.zeros(max(1, nsteps))
+        bad = lib().orc_npt(self.h, _dp(p), _dp(v), _dp(b), _dp(ls), int(nsteps), float(dt_ps), float(tol),
+                            float(pref_atm), float(pmass), float(hrel), _dp(Lt), _dp(Pt))
+        return dict(pos=p, vel=v, box=b, lstate=ls, L=Lt[:nsteps], P=Pt[:nsteps], bad=bad)
 
     def reassign_velocities(self, pos, T, seed, counter=0):
         p = np.ascontiguousarray(pos, np.float64)

@@ -3,6 +3,8 @@ import ctypes
 import os
 import re
 
+import pytest
+
 import fenzi_b200 as fz
 
 HDR = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "fenzi_b200.h")
@@ -40,3 +42,16 @@ def test_device_calls_before_upload_fail_cleanly():
         assert e.code == 7
     else:
         raise AssertionError("expected FZ_ERR_STATE")
+
+
+def test_server_without_gpu_fails_cleanly():
+    """No device: fz_server_create returns an error status (no worker thread starts)."""
+    import ctypes as C
+    L = fz.lib()
+    h = C.c_void_p()
+    code = L.fz_server_create(0, 1e9, 10, 2, C.byref(h))
+    if code == 0:  # a GPU is present: nothing to check here
+        L.fz_server_free(h)
+        pytest.skip("a CUDA device is present")
+    assert code in (3, 6)  # FZ_ERR_CUDA / FZ_ERR_ARG
+    assert fz.last_error()

@@ -57,6 +57,24 @@ def test_pme_matches_oracle(key):
     assert err <= 5e-5, err
 
 
+@pytest.mark.parametrize("K", [6, 10, 12])
+def test_pme_small_and_odd_grids(K):
+    """Grids of one brick per dimension (K = 6: the spread region wraps onto its own
+    brick), of edge-5 bricks (K = 10) and of edge-4 bricks (K = 12); all three use
+    the runtime FFT plan (no compile-time kernel for these sizes)."""
+    _, path = system(f"tiny_k{K}", name="custom", nw=60, nchains=1, chain_len=8, box=14.0, kgrid=K, rc=6.0,
+                     ron=5.0, seed=3)
+    s = fz.FenZi.ReadInput(path).LoadSystem()
+    s.InitMem(0)
+    orc = oracle_for(s)
+    s.ComputeAccelGPU(terms=fz.TERM_PME)
+    f = s.forces()
+    f0, _ = orc.forces(s.positions(), O.T_PME)
+    err = rel_rms(f, f0)
+    assert err <= 5e-5, err
+    s.close()
+
+
 def test_pme_vs_direct_ewald():
     """PME force error against a converged direct Ewald sum, relative to the total
     electrostatic force (real space + reciprocal): 3,000 TIP3P in 44.8 A, 48^3, beta 0.34."""

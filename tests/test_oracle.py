@@ -101,3 +101,73 @@ def test_pair_count_matches_brute_force():
     mol = np.arange(s.n) // 3
     close = (r2[iu] < 36.0) & (mol[iu[0]] != mol[iu[1]])
     assert orc.count_pairs(s.pos, 6.0) == int(close.sum())
+
+
+@pytest.fixture(scope="module")
+def npt_sys():
+    # beta 0.6: erfc(beta rc) ~ 3e-9, so the real-space cutoff step does not spoil the
+    # finite-difference virial
+    s = gen_system.build(name="custom", nw=80, nchains=1, chain_len=12, box=16.0, kgrid=16, rc=7.0, ron=5.5,
+                         beta=0.6, seed=23)
+    return s, gen_system.topology(s)
+
+
+def test_virial_fd_matches_bond_sum(npt_sys):
+    """-L_a dU/dL_a of the bond energy equals sum f_a d_a over the bonds."""
+    s, topo = npt_sys
+    orc = O.Oracle(topo)
+    w = orc.virial_fd(s.pos, 1e-6, O.T_BOND)
+    b = topo["bond"]
+    d = s.pos[b[:, 0]] - s.pos[b[:, 1]]
+    d -= np.round(d / topo["box"]) * topo["box"]
+    r = np.linalg.norm(d, axis=1)
+    f = -2.0 * topo["bond_k"] * (r - topo["bond_r0"]) / r
+    ref = (f[:, None] * d * d).sum(0)
+    np.testing.assert_allclose(w, ref, rtol=1e-6, atol=1e-6)
+
+
+def _enthalpy(topo, run, pos, vel, pref_atm, pmass):
+    t = dict(topo)
+    t["box"] = np.asarray(run["box"], float)
+    o = O.Oracle(t)
+    _, e = o.forces(pos)
+    L, Ldot = run["box"][0], run["lstate"][0]
+    V = float(np.prod(run["box"]))
+    rho = (run["box"][1] / L) * (run["box"][2] / L)
+    return sum(e.values()) + o.kinetic(vel) + pref_atm * 1.4586e-5 * V + 0.5 * pmass * rho * (3 * L * L * Ldot) ** 2
+
+
+def test_oracle_npt_conserves_enthalpy(npt_sys):
+    """Andersen barostat (oracle): H = U + KE + Pref V + piston KE stays flat while the
+    box moves (by ~5% here: the lattice start is far from 1 atm)."""
+    s, topo = npt_sys
+    orc = O.Oracle(topo)
+    v = orc.reassign_velocities(s.pos, 300.0, 5, 0)
+    P0 = orc.group_pressure(s.pos, v)  # atm
+    pmass = 2e-5
+    L0 = topo["box"][0]
+    lacc = (P0 - 1.0) * 1.4586e-5 / (3 * pmass * L0 * L0)
+    state = dict(pos=s.pos.copy(), vel=v, box=np.array(topo["box"], float), lstate=np.array([0.0, lacc]))
+    hs, Ls = [], []
+    for _ in range(8):
+        run = orc.npt(state["pos"], state["vel"], state["box"], state["lstate"], 15, dt_ps=0.0005, tol=1e-12,
+                      pref_atm=1.0, pmass=pmass)
+        assert run["bad"] == 0
+        state = run
+        hs.append(_enthalpy(topo, run, run["pos"], run["vel"], 1.0, pmass))
+        Ls.append(run["box"][0])
+    ke = orc.kinetic(state["vel"])
+    assert np.ptp(hs) < 3e-3 * ke, (np.ptp(hs), ke)
+    assert np.ptp(Ls) > 0.1, Ls  # the box moved
+
+
+def test_atomic_and_group_pressure_agree_for_rigid_water():
+    """For rigid units (SHAKE-constrained TIP3P) the atomic pressure, with the
+    instantaneous constraint virial, equals the pressure of the unit centres at every
+    instant: the intra-unit virial is exactly -2 x the internal kinetic energy."""
+    s = gen_system.build(name="custom", nw=90, nchains=0, box=14.5, kgrid=16, rc=6.5, ron=5.0, beta=0.65, seed=29)
+    orc = O.Oracle(gen_system.topology(s))
+    v = orc.reassign_velocities(s.pos, 300.0, 9, 0)
+    pa, _ = orc.pressure(s.pos, v)
+    pg = orc.group_pressure(s.pos, v)
+    assert abs(pa - pg) < 1e-3 * max(abs(pg), 100.0), (pa, pg)
