@@ -193,9 +193,8 @@ def served_jobs(njobs, seed):
     t = 0.0
     for i in range(njobs):
         natom = int(rng.integers(1500, 30001))
-        nch = int(rng.integers(0, 41))
-        nch = min(nch, max(0, (natom - 600) // 30))
-        nw = max(200, (natom - 30 * nch) // 3)
+        nch = min(int(rng.integers(0, 41)), natom // 120)  # chains at most a quarter of the atoms
+        nw = (natom - 30 * nch) // 3
         steps = int(round(float(np.exp(rng.uniform(np.log(1000), np.log(20000))))))
         nvt = bool(rng.integers(0, 2))
         t += float(rng.exponential(1.0 / 200.0))
@@ -217,8 +216,9 @@ def bench_served(device, njobs=32, seed=4242, check=4):
     root = tempfile.mkdtemp(prefix="fzserve_")
     paths = []
     for i, j in enumerate(jobs):
-        g = gen_system.build(name=f"job{i:02d}", nw=j["nw"], nchains=j["nchains"], chain_len=30, rc=10.0, ron=8.0,
-                             seed=j["seed"])
+        box = (j["nw"] / 0.0334 + 15.0 * 30 * j["nchains"]) ** (1.0 / 3.0)  # ~15 A^3 per chain atom
+        g = gen_system.build(name=f"job{i:02d}", nw=j["nw"], nchains=j["nchains"], chain_len=30, box=box, rc=10.0,
+                             ron=8.0, seed=j["seed"])
         paths.append(gen_system.write(g, os.path.join(root, f"j{i:02d}")))
 
     def load(i):
