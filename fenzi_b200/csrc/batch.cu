@@ -119,23 +119,24 @@ static fz_status capture(fz_batch* b) {
   FZ_CUDA(cudaMallocHost(&b->pinned_status, sizeof(int) * ns));
   FZ_CUDA(cudaStreamBeginCapture(b->master, cudaStreamCaptureModeThreadLocal));
   FZ_CUDA(cudaEventRecord(b->ev_start, b->master));
+  cudaError_t cap = cudaSuccess;
   for (int i = 0; i < ns; ++i) {
     Engine* e = b->systems[i]->eng;
     FZ_CUDA(cudaStreamWaitEvent(e->st, b->ev_start, 0));
     const long long l0 = e->launches;
+    e->capture_error = cudaSuccess;
     e->step_body();
+    if (e->capture_error != cudaSuccess) cap = e->capture_error;
     e->launches = l0;
     FZ_CUDA(cudaEventRecord(b->ev_done[i], e->st));
     FZ_CUDA(cudaStreamWaitEvent(b->master, b->ev_done[i], 0));
   }
   FZ_CUDA(cudaStreamEndCapture(b->master, &b->graph));
+  if (cap != cudaSuccess) return fail(FZ_ERR_CUDA, std::string("batch capture: ") + cudaGetErrorString(cap));
   FZ_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
   return FZ_OK;
 }
 
-static long long step_launches(const Engine* e) {
-  return 2 + 11 + 1 + ((e->nbond + e->nangle + e->nub + e->ndihe + e->nimpr + e->nexcl + e->n14 > 0) ? 1 : 0) + 12;
-}
 
 extern "C" fz_status fz_batch_step(fz_batch* b, int nsteps) {
   if (!b || nsteps < 0) return fail(FZ_ERR_ARG, "bad argument");
@@ -160,7 +161,8 @@ extern "C" fz_status fz_batch_step(fz_batch* b, int nsteps) {
     for (int i = 0; i < ns; ++i) {
       Engine* e = b->systems[i]->eng;
       e->step += k;
-      e->launches += (long long)k * step_launches(e);
+      e->launches += (long long)k * e->graph_step_launches();
+      e->graph_since_check = true;
       if (e->temp_reset_every > 0 && e->step % e->temp_reset_every == 0) {
         FZ_CUDA(cudaEventRecord(b->ev_master, b->master));
         FZ_CUDA(cudaStreamWaitEvent(e->st, b->ev_master, 0));

@@ -63,6 +63,14 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
     e->own_stream = true;
   }
   FZ_CUDA(cudaStreamCreateWithFlags(&e->st2, cudaStreamNonBlocking));
+  FZ_CUDA(cudaStreamCreateWithFlags(&e->st_cap, cudaStreamNonBlocking));
+  {
+    // conditional IF nodes for the neighbour kernels inside captured steps: measured
+    // ~12 us per step slower on B200 at 230,400 atoms than the flag-checking kernels
+    // they replace, so they are off unless FZ_GRAPH_COND=1
+    const char* v = std::getenv("FZ_GRAPH_COND");
+    e->cond_graph = v && std::atoi(v) == 1;
+  }
   FZ_CUDA(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
   FZ_CUDA(cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming));
   const int n = t.n;
@@ -143,11 +151,13 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
   e->ncons = (int)t.cons_d.size();
   int dev_sms = 148;
   cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device);
-  // pair kernel CTAs per SM (3 = register-limited maximum); PME overlaps it on a second stream
+  // pair kernel CTAs per SM: 3 (80-register build) or 4 (64-register build), env
+  // FZ_NB_CTAS_PER_SM; PME overlaps it on a second stream
   {
     const char* v = std::getenv("FZ_NB_CTAS_PER_SM");
-    const int per = v ? std::max(1, std::min(3, std::atoi(v))) : 3;
+    const int per = v ? std::max(1, std::min(4, std::atoi(v))) : 3;
     e->nb_grid = dev_sms * per;
+    e->nb_per_sm = per;
   }
   // ---- atom arrays
   std::vector<float4> pos4(n), vel4(n);
@@ -249,22 +259,36 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
     std::vector<int4> ua;
     std::vector<int> um;
     std::vector<float4> ud;
+    // grouped by class (atoms, constraints): each class is one integrator launch with
+    // its loops fixed at compile time
+    e->ncls = 0;
+    auto open_class = [&](int na, int nc) {
+      if (e->ncls > 0 && e->cls_na[e->ncls - 1] == na && e->cls_nc[e->ncls - 1] == nc) return;
+      e->cls_na[e->ncls] = na;
+      e->cls_nc[e->ncls] = nc;
+      e->cls_begin[e->ncls] = (int)ua.size();
+      e->ncls++;
+    };
     for (int i = 0; i < n; ++i)
       if (!in_cl[i]) {
+        open_class(1, 0);
         ua.push_back(make_int4(i, -1, -1, -1));
         um.push_back(1);
         ud.push_back(make_float4(0.f, 0.f, 0.f, 0.f));
       }
     for (int na = 2; na <= 4; ++na)
-      for (const auto& cl : t.clusters) {
-        if (cl.na != na) continue;
-        ua.push_back(make_int4(cl.atom[0], cl.atom[1], cl.atom[2], cl.atom[3]));
-        int meta = cl.na | (cl.nc << 4);
-        for (int k = 0; k < cl.nc; ++k) meta |= (cl.ca[k] << (8 + 4 * k)) | (cl.cb[k] << (10 + 4 * k));
-        um.push_back(meta);
-        ud.push_back(make_float4((float)cl.d[0], (float)cl.d[1], (float)cl.d[2], 0.f));
-      }
+      for (int nc = 1; nc <= 3; ++nc)
+        for (const auto& cl : t.clusters) {
+          if (cl.na != na || cl.nc != nc) continue;
+          open_class(na, nc);
+          ua.push_back(make_int4(cl.atom[0], cl.atom[1], cl.atom[2], cl.atom[3]));
+          int meta = cl.na | (cl.nc << 4);
+          for (int k = 0; k < cl.nc; ++k) meta |= (cl.ca[k] << (8 + 4 * k)) | (cl.cb[k] << (10 + 4 * k));
+          um.push_back(meta);
+          ud.push_back(make_float4((float)cl.d[0], (float)cl.d[1], (float)cl.d[2], 0.f));
+        }
     e->nunits = (int)ua.size();
+    e->cls_begin[e->ncls] = e->nunits;
     if ((r = e->upload(&e->unit_atoms, ua)) || (r = e->upload(&e->unit_meta, um)) || (r = e->upload(&e->unit_d, ud)))
       return r;
   }

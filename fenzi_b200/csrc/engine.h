@@ -28,7 +28,7 @@ struct Engine {
   int n = 0, nunits = 0, ncol = 0, nslots = 0, mask_cap = 0, all_images = 0;
   int ocap = 0;            // per-block pair-list capacity (multiple of 32)
   float rp2 = 0.f, prune_half2 = 0.f;
-  int nb_grid = 0;
+  int nb_grid = 0, nb_per_sm = 3;
   int dcx = 1, dcy = 1;
   int* blk_col = nullptr;
   std::vector<void*> allocs;
@@ -54,7 +54,8 @@ struct Engine {
   int4 *angle = nullptr, *dihe = nullptr, *impr = nullptr;
   float2 *bond_prm = nullptr, *angle_prm = nullptr, *ub_prm = nullptr, *impr_prm = nullptr;
   float4* dihe_prm = nullptr;
-  // integration units
+  // integration units, grouped in classes of equal (atoms, constraints)
+  int ncls = 0, cls_na[8] = {}, cls_nc[8] = {}, cls_begin[9] = {};
   int4* unit_atoms = nullptr;
   int* unit_meta = nullptr;
   float4* unit_d = nullptr;
@@ -88,6 +89,14 @@ struct Engine {
   cudaGraph_t step_graph = nullptr;
   cudaGraphExec_t step_exec = nullptr;
   bool use_graph = true;
+  // With cond_graph (env FZ_GRAPH_COND=1) the rebuild and prune kernels of captured
+  // steps are the bodies of two conditional IF nodes set from the device flags, else
+  // flag-checking kernels launched every step; st_cap captures the bodies.
+  bool cond_graph = false;
+  cudaStream_t st_cap = nullptr;
+  cudaError_t capture_error = cudaSuccess;
+  long long seen_rb_launch = 0, seen_pr_launch = 0;  // device counters already accounted
+  bool graph_since_check = false;                     // captured steps ran since check()
   // PME runs on a second stream concurrently with the pair and bonded kernels
   cudaStream_t st2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -154,6 +163,7 @@ struct Engine {
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
     if (st2) cudaStreamDestroy(st2);
+    if (st_cap) cudaStreamDestroy(st_cap);
     for (auto& x : ev)
       if (x) cudaEventDestroy(x);
     for (void* p : allocs) cudaFree(p);
@@ -223,6 +233,7 @@ struct Engine {
     a.items = items;
     a.chunk = chunk;
     a.grid = nb_grid;
+    a.minb = nb_per_sm;
     return a;
   }
   fzk::PmeArgs pme_args() const {
@@ -309,6 +320,14 @@ struct Engine {
     a.shake_maxit = 500;
     a.lam = 1.0;
     a.vfric = 1.0;
+    a.u_begin = 0;
+    a.u_end = nunits;
+    a.ncls = ncls;
+    for (int c = 0; c < 8; ++c) {
+      a.cls_na[c] = cls_na[c];
+      a.cls_nc[c] = cls_nc[c];
+    }
+    for (int c = 0; c < 9; ++c) a.cls_begin[c] = cls_begin[c];
     return a;
   }
 
@@ -352,9 +371,70 @@ struct Engine {
     stage_ms[4] += el(0, 1) + el(5, 6);
     timed_steps++;
   }
+  // Adds to the capture on st an IF node that runs body(stream) when *dflag != 0.
+  template <class F>
+  void conditional(const int* dflag, F body) {
+    cudaStreamCaptureStatus cs;
+    unsigned long long id;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    cudaGraphConditionalHandle h;
+    cudaError_t e = cudaStreamGetCaptureInfo(st, &cs, &id, &g, &deps, &nd);
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, g, 0, 0);
+    if (e != cudaSuccess) {
+      capture_error = e;
+      return;
+    }
+    fzk::launch_set_condition(h, dflag, st);
+    e = cudaStreamGetCaptureInfo(st, &cs, &id, &g, &deps, &nd);
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeIf;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, deps, nd, &np);
+    if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
+    if (e == cudaSuccess)
+      e = cudaStreamBeginCaptureToGraph(st_cap, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+      capture_error = e;
+      return;
+    }
+    body(st_cap);
+    cudaGraph_t out = nullptr;
+    e = cudaStreamEndCapture(st_cap, &out);
+    if (e != cudaSuccess) capture_error = e;
+  }
+  // neighbour maintenance: conditional nodes inside a capture, else flag-checking kernels
+  void rebuild_step() {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    const fzk::RebuildArgs ra = rebuild_args();
+    if (cond_graph && st_cap && cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusActive) {
+      conditional(flag, [&](cudaStream_t s) { fzk::launch_rebuild_build(ra, s); });
+      conditional(flag_prune, [&](cudaStream_t s) { fzk::launch_rebuild_prune(ra, s); });
+    } else {
+      fzk::launch_rebuild(ra, st);
+    }
+  }
+  // kernels one captured step launches besides the conditional bodies
+  long long graph_step_launches() const {
+    return 2 + (cond_graph ? 2 : 11) + 1 + ((nbond + nangle + nub + ndihe + nimpr + nexcl + n14 > 0) ? 1 : 0) + 12;
+  }
+  // launches of the conditional bodies (8 per rebuild, 3 per prune) since the last
+  // call, from the device counters; called after a synchronisation
+  void account_conditional(const int* cnt) {
+    if (cond_graph && graph_since_check)
+      launches += 8 * (cnt[fzk::CNT_REBUILDS] - seen_rb_launch) + 3 * (cnt[fzk::CNT_PRUNES] - seen_pr_launch);
+    graph_since_check = false;
+    seen_rb_launch = cnt[fzk::CNT_REBUILDS];
+    seen_pr_launch = cnt[fzk::CNT_PRUNES];
+  }
   // forces with PME on st2, overlapping the pair and bonded kernels on st
   void forces_overlapped() {
-    fzk::launch_rebuild(rebuild_args(), st);
+    rebuild_step();
     cudaEventRecord(ev_fork, st);
     cudaStreamWaitEvent(st2, ev_fork, 0);
     fzk::launch_pme(pme_args(), false, st2);
@@ -374,6 +454,7 @@ struct Engine {
   }
   fz_status graph_step() {
     if (!step_exec) {
+      capture_error = cudaSuccess;
       FZ_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
       const long long l0 = launches;
       step_body();
@@ -381,10 +462,13 @@ struct Engine {
       cudaGraph_t g = nullptr;
       FZ_CUDA(cudaStreamEndCapture(st, &g));
       step_graph = g;
+      if (capture_error != cudaSuccess)
+        return fail(FZ_ERR_CUDA, std::string("step capture: ") + cudaGetErrorString(capture_error));
       FZ_CUDA(cudaGraphInstantiate(&step_exec, step_graph, 0));
     }
     FZ_CUDA(cudaGraphLaunch(step_exec, st));
-    launches += 2 + 11 + 1 + ((nbond + nangle + nub + ndihe + nimpr + nexcl + n14 > 0) ? 1 : 0) + 12;
+    launches += graph_step_launches();
+    graph_since_check = true;
     return FZ_OK;
   }
   void drop_graph() {
@@ -395,9 +479,12 @@ struct Engine {
   }
   fz_status check() {
     int h = 0;
+    int cnt[fzk::CNT_COUNT];
     FZ_CUDA(cudaMemcpyAsync(&h, status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    FZ_CUDA(cudaMemcpyAsync(cnt, counters, sizeof(cnt), cudaMemcpyDeviceToHost, st));
     FZ_CUDA(cudaStreamSynchronize(st));
     FZ_CUDA(cudaGetLastError());
+    account_conditional(cnt);
     if (h) {
       std::string m = "device status:";
       if (h & fzk::ST_TILE_OVERFLOW) m += " pair-tile capacity exceeded;";

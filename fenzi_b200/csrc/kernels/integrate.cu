@@ -6,6 +6,8 @@
 // read by the neighbour kernels, so no host synchronisation is needed per step.
 // Constraint solves run in FP64 with an iteration cap (the reference loops without one,
 // src/shake.cu:195-271) and report non-convergence in the status word.
+#include <type_traits>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -18,6 +20,10 @@ struct Unit {
   double d[3];
 };
 
+// NA, NC > 0: the unit's class (atoms, constraints) is known at compile time, so the
+// per-atom loops below fold to that size and the unit's arrays stay small in
+// registers; NA = 0 reads both from the unit's metadata.
+template <int NA, int NC>
 __device__ __forceinline__ Unit load_unit(const IntegrateArgs& a, int u) {
   Unit U;
   const int4 at = a.unit_atoms[u];
@@ -27,8 +33,8 @@ __device__ __forceinline__ Unit load_unit(const IntegrateArgs& a, int u) {
   U.atom[1] = at.y;
   U.atom[2] = at.z;
   U.atom[3] = at.w;
-  U.na = meta & 15;
-  U.nc = (meta >> 4) & 15;
+  U.na = NA > 0 ? NA : meta & 15;
+  U.nc = NA > 0 ? NC : (meta >> 4) & 15;
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     U.ca[k] = (meta >> (8 + 4 * k)) & 3;
@@ -90,6 +96,7 @@ __device__ __forceinline__ void bond_vec(const Unit& U, int k, const double x[4]
   out[0] = out[1] = out[2] = 0.0;
 #pragma unroll
   for (int at = 0; at < 4; ++at) {
+    if (at >= U.na) continue;
     const double sg = sgn(U, k, at);
 #pragma unroll
     for (int c = 0; c < 3; ++c) out[c] += sg * x[at][c];
@@ -105,7 +112,8 @@ __device__ __forceinline__ void coef_matrix(const Unit& U, const double* im, dou
     for (int l = 0; l < 3; ++l) {
       double c = 0.0;
 #pragma unroll
-      for (int at = 0; at < 4; ++at) c += sgn(U, k, at) * sgn(U, l, at) * im[at];
+      for (int at = 0; at < 4; ++at)
+        if (at < U.na) c += sgn(U, k, at) * sgn(U, l, at) * im[at];
       cf[k][l] = c;
     }
 }
@@ -114,8 +122,8 @@ __device__ __forceinline__ void coef_matrix(const Unit& U, const double* im, dou
 // the reference bond vectors (src/shake.cu:159-271).  With s_k the unconstrained bond
 // vector and c_kl the inverse-mass coupling of constraints k and l,
 // C_k = s_k + sum_l c_kl lambda_l rd_l.  rn: unconstrained positions (in/out).
-__device__ int shake_unit(const Unit& U, const double rref[4][3], double rn[4][3], const double* im,
-                          const IntegrateArgs& a) {
+__device__ __forceinline__ int shake_unit(const Unit& U, const double rref[4][3], double rn[4][3], const double* im,
+                                          const IntegrateArgs& a) {
   double rd[3][3], s0[3][3], cf[3][3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
@@ -156,6 +164,7 @@ __device__ int shake_unit(const Unit& U, const double rref[4][3], double rn[4][3
   for (int at = 0; at < 4; ++at)
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
+      if (at >= U.na) continue;
       const double w = (k < nc) ? sgn(U, k, at) * lam[k] * im[at] : 0.0;
 #pragma unroll
       for (int c = 0; c < 3; ++c) rn[at][c] += w * rd[k][c];
@@ -164,8 +173,8 @@ __device__ int shake_unit(const Unit& U, const double rref[4][3], double rn[4][3
 }
 
 // RATTLE velocity stage: (v_a - v_b) . r_ab = 0, linear, solved directly
-__device__ void rattle_unit(const Unit& U, const double r[4][3], double v[4][3], const double* im,
-                            const IntegrateArgs& a) {
+__device__ __forceinline__ void rattle_unit(const Unit& U, const double r[4][3], double v[4][3], const double* im,
+                                            const IntegrateArgs& a) {
   double rd[3][3], vd[3][3], cf[3][3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
@@ -173,6 +182,7 @@ __device__ void rattle_unit(const Unit& U, const double r[4][3], double v[4][3],
     vd[k][0] = vd[k][1] = vd[k][2] = 0.0;
 #pragma unroll
     for (int at = 0; at < 4; ++at) {
+      if (at >= U.na) continue;
       const double sg = sgn(U, k, at);
 #pragma unroll
       for (int c = 0; c < 3; ++c) vd[k][c] += sg * v[at][c];
@@ -191,6 +201,7 @@ __device__ void rattle_unit(const Unit& U, const double r[4][3], double v[4][3],
   for (int at = 0; at < 4; ++at)
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
+      if (at >= U.na) continue;
       const double w = (k < U.nc) ? sgn(U, k, at) * mu[k] * im[at] : 0.0;
 #pragma unroll
       for (int c = 0; c < 3; ++c) v[at][c] -= w * rd[k][c];
@@ -237,11 +248,11 @@ __device__ __forceinline__ void scale_com_velocity(const Unit& U, double v[4][3]
 // NPT (Andersen barostat step with the integration units as scaling groups): the unit
 // moves rigidly with its mass centre scaled by a.lam about the origin (the box changed
 // by a.lam), and its centre-of-mass velocity is scaled by a.vfric before the kick.
-template <bool NPT>
+template <bool NPT, int NA, int NC>
 __global__ void __launch_bounds__(128) k_kick_drift(IntegrateArgs a) {
-  const int u = blockIdx.x * blockDim.x + threadIdx.x;
-  if (u >= a.nunits) return;
-  const Unit U = load_unit(a, u);
+  const int u = a.u_begin + blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= a.u_end) return;
+  const Unit U = load_unit<NA, NC>(a, u);
   const int n = a.p.n;
   double r0[4][3], rn[4][3], v[4][3], im[4];
   float q[4];
@@ -342,11 +353,12 @@ __global__ void __launch_bounds__(128) k_kick_drift(IntegrateArgs a) {
 // slots, minus the intra-unit part sum_a (r_a - R_unit) . F_a, which turns the atomic
 // force virial into the virial of the unit centres (constraint forces are internal to
 // a unit and drop out).
+template <int NA, int NC>
 __global__ void __launch_bounds__(128) k_unit_virial(IntegrateArgs a) {
-  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  const int u = a.u_begin + blockIdx.x * blockDim.x + threadIdx.x;
   double ke = 0.0, vir[3] = {0.0, 0.0, 0.0};
-  if (u < a.nunits) {
-    const Unit U = load_unit(a, u);
+  if (u < a.u_end) {
+    const Unit U = load_unit<NA, NC>(a, u);
     const int n = a.p.n;
     double r[4][3], im[4], p[3] = {0.0, 0.0, 0.0}, mt = 0.0;
 #pragma unroll
@@ -388,12 +400,12 @@ __global__ void __launch_bounds__(128) k_unit_virial(IntegrateArgs a) {
   energy_add(a.energy + EN_VIR_Z, vir[2]);
 }
 
-template <bool KIN>
+template <bool KIN, int NA, int NC>
 __global__ void __launch_bounds__(128) k_kick_rattle(IntegrateArgs a, int kick) {
-  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  const int u = a.u_begin + blockIdx.x * blockDim.x + threadIdx.x;
   double ke = 0.0;
-  if (u < a.nunits) {
-    const Unit U = load_unit(a, u);
+  if (u < a.u_end) {
+    const Unit U = load_unit<NA, NC>(a, u);
     const int n = a.p.n;
     double r[4][3], v[4][3], im[4];
 #pragma unroll
@@ -449,11 +461,12 @@ __global__ void __launch_bounds__(256) k_kinetic(IntegrateArgs a) {
 // velocities v, sum_l c_kl (r_k . r_l) lambda_l = -|v_k|^2 - r_k . (sum_a sgn_ka F_a / m_a),
 // give constraint forces G_a = sum_l sgn_la lambda_l r_l and the virial
 // sum_l lambda_l r_l (x) r_l (diagonal), added to the virial slots.
+template <int NA, int NC>
 __global__ void __launch_bounds__(128) k_constraint_virial(IntegrateArgs a) {
-  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  const int u = a.u_begin + blockIdx.x * blockDim.x + threadIdx.x;
   double vir[3] = {0.0, 0.0, 0.0};
-  if (u < a.nunits) {
-    const Unit U = load_unit(a, u);
+  if (u < a.u_end) {
+    const Unit U = load_unit<NA, NC>(a, u);
     if (U.nc > 0) {
       const int n = a.p.n;
       double r[4][3], v[4][3], f[4][3], im[4];
@@ -573,27 +586,69 @@ __global__ void k_zero_ll(long long* p, int n) {
   if (i < n) p[i] = 0;
 }
 
+template <int V>
+using IC = std::integral_constant<int, V>;
+
+// Runs f(args over one unit class, IC<NA>, IC<NC>) for every non-empty unit class,
+// with the compile-time specialisations free atom (1, 0), (2, 1), (3, 2), (3, 3) and
+// (4, 3), and the runtime form (0, 0) for any other class.
+template <class F>
+void for_classes(const IntegrateArgs& a0, F f) {
+  for (int c = 0; c < a0.ncls; ++c) {
+    IntegrateArgs a = a0;
+    a.u_begin = a0.cls_begin[c];
+    a.u_end = a0.cls_begin[c + 1];
+    if (a.u_end <= a.u_begin) continue;
+    const int na = a0.cls_na[c], nc = a0.cls_nc[c];
+    if (na == 1 && nc == 0)
+      f(a, IC<1>(), IC<0>());
+    else if (na == 2 && nc == 1)
+      f(a, IC<2>(), IC<1>());
+    else if (na == 3 && nc == 2)
+      f(a, IC<3>(), IC<2>());
+    else if (na == 3 && nc == 3)
+      f(a, IC<3>(), IC<3>());
+    else if (na == 4 && nc == 3)
+      f(a, IC<4>(), IC<3>());
+    else
+      f(a, IC<0>(), IC<0>());
+  }
+}
+
+static int unit_grid(const IntegrateArgs& a) { return (a.u_end - a.u_begin + 127) / 128; }
+
 void launch_kick_drift(const IntegrateArgs& a, cudaStream_t st) {
-  k_kick_drift<false><<<(a.nunits + 127) / 128, 128, 0, st>>>(a);
+  for_classes(a, [&](const IntegrateArgs& x, auto na, auto nc) {
+    k_kick_drift<false, decltype(na)::value, decltype(nc)::value><<<unit_grid(x), 128, 0, st>>>(x);
+  });
 }
 
 void launch_kick_drift_npt(const IntegrateArgs& a, cudaStream_t st) {
-  k_kick_drift<true><<<(a.nunits + 127) / 128, 128, 0, st>>>(a);
+  for_classes(a, [&](const IntegrateArgs& x, auto na, auto nc) {
+    k_kick_drift<true, decltype(na)::value, decltype(nc)::value><<<unit_grid(x), 128, 0, st>>>(x);
+  });
 }
 
 void launch_unit_virial(const IntegrateArgs& a, cudaStream_t st) {
-  k_unit_virial<<<(a.nunits + 127) / 128, 128, 0, st>>>(a);
+  for_classes(a, [&](const IntegrateArgs& x, auto na, auto nc) {
+    k_unit_virial<decltype(na)::value, decltype(nc)::value><<<unit_grid(x), 128, 0, st>>>(x);
+  });
 }
 
 void launch_constraint_virial(const IntegrateArgs& a, cudaStream_t st) {
-  k_constraint_virial<<<(a.nunits + 127) / 128, 128, 0, st>>>(a);
+  for_classes(a, [&](const IntegrateArgs& x, auto na, auto nc) {
+    k_constraint_virial<decltype(na)::value, decltype(nc)::value><<<unit_grid(x), 128, 0, st>>>(x);
+  });
 }
 
 void launch_kick_rattle(const IntegrateArgs& a, bool kinetic, bool kick, cudaStream_t st) {
-  if (kinetic)
-    k_kick_rattle<true><<<(a.nunits + 127) / 128, 128, 0, st>>>(a, kick ? 1 : 0);
-  else
-    k_kick_rattle<false><<<(a.nunits + 127) / 128, 128, 0, st>>>(a, kick ? 1 : 0);
+  for_classes(a, [&](const IntegrateArgs& x, auto na, auto nc) {
+    constexpr int NA = decltype(na)::value, NC = decltype(nc)::value;
+    if (kinetic)
+      k_kick_rattle<true, NA, NC><<<unit_grid(x), 128, 0, st>>>(x, kick ? 1 : 0);
+    else
+      k_kick_rattle<false, NA, NC><<<unit_grid(x), 128, 0, st>>>(x, kick ? 1 : 0);
+  });
 }
 
 void launch_kinetic(const IntegrateArgs& a, cudaStream_t st) {
@@ -605,7 +660,7 @@ void launch_reassign(const IntegrateArgs& a, double T, uint64_t seed, uint32_t c
   k_zero_ll<<<1, 32, 0, st>>>(psum, 3);
   k_reassign_draw<<<(a.p.n + 255) / 256, 256, 0, st>>>(a, T, seed, counter, psum);
   k_reassign_shift<<<(a.p.n + 255) / 256, 256, 0, st>>>(a, psum, inv_mtot);
-  k_kick_rattle<false><<<(a.nunits + 127) / 128, 128, 0, st>>>(a, 0);
+  launch_kick_rattle(a, false, false, st);
 }
 
 }  // namespace fzk

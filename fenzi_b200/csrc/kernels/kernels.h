@@ -40,6 +40,11 @@ struct RebuildArgs {
   int chunk;     // tiles per work item
 };
 void launch_rebuild(const RebuildArgs& a, cudaStream_t st);
+// the two halves of launch_rebuild: the outer-list build (flag) and the prune (flag_prune)
+void launch_rebuild_build(const RebuildArgs& a, cudaStream_t st);
+void launch_rebuild_prune(const RebuildArgs& a, cudaStream_t st);
+// one-thread kernel: graph conditional value = (*flag != 0)
+void launch_set_condition(cudaGraphConditionalHandle h, const int* flag, cudaStream_t st);
 
 struct NonbondedArgs {
   SysParams p;
@@ -59,6 +64,7 @@ struct NonbondedArgs {
   long long* energy;    // energy slots
   int ocap;
   int grid;
+  int minb;  // CTAs per SM the kernel is built for (3 or 4)
 };
 void launch_nonbonded(const NonbondedArgs& a, bool energy, cudaStream_t st);
 
@@ -127,6 +133,10 @@ struct IntegrateArgs {
   double box_d[3], inv_box_d[3];
   double shake_tol;
   int shake_maxit;
+  int u_begin, u_end;        // unit range of one launch (set by the launchers)
+  int ncls;                  // unit classes: units [cls_begin[c], cls_begin[c+1]) have
+  int cls_na[8], cls_nc[8];  //   cls_na[c] atoms and cls_nc[c] constraints
+  int cls_begin[9];
   double lam;    // barostat step: centre-of-mass scale of every unit (1 = none)
   double vfric;  // barostat step: centre-of-mass velocity scale of the half kicks (1 = none)
 };

@@ -297,20 +297,29 @@ __global__ void k_prune_begin(const int* __restrict__ flag_prune, int* counters)
   counters[CNT_ITEMS] = 0;
 }
 
-// exclusion bits of one tile for this lane's i atom: bit k set when j entry k (slot in
-// jb[k]) is an excluded partner (1-2, 1-3, 1-4)
-__device__ __forceinline__ uint32_t excl_bits(int ia, const uint32_t* jb, const int* __restrict__ excl_off,
+// Exclusion masks of one tile (this lane holding j entry je): the lane walks the
+// excluded partners (1-2, 1-3, 1-4) of its own j atom and, for each partner sitting in
+// i-block I, sets bit `lane` in that partner's i-lane mask in shared memory.  The
+// exclusion lists are symmetric, so i-lane l ends with bit k set exactly when j entry k
+// is an excluded partner of i atom l; images are not distinguished (the box is at
+// least twice the pair-list radius).  One pass over the j atoms' partner lists per tile.
+__device__ __forceinline__ uint32_t excl_mask(int I, uint32_t je, int lane, uint32_t* msk,
+                                              const int* __restrict__ perm, const int* __restrict__ excl_off,
                                               const int* __restrict__ excl_idx, const int* __restrict__ inv_perm) {
-  uint32_t mask = 0;
-  if (ia >= 0) {
-    const int e0 = excl_off[ia], e1 = excl_off[ia + 1];
+  msk[lane] = 0u;
+  __syncwarp();
+  const int ja = perm[je & kSlotMask];
+  if (ja >= 0) {
+    const int e0 = excl_off[ja], e1 = excl_off[ja + 1];
     for (int e = e0; e < e1; ++e) {
-      const uint32_t se = (uint32_t)inv_perm[excl_idx[e]];
-      for (int k = 0; k < 32; ++k)
-        if ((jb[k] & kSlotMask) == se) mask |= 1u << k;
+      const int sp = inv_perm[excl_idx[e]];
+      if ((sp >> 5) == I) atomicOr(&msk[sp & 31], 1u << lane);
     }
   }
-  return mask;
+  __syncwarp();
+  const uint32_t m = msk[lane];
+  __syncwarp();
+  return m;
 }
 
 // Inner (pruned) pair list, warp per i-block: keeps the outer entries that lie within
@@ -328,22 +337,21 @@ __global__ void __launch_bounds__(256) k_prune(SysParams p, const int* __restric
   if (!*flag_prune) return;
   __shared__ float4 ipos_all[8][32];
   __shared__ uint32_t buf_all[8][64];
+  __shared__ uint32_t msk_all[8][32];
   const int nblk = counters[CNT_SLOTS] >> 5;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int I = blockIdx.x * 8 + warp;
   if (I >= nblk) return;
   float4* ipos = ipos_all[warp];
   uint32_t* buf = buf_all[warp];
+  uint32_t* msk = msk_all[warp];
   const int islot = I * 32 + lane;
   const float4 pi = xyzq_s[islot];
   const int ia = perm[islot];
   if (ia >= 0) pos_prune[ia] = pi;
   ipos[lane] = pi;
   // diagonal tile mask (exclusions inside the block)
-  buf[lane] = (uint32_t)islot | ((uint32_t)kNoShift << kSlotBits);
-  __syncwarp();
-  dmask[islot] = excl_bits(ia, buf, excl_off, excl_idx, inv_perm);
-  __syncwarp();
+  dmask[islot] = excl_mask(I, (uint32_t)islot, lane, msk, perm, excl_off, excl_idx, inv_perm);
   const uint32_t dummy = (uint32_t)(p.nslots - 1) | ((uint32_t)kNoShift << kSlotBits);
   const int n = outer_n[I];
   const uint32_t* src = outer + (size_t)I * ocap;
@@ -353,7 +361,7 @@ __global__ void __launch_bounds__(256) k_prune(SysParams p, const int* __restric
   auto emit = [&]() {
     const uint32_t je = buf[lane];
     dst[ntile * 32 + lane] = je;
-    const uint32_t mask = excl_bits(ia, buf, excl_off, excl_idx, inv_perm);
+    const uint32_t mask = excl_mask(I, je, lane, msk, perm, excl_off, excl_idx, inv_perm);
     int m = -1;
     if (__ballot_sync(0xffffffffu, mask != 0)) {
       if (lane == 0) m = atomicAdd(&counters[CNT_MASKS], 1);
@@ -431,8 +439,23 @@ __global__ void k_rb_end(int* flag, int* flag_prune, int* counters) {
   *flag_prune = 1;  // a new outer list always gets a fresh inner list
 }
 
+// sets a graph conditional node's value from a device flag (the neighbour kernels run
+// inside an IF node only when their flag is raised)
+__global__ void k_set_condition(cudaGraphConditionalHandle h, const int* __restrict__ flag) {
+  cudaGraphSetConditional(h, *flag != 0 ? 1u : 0u);
+}
+
 // ------------------------------------------------------------------ launchers
+void launch_set_condition(cudaGraphConditionalHandle h, const int* flag, cudaStream_t st) {
+  k_set_condition<<<1, 1, 0, st>>>(h, flag);
+}
+
 void launch_rebuild(const RebuildArgs& a, cudaStream_t st) {
+  launch_rebuild_build(a, st);
+  launch_rebuild_prune(a, st);
+}
+
+void launch_rebuild_build(const RebuildArgs& a, cudaStream_t st) {
   const SysParams& p = a.p;
   const int ncol = p.ncol[0] * p.ncol[1];
   k_rb_begin<<<(ncol + 255) / 256, 256, 0, st>>>(a.flag, a.col_count, a.col_cursor, ncol, a.counters);
@@ -448,6 +471,11 @@ void launch_rebuild(const RebuildArgs& a, cudaStream_t st) {
                                                a.col_start, a.dcx, a.dcy, a.all_images, a.outer, a.outer_n, a.ocap,
                                                a.status);
   k_rb_end<<<1, 1, 0, st>>>(a.flag, a.flag_prune, a.counters);
+}
+
+void launch_rebuild_prune(const RebuildArgs& a, cudaStream_t st) {
+  const SysParams& p = a.p;
+  const int maxblk = (p.nslots) / 32;
   k_prune_begin<<<1, 1, 0, st>>>(a.flag_prune, a.counters);
   k_prune<<<(maxblk + 7) / 8, 256, 0, st>>>(p, a.flag_prune, a.counters, a.perm, a.inv_perm, a.xyzq_s, a.excl_off,
                                             a.excl_idx, a.outer, a.outer_n, a.inner, a.inner_nt, a.inner_m, a.masks,

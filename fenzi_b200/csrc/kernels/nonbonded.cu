@@ -170,8 +170,8 @@ __device__ __forceinline__ void run_tile(const PairConst& c, const SysParams& p,
 
 // Warp per i-block (blocks taken from a dynamic counter): the diagonal tile, then the
 // block's inner tiles; the i force stays in registers across tiles and is flushed once.
-template <bool ENERGY>
-__global__ void __launch_bounds__(256, 3)
+template <bool ENERGY, int MINB>
+__global__ void __launch_bounds__(256, MINB)
     k_nonbonded(SysParams p, PairConst c, const float4* __restrict__ xyzq, const int* __restrict__ typ,
                 const int* __restrict__ perm, const uint32_t* __restrict__ inner, const int* __restrict__ inner_nt,
                 const int* __restrict__ inner_m, const uint32_t* __restrict__ dmask,
@@ -257,14 +257,11 @@ void launch_nonbonded(const NonbondedArgs& a, bool energy, cudaStream_t st) {
   c.sw_b = d > 0.f ? -a.p.ron2 / d : 0.f;
   c.dsw_k = d > 0.f ? 12.f / d : 0.f;
   cudaMemsetAsync(a.counters + CNT_WORK, 0, sizeof(int), st);
-  if (energy)
-    k_nonbonded<true><<<a.grid, kWarps * 32, smem, st>>>(a.p, c, a.xyzq_s, a.typ_s, a.perm, a.inner, a.inner_nt,
-                                                          a.inner_m, a.dmask, a.masks, a.counters, a.items, a.chunk,
-                                                          a.ljtab, a.facc, a.energy, a.ocap);
-  else
-    k_nonbonded<false><<<a.grid, kWarps * 32, smem, st>>>(a.p, c, a.xyzq_s, a.typ_s, a.perm, a.inner, a.inner_nt,
-                                                           a.inner_m, a.dmask, a.masks, a.counters, a.items, a.chunk,
-                                                           a.ljtab, a.facc, a.energy, a.ocap);
+  // 3 CTAs per SM fit 80 registers a thread; the 4-CTA build is held to 64
+  auto k = energy ? (a.minb >= 4 ? k_nonbonded<true, 4> : k_nonbonded<true, 3>)
+                  : (a.minb >= 4 ? k_nonbonded<false, 4> : k_nonbonded<false, 3>);
+  k<<<a.grid, kWarps * 32, smem, st>>>(a.p, c, a.xyzq_s, a.typ_s, a.perm, a.inner, a.inner_nt, a.inner_m, a.dmask,
+                                       a.masks, a.counters, a.items, a.chunk, a.ljtab, a.facc, a.energy, a.ocap);
 }
 
 }  // namespace fzk

@@ -445,13 +445,20 @@ def write(s: System, outdir: str, prefix: str | None = None, extra_in: str = "")
     return inpath
 
 
-def ensemble(nsys=256, seed=2345, nw_min=216, nw_max=2000, rc=9.0, ron=7.5):
+def ensemble_sizes(nsys=256, seed=2345, nw_min=216, nw_max=2000):
+    """Waters per box of ensemble(): uniform in [nw_min, nw_max], seeded."""
+    return np.random.default_rng(seed).integers(nw_min, nw_max + 1, size=nsys)
+
+
+def ensemble(nsys=256, seed=2345, nw_min=216, nw_max=2000, rc=9.0, ron=7.5, only=None):
     """Independent TIP3P boxes (sizes uniform in [nw_min, nw_max] waters, seeded), each
-    at 0.0334 waters/A^3 with its own PME grid: smallest 2^a 3^b 5^c >= L / 1.2."""
-    rng = np.random.default_rng(seed)
-    sizes = rng.integers(nw_min, nw_max + 1, size=nsys)
+    at 0.0334 waters/A^3 with its own PME grid: smallest 2^a 3^b 5^c >= L / 1.2.
+    only: indices of the boxes to build (a shard); box i is the same in every shard."""
+    sizes = ensemble_sizes(nsys, seed, nw_min, nw_max)
     out = []
     for i, nw in enumerate(sizes):
+        if only is not None and i not in only:
+            continue
         L = (nw / 0.0334) ** (1.0 / 3.0)
         out.append(build(name=f"box{i:03d}", nw=int(nw), box=L, kgrid=fft_friendly(L / 1.2), rc=rc, ron=ron,
                          seed=seed + 1 + i))
