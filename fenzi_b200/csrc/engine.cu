@@ -196,6 +196,8 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
     FZ_CUDA(cudaMemcpyAsync(e->perm + nslots - 32, dp.data(), 32 * sizeof(int), cudaMemcpyHostToDevice, e->st));
   }
   if ((r = e->upload(&e->excl_off, t.excl_off)) || (r = e->upload(&e->excl_idx, t.excl_idx))) return r;
+  for (int i = 0; i < n; ++i) e->xmax = std::max(e->xmax, t.excl_off[i + 1] - t.excl_off[i]);
+  if ((r = e->alloc(&e->xn, nslots)) || (r = e->alloc(&e->xs, (size_t)nslots * e->xmax))) return r;
   // LJ tables with a zero padding type at index nt
   {
     const int nt1 = nt + 1;
@@ -493,7 +495,7 @@ static fz_status npt_step(Engine* e) {
   ia = e->int_args();
   ia.vfric = std::exp(-0.5 * dt * e->Ldot / Ln);
   fzk::launch_kick_rattle(ia, false, true, e->st);
-  e->launches += 4 + 11 + 1 + ((e->nbond + e->nangle + e->nub + e->ndihe + e->nimpr + e->nexcl + e->n14 > 0) ? 1 : 0) + 12;
+  e->launches += 4 + 12 + 1 + ((e->nbond + e->nangle + e->nub + e->ndihe + e->nimpr + e->nexcl + e->n14 > 0) ? 1 : 0) + 12;
   return FZ_OK;
 }
 

@@ -46,6 +46,7 @@ struct Engine {
   int2* items = nullptr;
   int chunk = 16;
   int *excl_off = nullptr, *excl_idx = nullptr;
+  int *xn = nullptr, *xs = nullptr, xmax = 1;  // per-slot excluded-partner slots
   int *flag = nullptr, *counters = nullptr, *status = nullptr;
   float2 *ljtab = nullptr, *lj14 = nullptr;
   // bonded
@@ -194,6 +195,9 @@ struct Engine {
     a.bb_hi = bb_hi;
     a.excl_off = excl_off;
     a.excl_idx = excl_idx;
+    a.xn = xn;
+    a.xs = xs;
+    a.xmax = xmax;
     a.masks = masks;
     a.mask_cap = mask_cap;
     a.all_images = all_images;
@@ -338,7 +342,7 @@ struct Engine {
   void forces(bool energies, int terms = FZ_TERM_ALL) {
     mark(1);
     fzk::launch_rebuild(rebuild_args(), st);
-    launches += 11;
+    launches += 12;
     mark(2);
     if (terms & FZ_TERM_NONBONDED) {
       fzk::launch_nonbonded(nb_args(), energies, st);
@@ -421,13 +425,13 @@ struct Engine {
   }
   // kernels one captured step launches besides the conditional bodies
   long long graph_step_launches() const {
-    return 2 + (cond_graph ? 2 : 11) + 1 + ((nbond + nangle + nub + ndihe + nimpr + nexcl + n14 > 0) ? 1 : 0) + 12;
+    return 2 + (cond_graph ? 2 : 12) + 1 + ((nbond + nangle + nub + ndihe + nimpr + nexcl + n14 > 0) ? 1 : 0) + 12;
   }
-  // launches of the conditional bodies (8 per rebuild, 3 per prune) since the last
+  // launches of the conditional bodies (9 per rebuild, 3 per prune) since the last
   // call, from the device counters; called after a synchronisation
   void account_conditional(const int* cnt) {
     if (cond_graph && graph_since_check)
-      launches += 8 * (cnt[fzk::CNT_REBUILDS] - seen_rb_launch) + 3 * (cnt[fzk::CNT_PRUNES] - seen_pr_launch);
+      launches += 9 * (cnt[fzk::CNT_REBUILDS] - seen_rb_launch) + 3 * (cnt[fzk::CNT_PRUNES] - seen_pr_launch);
     graph_since_check = false;
     seen_rb_launch = cnt[fzk::CNT_REBUILDS];
     seen_pr_launch = cnt[fzk::CNT_PRUNES];

@@ -21,6 +21,8 @@ struct RebuildArgs {
   int* typ_s;
   float4 *bb_lo, *bb_hi;
   const int *excl_off, *excl_idx;
+  int *xn, *xs;  // per slot: count and slots (stride xmax) of its excluded partners
+  int xmax;
   uint32_t* masks;
   int mask_cap, all_images;
   int* blk_col;   // block -> column

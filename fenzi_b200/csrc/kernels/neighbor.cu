@@ -290,6 +290,23 @@ __global__ void __launch_bounds__(256) k_rb_outer(SysParams p, const int* __rest
   }
 }
 
+// partner slots of every slot's excluded atoms (1-2, 1-3, 1-4), for the prune's masks
+__global__ void k_rb_xslot(SysParams p, const int* __restrict__ flag, const int* __restrict__ perm,
+                           const int* __restrict__ inv_perm, const int* __restrict__ excl_off,
+                           const int* __restrict__ excl_idx, int* xn, int* xs, int xmax) {
+  if (!*flag) return;
+  const int sl = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sl >= p.nslots) return;
+  const int a = perm[sl];
+  int m = 0;
+  if (a >= 0) {
+    const int e0 = excl_off[a];
+    m = min(excl_off[a + 1] - e0, xmax);
+    for (int k = 0; k < m; ++k) xs[(size_t)sl * xmax + k] = inv_perm[excl_idx[e0 + k]];
+  }
+  xn[sl] = m;
+}
+
 __global__ void k_prune_begin(const int* __restrict__ flag_prune, int* counters) {
   if (!*flag_prune) return;
   counters[CNT_MASKS] = 0;
@@ -298,28 +315,26 @@ __global__ void k_prune_begin(const int* __restrict__ flag_prune, int* counters)
 }
 
 // Exclusion masks of one tile (this lane holding j entry je): the lane walks the
-// excluded partners (1-2, 1-3, 1-4) of its own j atom and, for each partner sitting in
-// i-block I, sets bit `lane` in that partner's i-lane mask in shared memory.  The
-// exclusion lists are symmetric, so i-lane l ends with bit k set exactly when j entry k
-// is an excluded partner of i atom l; images are not distinguished (the box is at
-// least twice the pair-list radius).  One pass over the j atoms' partner lists per tile.
+// excluded partners (1-2, 1-3, 1-4) of its own j slot (xs/xn: partner slots per slot,
+// written at every rebuild) and, for each partner sitting in i-block I, sets bit
+// `lane` in that partner's i-lane mask in shared memory.  The exclusion lists are
+// symmetric, so i-lane l ends with bit k set exactly when j entry k is an excluded
+// partner of i atom l; images are not distinguished (the box is at least twice the
+// pair-list radius).
 __device__ __forceinline__ uint32_t excl_mask(int I, uint32_t je, int lane, uint32_t* msk,
-                                              const int* __restrict__ perm, const int* __restrict__ excl_off,
-                                              const int* __restrict__ excl_idx, const int* __restrict__ inv_perm) {
+                                              const int* __restrict__ xn, const int* __restrict__ xs, int xmax) {
   msk[lane] = 0u;
   __syncwarp();
-  const int ja = perm[je & kSlotMask];
-  if (ja >= 0) {
-    const int e0 = excl_off[ja], e1 = excl_off[ja + 1];
-    for (int e = e0; e < e1; ++e) {
-      const int sp = inv_perm[excl_idx[e]];
-      if ((sp >> 5) == I) atomicOr(&msk[sp & 31], 1u << lane);
-    }
+  const int sj = (int)(je & kSlotMask);
+  const int m = xn[sj];
+  for (int k = 0; k < m; ++k) {
+    const int sp = xs[(size_t)sj * xmax + k];
+    if ((sp >> 5) == I) atomicOr(&msk[sp & 31], 1u << lane);
   }
   __syncwarp();
-  const uint32_t m = msk[lane];
+  const uint32_t r = msk[lane];
   __syncwarp();
-  return m;
+  return r;
 }
 
 // Inner (pruned) pair list, warp per i-block: keeps the outer entries that lie within
@@ -328,9 +343,9 @@ __device__ __forceinline__ uint32_t excl_mask(int I, uint32_t je, int lane, uint
 // list was made at.  Run after every rebuild and whenever an atom has moved more than
 // delta/2 since the last prune, so no pair within rc is ever missed.
 __global__ void __launch_bounds__(256) k_prune(SysParams p, const int* __restrict__ flag_prune, int* counters,
-                                               const int* __restrict__ perm, const int* __restrict__ inv_perm,
-                                               const float4* __restrict__ xyzq_s, const int* __restrict__ excl_off,
-                                               const int* __restrict__ excl_idx, const uint32_t* __restrict__ outer,
+                                               const int* __restrict__ perm, const int* __restrict__ xn,
+                                               const float4* __restrict__ xyzq_s, const int* __restrict__ xs,
+                                               int xmax, const uint32_t* __restrict__ outer,
                                                const int* __restrict__ outer_n, uint32_t* inner, int* inner_nt,
                                                int* inner_m, uint32_t* masks, uint32_t* dmask, int mask_cap, int ocap,
                                                float rp2, float4* pos_prune, int2* items, int chunk, int* status) {
@@ -351,7 +366,7 @@ __global__ void __launch_bounds__(256) k_prune(SysParams p, const int* __restric
   if (ia >= 0) pos_prune[ia] = pi;
   ipos[lane] = pi;
   // diagonal tile mask (exclusions inside the block)
-  dmask[islot] = excl_mask(I, (uint32_t)islot, lane, msk, perm, excl_off, excl_idx, inv_perm);
+  dmask[islot] = excl_mask(I, (uint32_t)islot, lane, msk, xn, xs, xmax);
   const uint32_t dummy = (uint32_t)(p.nslots - 1) | ((uint32_t)kNoShift << kSlotBits);
   const int n = outer_n[I];
   const uint32_t* src = outer + (size_t)I * ocap;
@@ -361,7 +376,7 @@ __global__ void __launch_bounds__(256) k_prune(SysParams p, const int* __restric
   auto emit = [&]() {
     const uint32_t je = buf[lane];
     dst[ntile * 32 + lane] = je;
-    const uint32_t mask = excl_mask(I, je, lane, msk, perm, excl_off, excl_idx, inv_perm);
+    const uint32_t mask = excl_mask(I, je, lane, msk, xn, xs, xmax);
     int m = -1;
     if (__ballot_sync(0xffffffffu, mask != 0)) {
       if (lane == 0) m = atomicAdd(&counters[CNT_MASKS], 1);
@@ -377,10 +392,18 @@ __global__ void __launch_bounds__(256) k_prune(SysParams p, const int* __restric
     ++ntile;
     __syncwarp();
   };
+  // the next chunk's entries and positions are loaded before this chunk's distance
+  // tests, so the gathers overlap the arithmetic
+  uint32_t e_nx = lane < n ? src[lane] : dummy;
+  float4 r_nx = xyzq_s[e_nx & kSlotMask];
   for (int c0 = 0; c0 < n; c0 += 32) {
     const bool valid = c0 + lane < n;
-    const uint32_t e = valid ? src[c0 + lane] : dummy;
-    float4 r = xyzq_s[e & kSlotMask];
+    const uint32_t e = e_nx;
+    float4 r = r_nx;
+    if (c0 + 32 < n) {
+      e_nx = c0 + 32 + lane < n ? src[c0 + 32 + lane] : dummy;
+      r_nx = xyzq_s[e_nx & kSlotMask];
+    }
     const int code = (int)(e >> kSlotBits);
     if (code != kNoShift) {
       const float3 sh = shift_of(code, p);
@@ -465,6 +488,8 @@ void launch_rebuild_build(const RebuildArgs& a, cudaStream_t st) {
   k_rb_colsort<<<ncol, 256, kColCap * sizeof(unsigned long long), st>>>(
       p, a.flag, a.col_count, a.col_start, a.col_tmp, a.pos4, a.type, a.perm, a.inv_perm, a.xyzq_s, a.typ_s,
       a.blk_col, a.status);
+  k_rb_xslot<<<(p.nslots + 255) / 256, 256, 0, st>>>(p, a.flag, a.perm, a.inv_perm, a.excl_off, a.excl_idx, a.xn,
+                                                     a.xs, a.xmax);
   const int maxblk = (p.nslots) / 32;
   k_rb_bbox<<<(maxblk * 32 + 255) / 256, 256, 0, st>>>(p, a.flag, a.counters, a.perm, a.xyzq_s, a.bb_lo, a.bb_hi);
   k_rb_outer<<<(maxblk + 7) / 8, 256, 0, st>>>(p, a.flag, a.counters, a.perm, a.xyzq_s, a.bb_lo, a.bb_hi, a.blk_col,
@@ -477,8 +502,8 @@ void launch_rebuild_prune(const RebuildArgs& a, cudaStream_t st) {
   const SysParams& p = a.p;
   const int maxblk = (p.nslots) / 32;
   k_prune_begin<<<1, 1, 0, st>>>(a.flag_prune, a.counters);
-  k_prune<<<(maxblk + 7) / 8, 256, 0, st>>>(p, a.flag_prune, a.counters, a.perm, a.inv_perm, a.xyzq_s, a.excl_off,
-                                            a.excl_idx, a.outer, a.outer_n, a.inner, a.inner_nt, a.inner_m, a.masks,
+  k_prune<<<(maxblk + 7) / 8, 256, 0, st>>>(p, a.flag_prune, a.counters, a.perm, a.xn, a.xyzq_s, a.xs, a.xmax,
+                                            a.outer, a.outer_n, a.inner, a.inner_nt, a.inner_m, a.masks,
                                             a.dmask, a.mask_cap, a.ocap, a.rp2, a.pos_prune, a.items, a.chunk,
                                             a.status);
   k_prune_end<<<1, 1, 0, st>>>(a.flag_prune, a.counters);
