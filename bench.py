@@ -551,9 +551,9 @@ def main():
                 "step_roofline": {"t_ideal_ms": t_ideal * 1e3, "frac": t_ideal * 1e3 / ms_step,
                                   "model": "60 FLOP/pair / FP32 peak + (56N + 24K^3 + 120N) B / HBM"},
                 "stages_ms": stages, "rebuilds_in_timed_steps": rebuilds,
-                "pair_tiles": sysm.counters()["tiles"],
+                "pair_slots": sysm.counters()["pair_slots"],
                 "prunes_total": sysm.counters()["prunes"],
-                "pair_slot_efficiency": pairs / (sysm.counters()["tiles"] * 1024.0),
+                "pair_slot_efficiency": pairs / float(sysm.counters()["pair_slots"]),
                 "roofline": roof, "cpu_baseline": cpu,
                 "e2e": {"value": e2e_nsd, "unit": "ns/day", "h2d_bytes_per_step": 24 * natom / a.chunk,
                         "d2h_bytes_per_step": 24 * natom / a.chunk, "h2d_bytes_per_call": 24 * natom,

@@ -312,7 +312,7 @@ class FenZi:
     def counters(self):
         out = (C.c_longlong * 4)()
         _check(lib().fz_get_counters(self.h, out))
-        return dict(launches=out[0], rebuilds=out[1], tiles=out[2], prunes=out[3])
+        return dict(launches=out[0], rebuilds=out[1], pair_slots=out[2], prunes=out[3])
 
     def stage_timing(self, enable=True):
         _check(lib().fz_set_stage_timing(self.h, 1 if enable else 0))

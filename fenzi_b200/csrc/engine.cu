@@ -121,6 +121,7 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
   e->pref_atm = c.pref;
   e->nslots = ((n + 32 * e->ncol + 64 + 31) / 32) * 32;
   p.nslots = e->nslots;
+  if (e->nslots >= (1 << 26)) return fail(FZ_ERR_CAPACITY, "system too large: sorted slots exceed 2^26");
   for (int d = 0; d < 3; ++d) {
     e->K[d] = c.pme_grid[d];
     if (!fft_size_ok(e->K[d])) return fail(FZ_ERR_ARG, "PME grid sizes must be 2^a 3^b 5^c in [2, 1024]");
@@ -133,7 +134,7 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
   const double ab = 1.4 * a, R = plist;
   const double vm = ab * ab * ab + 6 * ab * ab * R + 3 * M_PI * ab * R * R + 4.0 / 3.0 * M_PI * R * R * R;
   e->ocap = (int)std::ceil(std::max(256.0, 1.25 * rho * vm) / 32.0) * 32;
-  e->mask_cap = (e->nslots / 32) * (e->ocap / 32);
+  e->mask_cap = (e->nslots / 32) * fzk::kNG * (e->ocap / 32);
   {
     const double delta = std::min(0.3, plist - c.cutoff);
     e->rp2 = (float)((c.cutoff + delta) * (c.cutoff + delta));
@@ -174,16 +175,16 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
       (r = e->alloc(&e->psum, 4)) || (r = e->upload(&e->type, t.type)))
     return r;
   // ---- sorted slots, columns, tiles
-  const int nslots = e->nslots, nblk = nslots / 32;
+  const int nslots = e->nslots, nblk = nslots / 32, ngrp = nblk * fzk::kNG;
   if ((r = e->alloc(&e->xyzq_s, nslots)) || (r = e->alloc(&e->typ_s, nslots)) || (r = e->alloc(&e->perm, nslots)) ||
       (r = e->alloc(&e->inv_perm, n)) || (r = e->alloc(&e->col_of, n)) || (r = e->alloc(&e->col_count, e->ncol)) ||
       (r = e->alloc(&e->col_cursor, e->ncol)) || (r = e->alloc(&e->col_start, e->ncol + 1)) ||
       (r = e->alloc(&e->col_tmp, nslots)) || (r = e->alloc(&e->bb_lo, nblk)) || (r = e->alloc(&e->blk_col, nblk)) || (r = e->alloc(&e->bb_hi, nblk)) ||
-      (r = e->alloc(&e->outer, (size_t)nblk * e->ocap)) || (r = e->alloc(&e->inner, (size_t)nblk * e->ocap)) ||
-      (r = e->alloc(&e->outer_n, nblk)) || (r = e->alloc(&e->inner_nt, nblk)) ||
-      (r = e->alloc(&e->inner_m, (size_t)nblk * (e->ocap / 32))) || (r = e->alloc(&e->dmask, (size_t)nblk * 32)) ||
-      (r = e->alloc(&e->masks, (size_t)e->mask_cap * 32)) || (r = e->alloc(&e->pos_prune, n)) ||
-      (r = e->alloc(&e->flag_prune, 1)) || (r = e->alloc(&e->items, (size_t)nblk * (e->ocap / 32 + 1))) ||
+      (r = e->alloc(&e->outer, (size_t)nblk * e->ocap)) || (r = e->alloc(&e->inner, (size_t)ngrp * e->ocap)) ||
+      (r = e->alloc(&e->outer_n, nblk)) || (r = e->alloc(&e->inner_nt, ngrp)) ||
+      (r = e->alloc(&e->inner_m, (size_t)ngrp * (e->ocap / 32))) || (r = e->alloc(&e->dmask, (size_t)nblk * 32)) ||
+      (r = e->alloc(&e->masks, (size_t)e->mask_cap * fzk::kIG)) || (r = e->alloc(&e->pos_prune, n)) ||
+      (r = e->alloc(&e->flag_prune, 1)) || (r = e->alloc(&e->items, (size_t)ngrp * (e->ocap / 32 + 1))) ||
       (r = e->alloc(&e->flag, 1)) || (r = e->alloc(&e->counters, fzk::CNT_COUNT)) || (r = e->alloc(&e->status, 1)))
     return r;
   {
@@ -338,11 +339,12 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
     e->release(e->inner_m);
     e->release(e->masks);
     e->ocap *= 2;
-    e->mask_cap = nblk * (e->ocap / 32);
+    e->mask_cap = ngrp * (e->ocap / 32);
     e->release(e->items);
-    if ((r = e->alloc(&e->items, (size_t)nblk * (e->ocap / 32 + 1))) ||
-        (r = e->alloc(&e->outer, (size_t)nblk * e->ocap)) || (r = e->alloc(&e->inner, (size_t)nblk * e->ocap)) ||
-        (r = e->alloc(&e->inner_m, (size_t)nblk * (e->ocap / 32))) || (r = e->alloc(&e->masks, (size_t)e->mask_cap * 32)))
+    if ((r = e->alloc(&e->items, (size_t)ngrp * (e->ocap / 32 + 1))) ||
+        (r = e->alloc(&e->outer, (size_t)nblk * e->ocap)) || (r = e->alloc(&e->inner, (size_t)ngrp * e->ocap)) ||
+        (r = e->alloc(&e->inner_m, (size_t)ngrp * (e->ocap / 32))) ||
+        (r = e->alloc(&e->masks, (size_t)e->mask_cap * fzk::kIG)))
       return r;
     const int zero = 0;
     FZ_CUDA(cudaMemcpyAsync(e->status, &zero, sizeof(int), cudaMemcpyHostToDevice, e->st));
@@ -356,7 +358,7 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
     int cnt2[fzk::CNT_COUNT];
     FZ_CUDA(cudaMemcpyAsync(cnt2, e->counters, sizeof(cnt2), cudaMemcpyDeviceToHost, e->st));
     FZ_CUDA(cudaStreamSynchronize(e->st));
-    const int want = std::max(1, std::min(16, cnt2[fzk::CNT_TILES] / (dev_sms * 24)));
+    const int want = std::max(1, std::min(64, cnt2[fzk::CNT_TILES] / (dev_sms * 24)));
     if (want != e->chunk) {
       e->chunk = want;
       FZ_CUDA(cudaMemcpyAsync(e->flag_prune, &one, sizeof(int), cudaMemcpyHostToDevice, e->st));
@@ -798,7 +800,7 @@ extern "C" fz_status fz_get_counters(fz_system* s, long long* out4) {
   FZ_CUDA(cudaStreamSynchronize(e->st));
   out4[0] = e->launches;
   out4[1] = cnt[fzk::CNT_REBUILDS];
-  out4[2] = cnt[fzk::CNT_TILES];
+  out4[2] = (long long)cnt[fzk::CNT_TILES] * fzk::kIG * 32;
   out4[3] = cnt[fzk::CNT_PRUNES];
   return FZ_OK;
 }

@@ -215,7 +215,9 @@ __global__ void __launch_bounds__(256) k_rb_outer(SysParams p, const int* __rest
                                                   const float4* __restrict__ xyzq_s, const float4* __restrict__ bb_lo,
                                                   const float4* __restrict__ bb_hi, const int* __restrict__ blk_col,
                                                   const int* __restrict__ col_start, int dcx, int dcy, int all_images,
-                                                  uint32_t* outer, int* outer_n, int ocap, int* status) {
+                                                  uint32_t* outer, int* outer_n, int ocap,
+                                                  const int* __restrict__ xn, const int* __restrict__ xs, int xmax,
+                                                  int* status) {
   if (!*flag) return;
   const int nblk = counters[CNT_SLOTS] >> 5;
   const int lane = threadIdx.x & 31;
@@ -277,7 +279,15 @@ __global__ void __launch_bounds__(256) k_rb_outer(SysParams p, const int* __rest
             const bool ok = perm[s] >= 0 && box_gap2(d, hi) < rl2;
             const unsigned b2 = __ballot_sync(0xffffffffu, ok);
             const int pos = count + __popc(b2 & ((1u << lane) - 1u));
-            if (ok && pos < ocap) out[pos] = (uint32_t)s | ((uint32_t)cc << kSlotBits);
+            if (ok && pos < ocap) {
+              // flag entries whose atom has an excluded partner in block I: only those
+              // need the prune's exclusion-mask walk
+              uint32_t fl = 0u;
+              const int m = xn[s];
+              for (int k = 0; k < m; ++k)
+                if ((xs[(size_t)s * xmax + k] >> 5) == I) fl = kExclBit;
+              out[pos] = (uint32_t)s | fl | ((uint32_t)cc << kSlotBits);
+            }
             count += __popc(b2);
           }
         }
@@ -342,7 +352,7 @@ __device__ __forceinline__ uint32_t excl_mask(int I, uint32_t je, int lane, uint
 // into full 32-entry tiles with their exclusion masks, and records the positions the
 // list was made at.  Run after every rebuild and whenever an atom has moved more than
 // delta/2 since the last prune, so no pair within rc is ever missed.
-__global__ void __launch_bounds__(256) k_prune(SysParams p, const int* __restrict__ flag_prune, int* counters,
+__global__ void __launch_bounds__(256, 6) k_prune(SysParams p, const int* __restrict__ flag_prune, int* counters,
                                                const int* __restrict__ perm, const int* __restrict__ xn,
                                                const float4* __restrict__ xyzq_s, const int* __restrict__ xs,
                                                int xmax, const uint32_t* __restrict__ outer,
@@ -351,14 +361,13 @@ __global__ void __launch_bounds__(256) k_prune(SysParams p, const int* __restric
                                                float rp2, float4* pos_prune, int2* items, int chunk, int* status) {
   if (!*flag_prune) return;
   __shared__ float4 ipos_all[8][32];
-  __shared__ uint32_t buf_all[8][64];
+  __shared__ uint32_t buf_all[8][kNG][64];
   __shared__ uint32_t msk_all[8][32];
   const int nblk = counters[CNT_SLOTS] >> 5;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int I = blockIdx.x * 8 + warp;
   if (I >= nblk) return;
   float4* ipos = ipos_all[warp];
-  uint32_t* buf = buf_all[warp];
   uint32_t* msk = msk_all[warp];
   const int islot = I * 32 + lane;
   const float4 pi = xyzq_s[islot];
@@ -370,26 +379,34 @@ __global__ void __launch_bounds__(256) k_prune(SysParams p, const int* __restric
   const uint32_t dummy = (uint32_t)(p.nslots - 1) | ((uint32_t)kNoShift << kSlotBits);
   const int n = outer_n[I];
   const uint32_t* src = outer + (size_t)I * ocap;
-  uint32_t* dst = inner + (size_t)I * ocap;
-  int* mdst = inner_m + (size_t)I * (ocap >> 5);
-  int count = 0, ntile = 0;
-  auto emit = [&]() {
+  int count[kNG], ntile[kNG];
+#pragma unroll
+  for (int s = 0; s < kNG; ++s) count[s] = ntile[s] = 0;
+  // one full 32-entry tile of i-group s: entries, and its exclusion words (one per i
+  // atom of the group) when any pair is excluded
+  auto emit = [&](int s) {
+    uint32_t* buf = buf_all[warp][s];
+    const int g = I * kNG + s;
     const uint32_t je = buf[lane];
-    dst[ntile * 32 + lane] = je;
-    const uint32_t mask = excl_mask(I, je, lane, msk, xn, xs, xmax);
+    inner[(size_t)g * ocap + ntile[s] * 32 + lane] = je;
+    uint32_t w = 0u;
+    if (__ballot_sync(0xffffffffu, (je & kExclBit) != 0u)) {
+      excl_mask(I, (je & kExclBit) ? je : dummy, lane, msk, xn, xs, xmax);
+      w = lane < kIG ? msk[s * kIG + lane] : 0u;
+    }
     int m = -1;
-    if (__ballot_sync(0xffffffffu, mask != 0)) {
+    if (__ballot_sync(0xffffffffu, w != 0)) {
       if (lane == 0) m = atomicAdd(&counters[CNT_MASKS], 1);
       m = __shfl_sync(0xffffffffu, m, 0);
       if (m >= mask_cap) {
         if (lane == 0) atomicOr(status, ST_MASK_OVERFLOW);
         m = -1;
-      } else {
-        masks[(size_t)m * 32 + lane] = mask;
+      } else if (lane < kIG) {
+        masks[(size_t)m * kIG + lane] = w;
       }
     }
-    if (lane == 0) mdst[ntile] = m;
-    ++ntile;
+    if (lane == 0) inner_m[(size_t)g * (ocap >> 5) + ntile[s]] = m;
+    ++ntile[s];
     __syncwarp();
   };
   // the next chunk's entries and positions are loaded before this chunk's distance
@@ -411,42 +428,57 @@ __global__ void __launch_bounds__(256) k_prune(SysParams p, const int* __restric
       r.y += sh.y;
       r.z += sh.z;
     }
-    float m2 = 3e38f;
-#pragma unroll 8
+    float m2[kNG];
+#pragma unroll
+    for (int s = 0; s < kNG; ++s) m2[s] = 3e38f;
+#pragma unroll
     for (int k = 0; k < 32; ++k) {
       const float4 q = ipos[k];
       const float dx = r.x - q.x, dy = r.y - q.y, dz = r.z - q.z;
-      m2 = fminf(m2, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+      m2[k / kIG] = fminf(m2[k / kIG], fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
     }
-    const bool keep = valid && m2 < rp2;
-    const unsigned b = __ballot_sync(0xffffffffu, keep);
-    if (keep) buf[count + __popc(b & ((1u << lane) - 1u))] = e;
-    __syncwarp();
-    count += __popc(b);
-    if (count >= 32) {
-      emit();
-      const uint32_t rest = buf[32 + lane];
+#pragma unroll
+    for (int s = 0; s < kNG; ++s) {
+      uint32_t* buf = buf_all[warp][s];
+      const bool keep = valid && m2[s] < rp2;
+      const unsigned b = __ballot_sync(0xffffffffu, keep);
+      if (keep) buf[count[s] + __popc(b & ((1u << lane) - 1u))] = e;
       __syncwarp();
-      buf[lane] = rest;
-      __syncwarp();
-      count -= 32;
+      count[s] += __popc(b);
+      if (count[s] >= 32) {
+        emit(s);
+        const uint32_t rest = buf[32 + lane];
+        __syncwarp();
+        buf[lane] = rest;
+        __syncwarp();
+        count[s] -= 32;
+      }
     }
   }
-  if (count > 0) {
-    if (lane >= count) buf[lane] = dummy;
-    __syncwarp();
-    emit();
+#pragma unroll
+  for (int s = 0; s < kNG; ++s) {
+    if (count[s] > 0) {
+      uint32_t* buf = buf_all[warp][s];
+      if (lane >= count[s]) buf[lane] = dummy;
+      __syncwarp();
+      emit(s);
+    }
   }
-  // work items for the pair kernel: chunks of <= `chunk` tiles (tile 0 is the diagonal)
-  const int nitems = (ntile + 1 + chunk - 1) / chunk;
-  int base = 0;
-  if (lane == 0) {
-    inner_nt[I] = ntile;
-    atomicAdd(&counters[CNT_TILES], ntile + 1);
-    base = atomicAdd(&counters[CNT_ITEMS], nitems);
+  // work items for the pair kernel, per i-group: chunks of <= `chunk` tiles (tile 0
+  // is the group against its own block, upper triangle)
+#pragma unroll
+  for (int s = 0; s < kNG; ++s) {
+    const int g = I * kNG + s;
+    const int nitems = (ntile[s] + 1 + chunk - 1) / chunk;
+    int base = 0;
+    if (lane == 0) {
+      inner_nt[g] = ntile[s];
+      atomicAdd(&counters[CNT_TILES], ntile[s] + 1);
+      base = atomicAdd(&counters[CNT_ITEMS], nitems);
+    }
+    base = __shfl_sync(0xffffffffu, base, 0);
+    for (int k = lane; k < nitems; k += 32) items[base + k] = make_int2(g, k * chunk);
   }
-  base = __shfl_sync(0xffffffffu, base, 0);
-  for (int k = lane; k < nitems; k += 32) items[base + k] = make_int2(I, k * chunk);
 }
 
 __global__ void k_prune_end(int* flag_prune, int* counters) {
@@ -494,6 +526,7 @@ void launch_rebuild_build(const RebuildArgs& a, cudaStream_t st) {
   k_rb_bbox<<<(maxblk * 32 + 255) / 256, 256, 0, st>>>(p, a.flag, a.counters, a.perm, a.xyzq_s, a.bb_lo, a.bb_hi);
   k_rb_outer<<<(maxblk + 7) / 8, 256, 0, st>>>(p, a.flag, a.counters, a.perm, a.xyzq_s, a.bb_lo, a.bb_hi, a.blk_col,
                                                a.col_start, a.dcx, a.dcy, a.all_images, a.outer, a.outer_n, a.ocap,
+                                               a.xn, a.xs, a.xmax,
                                                a.status);
   k_rb_end<<<1, 1, 0, st>>>(a.flag, a.flag_prune, a.counters);
 }

@@ -89,8 +89,13 @@ __device__ __forceinline__ float pair_force(const PairConst& c, float r2, float 
   return ok ? fr : 0.f;
 }
 
-// One 32 x 32 tile: j data (image shift applied) staged in this warp's shared ring,
-// i force accumulated in registers, j force rotated and flushed at the end.
+// One tile of kIG i atoms x 32 j entries.  Lane = h * kIG + il holds i atom il of the
+// group and works on segment h of the j entries (kIG of them); the tile's j data
+// (image shift applied) are staged in this warp's shared ring, doubled within each
+// segment, so at step k lane il reads entry h * kIG + (il + k) % kIG at a constant
+// offset; the i force stays in registers, each j force accumulator rotates through
+// its segment (3 width-kIG shuffles per step) and is back on the lane that loaded the
+// entry after kIG steps.  excl: bit e set when entry e is excluded for this lane's i.
 template <bool ENERGY>
 __device__ __forceinline__ void run_tile(const PairConst& c, const SysParams& p, const float4& xi, float qi,
                                          const float2* ljrow, uint32_t je, uint32_t excl, float4* jx, int* jt,
@@ -108,20 +113,28 @@ __device__ __forceinline__ void run_tile(const PairConst& c, const SysParams& p,
     xj.z += s.z;
   }
   const int tyj = typ[jslot];
+  const int il = lane & (kIG - 1), seg = (lane / kIG) * 2 * kIG;
   __syncwarp();
-  jx[lane] = xj;
-  jx[lane + 32] = xj;
-  jt[lane] = tyj;
-  jt[lane + 32] = tyj;
+  jx[seg + il] = xj;
+  jx[seg + il + kIG] = xj;
+  jt[seg + il] = tyj;
+  jt[seg + il + kIG] = tyj;
   __syncwarp();
-  // bit k of mrot: pair (lane, lane + k) excluded
-  const uint32_t mrot = __funnelshift_r(excl, excl, lane);
-  const float4* jxl = jx + lane;
-  const int* jtl = jt + lane;
+  // bit k of mrot: pair (il, entry h * kIG + (il + k) % kIG) excluded
+  uint32_t mrot;
+  if (kIG == 32) {
+    mrot = __funnelshift_r(excl, excl, il);
+  } else {
+    const uint32_t segm = (1u << (kIG & 31)) - 1u;
+    const uint32_t w = (excl >> ((lane / kIG) * kIG)) & segm;
+    mrot = ((w >> il) | (w << ((kIG - il) & 31))) & segm;
+  }
+  const float4* jxl = jx + seg + il;
+  const int* jtl = jt + seg + il;
   float fjx = 0.f, fjy = 0.f, fjz = 0.f;
   if (__any_sync(0xffffffffu, mrot != 0u)) {
 #pragma unroll 8
-    for (int k = 0; k < 32; ++k) {
+    for (int k = 0; k < kIG; ++k) {
       const float4 b = jxl[k];
       const float dx = xi.x - b.x, dy = xi.y - b.y, dz = xi.z - b.z;
       const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
@@ -135,13 +148,13 @@ __device__ __forceinline__ void run_tile(const PairConst& c, const SysParams& p,
       fix = fmaf(fr, dx, fix);
       fiy = fmaf(fr, dy, fiy);
       fiz = fmaf(fr, dz, fiz);
-      fjx = __shfl_sync(0xffffffffu, fmaf(-fr, dx, fjx), src);
-      fjy = __shfl_sync(0xffffffffu, fmaf(-fr, dy, fjy), src);
-      fjz = __shfl_sync(0xffffffffu, fmaf(-fr, dz, fjz), src);
+      fjx = __shfl_sync(0xffffffffu, fmaf(-fr, dx, fjx), src, kIG);
+      fjy = __shfl_sync(0xffffffffu, fmaf(-fr, dy, fjy), src, kIG);
+      fjz = __shfl_sync(0xffffffffu, fmaf(-fr, dz, fjz), src, kIG);
     }
   } else {
 #pragma unroll 8
-    for (int k = 0; k < 32; ++k) {
+    for (int k = 0; k < kIG; ++k) {
       const float4 b = jxl[k];
       const float dx = xi.x - b.x, dy = xi.y - b.y, dz = xi.z - b.z;
       const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
@@ -154,9 +167,9 @@ __device__ __forceinline__ void run_tile(const PairConst& c, const SysParams& p,
       fix = fmaf(fr, dx, fix);
       fiy = fmaf(fr, dy, fiy);
       fiz = fmaf(fr, dz, fiz);
-      fjx = __shfl_sync(0xffffffffu, fmaf(-fr, dx, fjx), src);
-      fjy = __shfl_sync(0xffffffffu, fmaf(-fr, dy, fjy), src);
-      fjz = __shfl_sync(0xffffffffu, fmaf(-fr, dz, fjz), src);
+      fjx = __shfl_sync(0xffffffffu, fmaf(-fr, dx, fjx), src, kIG);
+      fjy = __shfl_sync(0xffffffffu, fmaf(-fr, dy, fjy), src, kIG);
+      fjz = __shfl_sync(0xffffffffu, fmaf(-fr, dz, fjz), src, kIG);
     }
   }
   const int aj = perm[jslot];
@@ -189,57 +202,69 @@ __global__ void __launch_bounds__(256, MINB)
   float4* jx = jx_all[warp];
   int* jt = jt_all[warp];
   const int n = p.n;
-  const int src = (lane + 1) & 31;
-  double e_vdw = 0.0, e_el = 0.0, w_acc[3] = {0.0, 0.0, 0.0};
+  const int il = lane & (kIG - 1);
+  const int src = (il + 1) & (kIG - 1);  // segment-relative source lane of the j-force rotation
+  // energy and virial sums per lane in fixed point, item by item: integer sums do not
+  // depend on which items a warp happens to fetch, so energies are bit-reproducible
+  long long e_vdw = 0, e_el = 0, w_acc[3] = {0, 0, 0};
   for (;;) {
     int it = 0;
     if (lane == 0) it = atomicAdd(&counters[CNT_WORK], 1);
     it = __shfl_sync(0xffffffffu, it, 0);
     if (it >= nitems) break;
     const int2 item = items[it];
-    const int I = item.x;
-    const int islot = I * 32 + lane;
+    const int g = item.x;  // i-group: block I, atoms s * kIG .. s * kIG + kIG - 1
+    const int I = g / kNG, s = g % kNG;
+    const int ib = s * kIG + il;  // this lane's i atom, index within the block
+    const int islot = I * 32 + ib;
     const float4 xi = xyzq[islot];
     const float2* ljrow = lj + typ[islot] * nt1;
     const float qi = xi.w * p.cc;
     float fix = 0.f, fiy = 0.f, fiz = 0.f;
     float ev = 0.f, ee = 0.f, vir[3] = {0.f, 0.f, 0.f};
-    // tile 0 of a block is the diagonal (the block with itself, upper triangle j > i)
+    // tile 0 of a group is the group against its own block (upper triangle j > i)
     int t = item.y;
-    const int tend = min(inner_nt[I] + 1, t + chunk);
+    const int tend = min(inner_nt[g] + 1, t + chunk);
     if (t == 0) {
-      const uint32_t tri = (lane == 31) ? 0xffffffffu : ((2u << lane) - 1u);
-      run_tile<ENERGY>(c, p, xi, qi, ljrow, (uint32_t)islot | ((uint32_t)kNoShift << kSlotBits),
+      const uint32_t tri = (ib == 31) ? 0xffffffffu : ((2u << ib) - 1u);
+      run_tile<ENERGY>(c, p, xi, qi, ljrow, (uint32_t)(I * 32 + lane) | ((uint32_t)kNoShift << kSlotBits),
                        dmask[islot] | tri, jx, jt, xyzq, typ, perm, facc, lane, src, fix, fiy, fiz, ev, ee,
                        vir);
       t = 1;
     }
-    const uint32_t* jl = inner + (size_t)I * ocap - 32;  // inner tile t-1
-    const int* ml = inner_m + (size_t)I * (ocap >> 5) - 1;
+    const uint32_t* jl = inner + (size_t)g * ocap - 32;  // inner tile t-1
+    const int* ml = inner_m + (size_t)g * (ocap >> 5) - 1;
     for (; t < tend; ++t) {
       const int m = ml[t];
-      const uint32_t excl = m >= 0 ? masks[(size_t)m * 32 + lane] : 0u;
+      const uint32_t excl = m >= 0 ? masks[(size_t)m * kIG + il] : 0u;
       run_tile<ENERGY>(c, p, xi, qi, ljrow, jl[t * 32 + lane], excl, jx, jt, xyzq, typ, perm, facc, lane, src, fix,
                        fiy, fiz, ev, ee, vir);
     }
+    // the i force of lane il is split over the 32 / kIG segments
+#pragma unroll
+    for (int off = kIG; off < 32; off <<= 1) {
+      fix += __shfl_xor_sync(0xffffffffu, fix, off);
+      fiy += __shfl_xor_sync(0xffffffffu, fiy, off);
+      fiz += __shfl_xor_sync(0xffffffffu, fiz, off);
+    }
     const int ai = perm[islot];
-    if (ai >= 0) {
+    if (lane < kIG && ai >= 0) {
       red_add(facc + ai, to_fix(fix));
       red_add(facc + n + ai, to_fix(fiy));
       red_add(facc + 2 * n + ai, to_fix(fiz));
     }
     if (ENERGY) {
-      e_vdw += (double)ev;
-      e_el += (double)ee;
-      for (int d = 0; d < 3; ++d) w_acc[d] += (double)vir[d];
+      e_vdw += __double2ll_rn((double)ev * kFixE);
+      e_el += __double2ll_rn((double)ee * kFixE);
+      for (int d = 0; d < 3; ++d) w_acc[d] += __double2ll_rn((double)vir[d] * kFixE);
     }
   }
   if (ENERGY) {
-    energy_add(energy + EN_VDW, e_vdw);
-    energy_add(energy + EN_ELEC, e_el);
-    energy_add(energy + EN_VIR_X, w_acc[0]);
-    energy_add(energy + EN_VIR_Y, w_acc[1]);
-    energy_add(energy + EN_VIR_Z, w_acc[2]);
+    energy_add_fix(energy + EN_VDW, e_vdw);
+    energy_add_fix(energy + EN_ELEC, e_el);
+    energy_add_fix(energy + EN_VIR_X, w_acc[0]);
+    energy_add_fix(energy + EN_VIR_Y, w_acc[1]);
+    energy_add_fix(energy + EN_VIR_Z, w_acc[2]);
   }
 }
 

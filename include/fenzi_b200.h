@@ -170,7 +170,8 @@ fz_status fz_get_forces_fixed(fz_system* sys, long long* out3n);
 fz_status fz_set_state_f32(fz_system* sys, const float* pos3n, const float* vel3n);
 fz_status fz_get_state_f32(fz_system* sys, float* pos3n, float* vel3n);
 /* Device-side work counters: [0] kernel launches issued, [1] neighbour-list rebuilds,
- * [2] 32x32 pair tiles in the current (pruned) list, [3] list prunes. */
+ * [2] pair slots (i x j pairs the pair kernel evaluates per step, within or beyond the
+ * cutoff) of the current pruned list, [3] list prunes. */
 fz_status fz_get_counters(fz_system* sys, long long* out4);
 /* Virial diagonal accumulated by the last fz_compute_forces_terms(..., energies = 1)
  * (force terms only: no constraint or kinetic part). */
