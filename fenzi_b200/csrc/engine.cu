@@ -152,11 +152,12 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
   e->ncons = (int)t.cons_d.size();
   int dev_sms = 148;
   cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device);
-  // pair kernel CTAs per SM: 3 (80-register build) or 4 (64-register build), env
-  // FZ_NB_CTAS_PER_SM; PME overlaps it on a second stream
+  // pair kernel CTAs per SM: 4 (64-register build, default: 0.614 vs 0.624 ms/step at
+  // 230,400 atoms) or 3 (80-register build), env FZ_NB_CTAS_PER_SM; PME overlaps it on
+  // a second stream
   {
     const char* v = std::getenv("FZ_NB_CTAS_PER_SM");
-    const int per = v ? std::max(1, std::min(4, std::atoi(v))) : 3;
+    const int per = v ? std::max(1, std::min(4, std::atoi(v))) : 4;
     e->nb_grid = dev_sms * per;
     e->nb_per_sm = per;
   }

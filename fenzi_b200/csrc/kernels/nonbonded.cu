@@ -89,7 +89,8 @@ __device__ __forceinline__ float pair_force(const PairConst& c, float r2, float 
   return ok ? fr : 0.f;
 }
 
-// One tile of kIG i atoms x 32 j entries.  Lane = h * kIG + il holds i atom il of the
+// One tile of kIG i atoms x 32 j entries (xj, tyj: this lane's entry, loaded by the
+// caller one tile ahead).  Lane = h * kIG + il holds i atom il of the
 // group and works on segment h of the j entries (kIG of them); the tile's j data
 // (image shift applied) are staged in this warp's shared ring, doubled within each
 // segment, so at step k lane il reads entry h * kIG + (il + k) % kIG at a constant
@@ -98,21 +99,18 @@ __device__ __forceinline__ float pair_force(const PairConst& c, float r2, float 
 // entry after kIG steps.  excl: bit e set when entry e is excluded for this lane's i.
 template <bool ENERGY>
 __device__ __forceinline__ void run_tile(const PairConst& c, const SysParams& p, const float4& xi, float qi,
-                                         const float2* ljrow, uint32_t je, uint32_t excl, float4* jx, int* jt,
-                                         const float4* __restrict__ xyzq, const int* __restrict__ typ,
-                                         const int* __restrict__ perm, long long* __restrict__ facc, int lane,
-                                         int src, float& fix, float& fiy, float& fiz, float& ev, float& ee,
-                                         float* vir) {
+                                         const float2* ljrow, uint32_t je, uint32_t excl, float4 xj, int tyj,
+                                         float4* jx, int* jt, const int* __restrict__ perm,
+                                         long long* __restrict__ facc, int lane, int src, float& fix, float& fiy,
+                                         float& fiz, float& ev, float& ee, float* vir) {
   const int jslot = (int)(je & kSlotMask);
   const int code = (int)(je >> kSlotBits);
-  float4 xj = xyzq[jslot];
   if (code != kNoShift) {
     const float3 s = shift_of(code, p);
     xj.x += s.x;
     xj.y += s.y;
     xj.z += s.z;
   }
-  const int tyj = typ[jslot];
   const int il = lane & (kIG - 1), seg = (lane / kIG) * 2 * kIG;
   __syncwarp();
   jx[seg + il] = xj;
@@ -222,23 +220,35 @@ __global__ void __launch_bounds__(256, MINB)
     const float qi = xi.w * p.cc;
     float fix = 0.f, fiy = 0.f, fiz = 0.f;
     float ev = 0.f, ee = 0.f, vir[3] = {0.f, 0.f, 0.f};
-    // tile 0 of a group is the group against its own block (upper triangle j > i)
+    // tile 0 of a group is the group against its own block (upper triangle j > i);
+    // each tile's entry, exclusion word and j data are loaded one tile ahead
     int t = item.y;
     const int tend = min(inner_nt[g] + 1, t + chunk);
-    if (t == 0) {
-      const uint32_t tri = (ib == 31) ? 0xffffffffu : ((2u << ib) - 1u);
-      run_tile<ENERGY>(c, p, xi, qi, ljrow, (uint32_t)(I * 32 + lane) | ((uint32_t)kNoShift << kSlotBits),
-                       dmask[islot] | tri, jx, jt, xyzq, typ, perm, facc, lane, src, fix, fiy, fiz, ev, ee,
-                       vir);
-      t = 1;
-    }
     const uint32_t* jl = inner + (size_t)g * ocap - 32;  // inner tile t-1
     const int* ml = inner_m + (size_t)g * (ocap >> 5) - 1;
+    auto fetch = [&](int tt, uint32_t& je, uint32_t& ex, float4& xj, int& tyj) {
+      if (tt == 0) {
+        je = (uint32_t)(I * 32 + lane) | ((uint32_t)kNoShift << kSlotBits);
+        ex = dmask[islot] | ((ib == 31) ? 0xffffffffu : ((2u << ib) - 1u));
+      } else {
+        je = jl[tt * 32 + lane];
+        const int m = ml[tt];
+        ex = m >= 0 ? masks[(size_t)m * kIG + il] : 0u;
+      }
+      xj = xyzq[je & kSlotMask];
+      tyj = typ[je & kSlotMask];
+    };
+    uint32_t je_n, ex_n;
+    float4 xj_n;
+    int ty_n;
+    fetch(t, je_n, ex_n, xj_n, ty_n);
     for (; t < tend; ++t) {
-      const int m = ml[t];
-      const uint32_t excl = m >= 0 ? masks[(size_t)m * kIG + il] : 0u;
-      run_tile<ENERGY>(c, p, xi, qi, ljrow, jl[t * 32 + lane], excl, jx, jt, xyzq, typ, perm, facc, lane, src, fix,
-                       fiy, fiz, ev, ee, vir);
+      const uint32_t je = je_n, ex = ex_n;
+      const float4 xj = xj_n;
+      const int ty = ty_n;
+      if (t + 1 < tend) fetch(t + 1, je_n, ex_n, xj_n, ty_n);
+      run_tile<ENERGY>(c, p, xi, qi, ljrow, je, ex, xj, ty, jx, jt, perm, facc, lane, src, fix, fiy, fiz, ev, ee,
+                       vir);
     }
     // the i force of lane il is split over the 32 / kIG segments
 #pragma unroll
