@@ -91,7 +91,7 @@ EXPORTS = ["fz_last_error", "fz_version", "fz_read_input", "fz_load_system", "fz
            "fz_pme_reciprocal_static", "fz_batch_create", "fz_batch_add", "fz_batch_step", "fz_batch_free",
            "fz_set_barostat", "fz_get_virial", "fz_batch_remove", "fz_batch_size", "fz_server_create",
            "fz_server_submit", "fz_server_info", "fz_server_wait", "fz_server_positions", "fz_server_stats",
-           "fz_server_free", "fz_server_estimate_bytes"]
+           "fz_server_free", "fz_server_estimate_bytes", "fz_checkpoint_save", "fz_checkpoint_load"]
 
 STAGES = ["neighbour", "nonbonded", "bonded", "pme", "integrate"]
 
@@ -154,6 +154,8 @@ def lib():
             "fz_server_stats": ([vp, dp], C.c_int),
             "fz_server_free": ([vp], C.c_int),
             "fz_server_estimate_bytes": ([vp, dp], C.c_int),
+            "fz_checkpoint_save": ([vp, C.c_char_p, C.c_int], C.c_int),
+            "fz_checkpoint_load": ([vp, C.c_char_p, C.c_int], C.c_int),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -265,6 +267,14 @@ class FenZi:
         e = Energies()
         _check(lib().fz_eval_props(self.h, C.byref(e)))
         return e.as_dict()
+
+    def SaveCheckpoint(self, path: str, fmt: str | None = None):
+        """Restart file in the reference's layout: fmt 'a' (ascii), 'b' (binary) or None
+        (the input's checkpointformat)."""
+        _check(lib().fz_checkpoint_save(self.h, path.encode(), ord(fmt) if fmt else 0))
+
+    def LoadCheckpoint(self, path: str, fmt: str | None = None):
+        _check(lib().fz_checkpoint_load(self.h, path.encode(), ord(fmt) if fmt else 0))
 
     def set_barostat(self, enable: bool = True, pref_atm: float | None = None, pmass: float | None = None):
         """Andersen constant-pressure dynamics (the reference's PCONSTANT build) for the

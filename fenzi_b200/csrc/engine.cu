@@ -375,7 +375,7 @@ constexpr double kPatm = 68558.64100846418;     // kcal/mol/A^3 -> atm (src/cell
 
 // Moves the engine to a new box (x edge L, aspect ratios kept): parameters passed by
 // value to the kernels, the column search reach, and the PME influence tables.
-static fz_status set_box(Engine* e, double L) {
+fz_status set_box(Engine* e, double L) {
   fzk::SysParams& p = e->p;
   for (int d = 0; d < 3; ++d) e->box_d[d] = L * e->ratio[d];
   const double lmin = std::min(e->box_d[0], std::min(e->box_d[1], e->box_d[2]));

@@ -504,4 +504,8 @@ struct Engine {
   }
 };
 
+// moves an engine to the box with x edge L (aspect ratios kept): kernel parameters,
+// column reach and PME influence tables (engine.cu)
+fz_status set_box(Engine* e, double L);
+
 }  // namespace fz

@@ -149,6 +149,13 @@ fz_status fz_step(fz_system* sys, int nsteps);
  * virial (force terms, PME reciprocal term and the instantaneous constraint forces)
  * and the pressure (src/evalprops.cu:214-218). */
 fz_status fz_eval_props(fz_system* sys, fz_energies* out);
+/* SaveCheckpointBinary/Ascii and LoadCheckpointBinary/Ascii (src/prmwrite.cu:31-252):
+ * restart files in the reference's two layouts; format 'a' (ascii), 'b' (binary) or 0
+ * (the input's checkpointformat, binary when unset).  Loading sets positions,
+ * velocities, the step count, the seed and the box (and the barostat's box velocity);
+ * the atom count must match. */
+fz_status fz_checkpoint_save(fz_system* sys, const char* path, int format);
+fz_status fz_checkpoint_load(fz_system* sys, const char* path, int format);
 /* Andersen constant-pressure dynamics for the following fz_step calls (the reference's
  * PCONSTANT build: src/cell_based_kernels.cu:566-579 piston acceleration,
  * src/mdcuda.cu:58-88 half kicks; keywords pref/pmass, src/prmread.cu:663-670).

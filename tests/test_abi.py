@@ -36,12 +36,11 @@ def test_device_calls_before_upload_fail_cleanly():
     from tests.helpers import system
     _, path = system("small")
     s = fz.FenZi.ReadInput(path).LoadSystem()
-    try:
-        s.SingleStep(1)
-    except fz.FenZiError as e:
-        assert e.code == 7
-    else:
-        raise AssertionError("expected FZ_ERR_STATE")
+    for call in (lambda: s.SingleStep(1), lambda: s.SaveCheckpoint("/nonexistent/x.rst", "b"),
+                 lambda: s.LoadCheckpoint("/nonexistent/x.rst", "b")):
+        with pytest.raises(fz.FenZiError) as ei:
+            call()
+        assert ei.value.code == 7  # FZ_ERR_STATE
 
 
 def test_server_without_gpu_fails_cleanly():
