@@ -91,7 +91,8 @@ EXPORTS = ["fz_last_error", "fz_version", "fz_read_input", "fz_load_system", "fz
            "fz_pme_reciprocal_static", "fz_batch_create", "fz_batch_add", "fz_batch_step", "fz_batch_free",
            "fz_set_barostat", "fz_get_virial", "fz_batch_remove", "fz_batch_size", "fz_server_create",
            "fz_server_submit", "fz_server_info", "fz_server_wait", "fz_server_positions", "fz_server_stats",
-           "fz_server_free", "fz_server_estimate_bytes", "fz_checkpoint_save", "fz_checkpoint_load"]
+           "fz_server_free", "fz_server_estimate_bytes", "fz_checkpoint_save", "fz_checkpoint_load",
+           "fz_dcd_open", "fz_dcd_write", "fz_dcd_close"]
 
 STAGES = ["neighbour", "nonbonded", "bonded", "pme", "integrate"]
 
@@ -156,6 +157,9 @@ def lib():
             "fz_server_estimate_bytes": ([vp, dp], C.c_int),
             "fz_checkpoint_save": ([vp, C.c_char_p, C.c_int], C.c_int),
             "fz_checkpoint_load": ([vp, C.c_char_p, C.c_int], C.c_int),
+            "fz_dcd_open": ([vp, C.c_char_p, C.c_int, C.POINTER(vp)], C.c_int),
+            "fz_dcd_write": ([vp], C.c_int),
+            "fz_dcd_close": ([vp], C.c_int),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -462,6 +466,28 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+class Trajectory:
+    """CHARMM DCD trajectory of one system (fz_dcd_*): write() appends the current frame."""
+
+    def __init__(self, system: FenZi, path: str, every: int = 1):
+        self.h = C.c_void_p()
+        _check(lib().fz_dcd_open(system.h, path.encode(), int(every), C.byref(self.h)))
+
+    def write(self):
+        _check(lib().fz_dcd_write(self.h))
+
+    def close(self):
+        if self.h:
+            _check(lib().fz_dcd_close(self.h))
+            self.h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def pme_reciprocal_static(device, pos4_ptr, n, box, K, beta, facc_ptr, stream=None, energy=True):

@@ -119,3 +119,101 @@ extern "C" fz_status fz_checkpoint_load(fz_system* s, const char* path, int form
   e->seed = (unsigned long long)(long long)seed;
   return fz_set_state_f32(s, pos.data(), vel.data());
 }
+
+// ---------------------------------------------------------------- DCD trajectories
+// The CHARMM DCD layout the reference writes through charmm_trj_write_header/titles/
+// natoms/frame (src/io/charmmio.c, called from src/fenzi.cu:280-340, 513-528): Fortran
+// unformatted records (int32 length, payload, int32 length).  Header record "CORD" +
+// 20 int32 control words: frames, first step, output frequency, steps, 3 zeros,
+// degrees-of-freedom word 1, fixed atoms 0, time step (float, AKMA units), unit cell
+// flag 1, 4-D flag 0, charges flag 0, 6 zeros, version 34.  Then one 80-character
+// title, the atom count, and per frame a unit-cell record of 6 doubles (A, 0, B, 0, 0,
+// C for the rectangular box) and the X, Y, Z float records.
+struct fz_dcd {
+  fz_system* sys = nullptr;
+  FILE* f = nullptr;
+  int every = 1, frames = 0;
+  std::vector<float> pos, buf;
+};
+
+static bool rec(FILE* f, const void* a, uint32_t na, const void* b = nullptr, uint32_t nb = 0) {
+  const uint32_t len = na + nb;
+  return std::fwrite(&len, 4, 1, f) == 1 && (na == 0 || std::fwrite(a, 1, na, f) == na) &&
+         (nb == 0 || std::fwrite(b, 1, nb, f) == nb) && std::fwrite(&len, 4, 1, f) == 1;
+}
+
+static bool dcd_header(fz_dcd* d) {
+  const fz_system* s = d->sys;
+  uint32_t ctl[20] = {};
+  ctl[0] = (uint32_t)d->frames;
+  ctl[1] = (uint32_t)d->every;
+  ctl[2] = (uint32_t)d->every;
+  ctl[3] = (uint32_t)(d->frames * d->every);
+  ctl[7] = 1;
+  ctl[8] = 0;
+  const float dt = (float)(s->cfg.timestep_ps / 4.888821e-2);  // ps -> AKMA time (src/fenzi.cu:320)
+  std::memcpy(&ctl[9], &dt, 4);
+  ctl[10] = 1;
+  ctl[11] = 0;
+  ctl[12] = 0;
+  ctl[19] = 34;
+  char title[80];
+  std::memset(title, ' ', 80);
+  const char* t = "Generated by fenzi_b200";
+  std::memcpy(title, t, std::strlen(t));
+  const int32_t ntitles = 1, natoms = s->top.n;
+  return rec(d->f, "CORD", 4, ctl, sizeof ctl) && rec(d->f, &ntitles, 4, title, 80) && rec(d->f, &natoms, 4);
+}
+
+extern "C" fz_status fz_dcd_open(fz_system* s, const char* path, int every, fz_dcd** out) {
+  if (!s || !path || !out) return fail(FZ_ERR_ARG, "null argument");
+  if (!s->eng) return fail(FZ_ERR_STATE, "fz_upload has not been called");
+  fz_dcd* d = new fz_dcd();
+  d->sys = s;
+  d->every = every > 0 ? every : 1;
+  d->f = std::fopen(path, "wb");
+  if (!d->f) {
+    delete d;
+    return fail(FZ_ERR_IO, std::string("cannot write ") + path);
+  }
+  if (!dcd_header(d)) {
+    std::fclose(d->f);
+    delete d;
+    return fail(FZ_ERR_IO, std::string("write error on ") + path);
+  }
+  *out = d;
+  return FZ_OK;
+}
+
+extern "C" fz_status fz_dcd_write(fz_dcd* d) {
+  if (!d || !d->f) return fail(FZ_ERR_ARG, "null trajectory");
+  fz_system* s = d->sys;
+  if (!s->eng) return fail(FZ_ERR_STATE, "the system's device state is gone");
+  const int n = s->top.n;
+  d->pos.resize(3 * (size_t)n);
+  d->buf.resize((size_t)n);
+  fz_status r;
+  if ((r = fz_get_state_f32(s, d->pos.data(), nullptr))) return r;
+  const Engine* e = s->eng;
+  const double cell[6] = {e->box_d[0], 0.0, e->box_d[1], 0.0, 0.0, e->box_d[2]};
+  bool ok = rec(d->f, cell, sizeof cell);
+  for (int c = 0; ok && c < 3; ++c) {
+    for (int i = 0; i < n; ++i) d->buf[i] = d->pos[3 * (size_t)i + c];
+    ok = rec(d->f, d->buf.data(), 4u * (uint32_t)n);
+  }
+  if (!ok) return fail(FZ_ERR_IO, "trajectory write error");
+  d->frames++;
+  return FZ_OK;
+}
+
+extern "C" fz_status fz_dcd_close(fz_dcd* d) {
+  if (!d) return FZ_OK;
+  bool ok = true;
+  if (d->f) {
+    // the header's frame and step counts are those written
+    ok = std::fseek(d->f, 0, SEEK_SET) == 0 && dcd_header(d);
+    ok = (std::fclose(d->f) == 0) && ok;
+  }
+  delete d;
+  return ok ? FZ_OK : fail(FZ_ERR_IO, "trajectory close error");
+}

@@ -156,6 +156,14 @@ fz_status fz_eval_props(fz_system* sys, fz_energies* out);
  * the atom count must match. */
 fz_status fz_checkpoint_save(fz_system* sys, const char* path, int format);
 fz_status fz_checkpoint_load(fz_system* sys, const char* path, int format);
+/* CHARMM DCD trajectory (charmm_trj_write_header/titles/natoms/frame,
+ * src/io/charmmio.c; written every trjFreq steps by src/fenzi.cu:513-528): open writes
+ * the header, write appends the system's current positions and unit cell, close
+ * patches the frame count.  every = steps between frames (header only). */
+typedef struct fz_dcd fz_dcd;
+fz_status fz_dcd_open(fz_system* sys, const char* path, int every, fz_dcd** out);
+fz_status fz_dcd_write(fz_dcd* traj);
+fz_status fz_dcd_close(fz_dcd* traj);
 /* Andersen constant-pressure dynamics for the following fz_step calls (the reference's
  * PCONSTANT build: src/cell_based_kernels.cu:566-579 piston acceleration,
  * src/mdcuda.cu:58-88 half kicks; keywords pref/pmass, src/prmread.cu:663-670).

@@ -70,3 +70,39 @@ def test_load_rejects_wrong_atom_count_and_missing_file():
         s.LoadCheckpoint(os.path.join(d, "missing.rst"), "b")
     assert ei.value.code == 1  # FZ_ERR_IO
     s.close()
+
+
+def _records(raw):
+    out, o = [], 0
+    while o < len(raw):
+        n, = struct.unpack_from("<i", raw, o)
+        out.append(raw[o + 4:o + 4 + n])
+        assert struct.unpack_from("<i", raw, o + 4 + n)[0] == n
+        o += 8 + n
+    return out
+
+
+def test_dcd_layout_and_frames():
+    s = _sys()
+    s.InitVelocity(T=300.0, seed=5, counter=0)
+    path = os.path.join(tempfile.mkdtemp(prefix="fzdcd_"), "t.dcd")
+    frames = []
+    with fz.Trajectory(s, path, every=10) as tr:
+        for _ in range(3):
+            s.SingleStep(10)
+            tr.write()
+            frames.append(s.positions().astype(np.float32))
+    r = _records(open(path, "rb").read())
+    assert r[0][:4] == b"CORD"
+    ctl = struct.unpack("<20i", r[0][4:84])
+    assert ctl[0] == 3 and ctl[1] == 10 and ctl[2] == 10 and ctl[3] == 30 and ctl[10] == 1 and ctl[19] == 34
+    assert abs(struct.unpack("<f", r[0][40:44])[0] - s.cfg.timestep_ps / 4.888821e-2) < 1e-6
+    assert struct.unpack_from("<i", r[1])[0] == 1 and len(r[1]) == 84
+    assert struct.unpack("<i", r[2])[0] == s.n
+    assert len(r) == 3 + 3 * 4
+    for k in range(3):
+        cell = struct.unpack("<6d", r[3 + 4 * k])
+        assert np.allclose([cell[0], cell[2], cell[5]], s.cfg.box[:3]) and cell[1] == cell[3] == cell[4] == 0.0
+        xyz = np.stack([np.frombuffer(r[4 + 4 * k + c], dtype="<f4") for c in range(3)], axis=1)
+        assert np.array_equal(xyz, frames[k])
+    s.close()
