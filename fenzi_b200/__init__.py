@@ -92,7 +92,7 @@ EXPORTS = ["fz_last_error", "fz_version", "fz_read_input", "fz_load_system", "fz
            "fz_set_barostat", "fz_get_virial", "fz_batch_remove", "fz_batch_size", "fz_server_create",
            "fz_server_submit", "fz_server_info", "fz_server_wait", "fz_server_positions", "fz_server_stats",
            "fz_server_free", "fz_server_estimate_bytes", "fz_checkpoint_save", "fz_checkpoint_load",
-           "fz_dcd_open", "fz_dcd_write", "fz_dcd_close"]
+           "fz_dcd_open", "fz_dcd_write", "fz_dcd_close", "fz_minimize"]
 
 STAGES = ["neighbour", "nonbonded", "bonded", "pme", "integrate"]
 
@@ -160,6 +160,7 @@ def lib():
             "fz_dcd_open": ([vp, C.c_char_p, C.c_int, C.POINTER(vp)], C.c_int),
             "fz_dcd_write": ([vp], C.c_int),
             "fz_dcd_close": ([vp], C.c_int),
+            "fz_minimize": ([vp, C.c_int, C.POINTER(C.c_int), dp], C.c_int),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -271,6 +272,13 @@ class FenZi:
         e = Energies()
         _check(lib().fz_eval_props(self.h, C.byref(e)))
         return e.as_dict()
+
+    def Minimize(self, nsteps: int | None = None):
+        """MinimizeStep loop (CG then SD); returns (moves made, final potential energy)."""
+        k, e = C.c_int(), C.c_double()
+        n = self.cfg.minimize_steps if nsteps is None else nsteps
+        _check(lib().fz_minimize(self.h, int(n), C.byref(k), C.byref(e)))
+        return k.value, e.value
 
     def SaveCheckpoint(self, path: str, fmt: str | None = None):
         """Restart file in the reference's layout: fmt 'a' (ascii), 'b' (binary) or None

@@ -628,6 +628,72 @@ extern "C" fz_status fz_eval_props(fz_system* s, fz_energies* out) {
   return FZ_OK;
 }
 
+// MinimizeStep loop of the reference's main (src/dynamics.cu:491-620,
+// src/fenzi.cu:397-418): conjugate-gradient moves until the energy rises, then
+// steepest descent until it rises again; a move that raises the energy is undone and
+// retried with the next method; every 100 steps the step factor is multiplied by
+// 100 x its rate (conjgradrate / steepdesrate).
+extern "C" fz_status fz_minimize(fz_system* s, int max_steps, int* steps_done, double* energy_out) {
+  fz_status r;
+  if ((r = need_engine(s))) return r;
+  if (max_steps < 0) return fail(FZ_ERR_ARG, "fz_minimize: max_steps < 0");
+  Engine* e = s->eng;
+  const fz_config& c = s->cfg;
+  if (!e->min_pos) {
+    if ((r = e->alloc(&e->min_prev_f, e->n)) || (r = e->alloc(&e->min_dir, e->n)) || (r = e->alloc(&e->min_pos, e->n)))
+      return r;
+  } else {
+    FZ_CUDA(cudaMemsetAsync(e->min_prev_f, 0, sizeof(float4) * e->n, e->st));
+    FZ_CUDA(cudaMemsetAsync(e->min_dir, 0, sizeof(float4) * e->n, e->st));
+  }
+  e->drop_graph();
+  auto energy = [&](double* out) -> fz_status {
+    FZ_CUDA(cudaMemsetAsync(e->facc, 0, 3 * sizeof(long long) * e->n, e->st));
+    FZ_CUDA(cudaMemsetAsync(e->energy, 0, fzk::EN_COUNT * sizeof(long long), e->st));
+    e->forces(true);
+    e->forces_valid = true;
+    long long en[fzk::EN_COUNT];
+    fz_status rr = read_slots(e, en, nullptr);
+    if (rr) return rr;
+    double u = e->self_energy;
+    for (int k = fzk::EN_BOND; k <= fzk::EN_EWEXCL; ++k) u += en[k] / fzk::kFixE;
+    *out = u;
+    return FZ_OK;
+  };
+  int method = 1;
+  double fac[3] = {0.0, c.conjgradfac, c.steepdesfac};
+  const double rate[3] = {0.0, c.conjgradrate, c.steepdesrate};
+  double prev = 0.0, cur = 0.0;
+  if ((r = energy(&cur))) return r;
+  int step = 0;
+  for (; step < max_steps && method != 0; ++step) {
+    FZ_CUDA(cudaMemcpyAsync(e->min_pos, e->pos4, sizeof(float4) * e->n, cudaMemcpyDeviceToDevice, e->st));
+    fzk::IntegrateArgs ia = e->int_args();
+    ia.min_prev_f = e->min_prev_f;
+    ia.min_dir = e->min_dir;
+    ia.min_method = method;
+    ia.min_fac = (float)fac[method];
+    fzk::launch_min_step(ia, e->st);
+    prev = cur;
+    if ((r = energy(&cur))) return r;
+    if (cur > prev) {  // undo the move, switch method
+      FZ_CUDA(cudaMemcpyAsync(e->pos4, e->min_pos, sizeof(float4) * e->n, cudaMemcpyDeviceToDevice, e->st));
+      const int one = 1;
+      FZ_CUDA(cudaMemcpyAsync(e->flag, &one, sizeof(int), cudaMemcpyHostToDevice, e->st));
+      if ((r = energy(&cur))) return r;
+      method = method == 1 ? 2 : 0;
+    }
+    if (step > 0 && step % 100 == 0 && method != 0) fac[method] *= rate[method] * 100.0;
+  }
+  FZ_CUDA(cudaMemsetAsync(e->facc, 0, 3 * sizeof(long long) * e->n, e->st));
+  e->forces(false);
+  e->forces_valid = true;
+  if ((r = e->check())) return r;
+  if (steps_done) *steps_done = step;
+  if (energy_out) *energy_out = cur;
+  return FZ_OK;
+}
+
 extern "C" fz_status fz_set_barostat(fz_system* s, int enable, double pref_atm, double pmass) {
   fz_status r;
   if ((r = need_engine(s))) return r;

@@ -55,6 +55,9 @@ struct Engine {
   int4 *angle = nullptr, *dihe = nullptr, *impr = nullptr;
   float2 *bond_prm = nullptr, *angle_prm = nullptr, *ub_prm = nullptr, *impr_prm = nullptr;
   float4* dihe_prm = nullptr;
+  // minimiser state (allocated on first use): previous force, search direction,
+  // positions before the last move
+  float4 *min_prev_f = nullptr, *min_dir = nullptr, *min_pos = nullptr;
   // integration units, grouped in classes of equal (atoms, constraints)
   int ncls = 0, cls_na[8] = {}, cls_nc[8] = {}, cls_begin[9] = {};
   int4* unit_atoms = nullptr;

@@ -525,6 +525,78 @@ __global__ void __launch_bounds__(128) k_constraint_virial(IntegrateArgs a) {
   energy_add(a.energy + EN_VIR_Z, vir[2]);
 }
 
+// Minimiser move of one unit: ConjugatedGradient / SteepestDescent (src/mdcuda.cu:126-351).
+// Conjugate gradient, per atom as the reference: gamma = |F|^2 / |F_prev|^2 (F_prev = F
+// when |F_prev|^2 < 1e-8), direction H = (F + gamma H_prev) x fac; steepest descent:
+// step F x fac.  Unlike the reference, which moves constrained atoms freely, SHAKE then
+// puts the unit back on its constraints (the old positions as reference vectors), so
+// minimised rigid waters stay rigid.  Velocities are zeroed as in the reference.
+template <int NA, int NC>
+__global__ void __launch_bounds__(128) k_min_step(IntegrateArgs a) {
+  const int u = a.u_begin + blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= a.u_end) return;
+  const Unit U = load_unit<NA, NC>(a, u);
+  const int n = a.p.n;
+  double r0[4][3], rn[4][3], im[4];
+  float q[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    im[k] = 0.0;
+    q[k] = 0.f;
+    for (int c = 0; c < 3; ++c) r0[k][c] = rn[k][c] = 0.0;
+    if (k >= U.na) continue;
+    const int i = U.atom[k];
+    const float4 pr = a.pos4[i];
+    im[k] = a.vel4[i].w;
+    q[k] = pr.w;
+    r0[k][0] = pr.x;
+    r0[k][1] = pr.y;
+    r0[k][2] = pr.z;
+    const double3 F = force_of(a.facc, n, i);
+    a.facc[i] = 0;
+    a.facc[n + i] = 0;
+    a.facc[2 * n + i] = 0;
+    float3 step;
+    if (a.min_method == 1) {
+      float4 f1 = a.min_prev_f[i];
+      const float3 f = make_float3((float)F.x, (float)F.y, (float)F.z);
+      const float ff = f.x * f.x + f.y * f.y + f.z * f.z;
+      float f11 = f1.x * f1.x + f1.y * f1.y + f1.z * f1.z;
+      if (f11 < 1e-8f) f11 = ff;
+      const float gamma = f11 > 0.f ? ff / f11 : 0.f;
+      const float4 h0 = a.min_dir[i];
+      step = make_float3((f.x + h0.x * gamma) * a.min_fac, (f.y + h0.y * gamma) * a.min_fac,
+                         (f.z + h0.z * gamma) * a.min_fac);
+      a.min_dir[i] = make_float4(step.x, step.y, step.z, 0.f);
+      a.min_prev_f[i] = make_float4(f.x, f.y, f.z, 0.f);
+    } else {
+      step = make_float3((float)F.x * a.min_fac, (float)F.y * a.min_fac, (float)F.z * a.min_fac);
+    }
+    rn[k][0] = r0[k][0] + step.x;
+    rn[k][1] = r0[k][1] + step.y;
+    rn[k][2] = r0[k][2] + step.z;
+  }
+  if (U.nc > 0 && shake_unit(U, r0, rn, im, a)) atomicOr(a.status, ST_SHAKE_NOCONV);
+  bool far = false, moved = false;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (k >= U.na) continue;
+    const int i = U.atom[k];
+    const float4 np = make_float4((float)rn[k][0], (float)rn[k][1], (float)rn[k][2], q[k]);
+    a.pos4[i] = np;
+    a.vel4[i] = make_float4(0.f, 0.f, 0.f, (float)im[k]);
+    a.xyzq_s[a.inv_perm[i]] = np;
+    const float4 pb = a.pos_build[i];
+    const float dx = np.x - pb.x, dy = np.y - pb.y, dz = np.z - pb.z;
+    far |= dx * dx + dy * dy + dz * dz > a.p.skin_half2;
+    const float4 pp = a.pos_prune[i];
+    const float ex = np.x - pp.x, ey = np.y - pp.y, ez = np.z - pp.z;
+    moved |= ex * ex + ey * ey + ez * ez > a.prune_half2;
+  }
+  if (far) *a.flag = 1;
+  if (moved) *a.flag_prune = 1;
+}
+
 // ---------------------------------------------------------------- velocity reassignment
 __device__ __forceinline__ uint64_t splitmix64(uint64_t z) {
   z += 0x9E3779B97F4A7C15ULL;
@@ -648,6 +720,12 @@ void launch_kick_rattle(const IntegrateArgs& a, bool kinetic, bool kick, cudaStr
       k_kick_rattle<true, NA, NC><<<unit_grid(x), 128, 0, st>>>(x, kick ? 1 : 0);
     else
       k_kick_rattle<false, NA, NC><<<unit_grid(x), 128, 0, st>>>(x, kick ? 1 : 0);
+  });
+}
+
+void launch_min_step(const IntegrateArgs& a, cudaStream_t st) {
+  for_classes(a, [&](const IntegrateArgs& x, auto na, auto nc) {
+    k_min_step<decltype(na)::value, decltype(nc)::value><<<unit_grid(x), 128, 0, st>>>(x);
   });
 }
 

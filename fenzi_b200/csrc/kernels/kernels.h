@@ -139,6 +139,10 @@ struct IntegrateArgs {
   int ncls;                  // unit classes: units [cls_begin[c], cls_begin[c+1]) have
   int cls_na[8], cls_nc[8];  //   cls_na[c] atoms and cls_nc[c] constraints
   int cls_begin[9];
+  float4* min_prev_f;        // minimiser: previous force and search direction per atom
+  float4* min_dir;
+  int min_method;            //   1 conjugate gradient, 2 steepest descent
+  float min_fac;             //   step factor (A per kcal/mol/A)
   double lam;    // barostat step: centre-of-mass scale of every unit (1 = none)
   double vfric;  // barostat step: centre-of-mass velocity scale of the half kicks (1 = none)
 };
@@ -149,6 +153,8 @@ void launch_kick_drift(const IntegrateArgs& a, cudaStream_t st);
 void launch_kick_drift_npt(const IntegrateArgs& a, cudaStream_t st);
 // barostat step: unit centre-of-mass kinetic energy and intra-unit virial correction
 void launch_unit_virial(const IntegrateArgs& a, cudaStream_t st);
+// one minimiser move of every unit (forces zeroed, constraints re-imposed, list flags)
+void launch_min_step(const IntegrateArgs& a, cudaStream_t st);
 // adds the instantaneous constraint virial of the current positions/velocities/forces
 void launch_constraint_virial(const IntegrateArgs& a, cudaStream_t st);
 // kick (F/2) + RATTLE (+ kinetic energy)

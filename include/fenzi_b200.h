@@ -164,6 +164,13 @@ typedef struct fz_dcd fz_dcd;
 fz_status fz_dcd_open(fz_system* sys, const char* path, int every, fz_dcd** out);
 fz_status fz_dcd_write(fz_dcd* traj);
 fz_status fz_dcd_close(fz_dcd* traj);
+/* MinimizeStep x minimizesteps (src/dynamics.cu:491-620, src/fenzi.cu:397-418):
+ * conjugate-gradient moves (conjgradfac, conjgradrate) until the potential energy
+ * rises, then steepest descent (steepdesfac, steepdesrate) until it rises again, at
+ * most max_steps moves; constraints are kept.  Velocities are zeroed: call
+ * fz_reassign_velocities before dynamics.  Reports the moves made and the final
+ * potential energy (kcal/mol). */
+fz_status fz_minimize(fz_system* sys, int max_steps, int* steps_done, double* energy_out);
 /* Andersen constant-pressure dynamics for the following fz_step calls (the reference's
  * PCONSTANT build: src/cell_based_kernels.cu:566-579 piston acceleration,
  * src/mdcuda.cu:58-88 half kicks; keywords pref/pmass, src/prmread.cu:663-670).
