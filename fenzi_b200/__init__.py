@@ -55,6 +55,8 @@ class Config(C.Structure):
         ("pmass", C.c_double), ("pref", C.c_double), ("shake", C.c_int), ("shake_tol", C.c_double),
         ("hfac", C.c_double), ("printlevel", C.c_int), ("printtostdout", C.c_int), ("keepcheckpoints", C.c_int),
         ("checkpointformat", C.c_char), ("seed", C.c_longlong), ("unknown_keywords", C.c_int),
+        ("consharm", C.c_int), ("consharm_seg", (C.c_char * 64) * 2), ("consharm_dist", C.c_double * 3),
+        ("consharm_fc", C.c_double), ("consfix_nseg", C.c_int), ("consfix_seg", (C.c_char * 64) * 8),
     ]
 
 

@@ -150,6 +150,21 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
   e->seed = (unsigned long long)c.seed;
   e->self_energy = t.self_energy;
   e->ncons = (int)t.cons_d.size();
+  // fixed segments (consfix) and the two restraint segments (consharm), by PSF segment
+  // name, case-insensitive as the reference compares them (src/prmread.cu:365-380)
+  std::vector<char> fixed(n, 0);
+  std::vector<int> rseg(n, -1);
+  for (int i = 0; i < n; ++i) {
+    const std::string& sg = t.seg_names.size() == (size_t)n ? t.seg_names[i] : std::string();
+    for (int j = 0; j < c.consfix_nseg; ++j)
+      if (!cicompare(sg, c.consfix_seg[j])) fixed[i] = 1;
+    if (c.consharm) {
+      if (!cicompare(sg, c.consharm_seg[0])) rseg[i] = 0;
+      else if (!cicompare(sg, c.consharm_seg[1])) rseg[i] = 1;
+    }
+  }
+  e->nfixed = 0;
+  for (int i = 0; i < n; ++i) e->nfixed += fixed[i];
   int dev_sms = 148;
   cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device);
   // pair kernel CTAs per SM: 4 (64-register build, default: 0.614 vs 0.624 ms/step at
@@ -166,7 +181,8 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
   double mt = 0;
   for (int i = 0; i < n; ++i) {
     pos4[i] = make_float4((float)t.pos[3 * i], (float)t.pos[3 * i + 1], (float)t.pos[3 * i + 2], (float)t.q[i]);
-    vel4[i] = make_float4(0.f, 0.f, 0.f, t.mass[i] > 0 ? (float)(1.0 / t.mass[i]) : 0.f);
+    // a fixed atom has inverse mass 0: no kick, drift or minimiser move reaches it
+    vel4[i] = make_float4(0.f, 0.f, 0.f, (t.mass[i] > 0 && !fixed[i]) ? (float)(1.0 / t.mass[i]) : 0.f);
     mt += t.mass[i];
   }
   e->inv_mtot = mt > 0 ? 1.0 / mt : 0.0;
@@ -175,6 +191,23 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
       (r = e->alloc(&e->facc, 3 * (size_t)n)) || (r = e->alloc(&e->energy, fzk::EN_COUNT)) ||
       (r = e->alloc(&e->psum, 4)) || (r = e->upload(&e->type, t.type)))
     return r;
+  if (c.consharm) {
+    double m0 = 0, m1 = 0;
+    for (int i = 0; i < n; ++i) {
+      if (rseg[i] == 0) m0 += t.mass[i];
+      if (rseg[i] == 1) m1 += t.mass[i];
+    }
+    if (!(m0 > 0 && m1 > 0)) return fail(FZ_ERR_ARG, "consharm: a restraint segment has no atoms");
+    e->restraint = true;
+    e->rs_inv_m[0] = 1.0 / m0;
+    e->rs_inv_m[1] = 1.0 / m1;
+    for (int d = 0; d < 3; ++d) e->rs_dist[d] = c.consharm_dist[d];
+    e->rs_fc = c.consharm_fc;
+    std::vector<float> ms(n);
+    for (int i = 0; i < n; ++i) ms[i] = (float)t.mass[i];
+    if ((r = e->upload(&e->rs_seg, rseg)) || (r = e->upload(&e->rs_mass, ms)) || (r = e->alloc(&e->rs_acc, 8)))
+      return r;
+  }
   // ---- sorted slots, columns, tiles
   const int nslots = e->nslots, nblk = nslots / 32, ngrp = nblk * fzk::kNG;
   if ((r = e->alloc(&e->xyzq_s, nslots)) || (r = e->alloc(&e->typ_s, nslots)) || (r = e->alloc(&e->perm, nslots)) ||
@@ -257,9 +290,14 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
   }
   // ---- integration units: free atoms first, then clusters (by size)
   {
+    // clusters whose atoms are all fixed need no constraint solve: free units
     std::vector<int> in_cl(n, 0);
-    for (const auto& cl : t.clusters)
-      for (int k = 0; k < cl.na; ++k) in_cl[cl.atom[k]] = 1;
+    for (const auto& cl : t.clusters) {
+      bool all_fixed = true;
+      for (int k = 0; k < cl.na; ++k) all_fixed = all_fixed && fixed[cl.atom[k]];
+      if (!all_fixed)
+        for (int k = 0; k < cl.na; ++k) in_cl[cl.atom[k]] = 1;
+    }
     std::vector<int4> ua;
     std::vector<int> um;
     std::vector<float4> ud;
@@ -283,7 +321,7 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
     for (int na = 2; na <= 4; ++na)
       for (int nc = 1; nc <= 3; ++nc)
         for (const auto& cl : t.clusters) {
-          if (cl.na != na || cl.nc != nc) continue;
+          if (cl.na != na || cl.nc != nc || !in_cl[cl.atom[0]]) continue;
           open_class(na, nc);
           ua.push_back(make_int4(cl.atom[0], cl.atom[1], cl.atom[2], cl.atom[3]));
           int meta = cl.na | (cl.nc << 4);
@@ -610,7 +648,8 @@ extern "C" fz_status fz_eval_props(fz_system* s, fz_energies* out) {
   out->potential = out->bond + out->angle + out->ureyb + out->dihed + out->impr + out->vdw + out->elec + out->pme +
                    out->ewexcl + out->ewself;
   out->kinetic = en[fzk::EN_KIN] * s_;
-  const double dof = 3.0 * e->n - 6.0 - e->ncons;  // src/evalprops.cu:225
+  // src/evalprops.cu:225 (with consfix: the atoms outside fixed segments, :223)
+  const double dof = 3.0 * (e->n - e->nfixed) - 6.0 - e->ncons;
   out->temperature = dof > 0 ? 2.0 * out->kinetic / (kRC * dof) : 0.0;
   out->virial[0] = en[fzk::EN_VIR_X] * s_;
   out->virial[1] = en[fzk::EN_VIR_Y] * s_;

@@ -55,6 +55,14 @@ struct Engine {
   int4 *angle = nullptr, *dihe = nullptr, *impr = nullptr;
   float2 *bond_prm = nullptr, *angle_prm = nullptr, *ub_prm = nullptr, *impr_prm = nullptr;
   float4* dihe_prm = nullptr;
+  int nfixed = 0;  // atoms of fixed (consfix) segments
+  // consharm restraint: segment of every atom (0, 1, -1), masses, fixed-point mass
+  // centre sums (x0 y0 z0 x1 y1 z1), inverse segment masses, target offset, constant
+  bool restraint = false;
+  int* rs_seg = nullptr;
+  float* rs_mass = nullptr;
+  long long* rs_acc = nullptr;
+  double rs_inv_m[2] = {0, 0}, rs_dist[3] = {0, 0, 0}, rs_fc = 0;
   // minimiser state (allocated on first use): previous force, search direction,
   // positions before the last move
   float4 *min_prev_f = nullptr, *min_dir = nullptr, *min_pos = nullptr;
@@ -356,6 +364,7 @@ struct Engine {
       fzk::launch_bonded(bonded_args(), energies, st);
       launches += (nbond + nangle + nub + ndihe + nimpr + nexcl + n14 > 0) ? 1 : 0;
     }
+    if ((terms & FZ_TERM_BONDED) && restraint) restraint_forces(st);
     mark(4);
     if (terms & FZ_TERM_PME) {
       fzk::launch_pme(pme_args(), energies, st);
@@ -377,6 +386,11 @@ struct Engine {
     stage_ms[3] += el(4, 5);
     stage_ms[4] += el(0, 1) + el(5, 6);
     timed_steps++;
+  }
+  // consharm: mass centres of the two segments, then the pull on segment 1's atoms
+  void restraint_forces(cudaStream_t s) {
+    cudaMemsetAsync(rs_acc, 0, 8 * sizeof(long long), s);
+    fzk::launch_restraint(p, pos4, rs_seg, rs_mass, rs_acc, rs_inv_m[0], rs_inv_m[1], rs_dist, rs_fc, facc, s);
   }
   // Adds to the capture on st an IF node that runs body(stream) when *dflag != 0.
   template <class F>
@@ -447,6 +461,7 @@ struct Engine {
     fzk::launch_pme(pme_args(), false, st2);
     fzk::launch_nonbonded(nb_args(), false, st);
     fzk::launch_bonded(bonded_args(), false, st);
+    if (restraint) restraint_forces(st);
     cudaEventRecord(ev_join, st2);
     cudaStreamWaitEvent(st, ev_join, 0);
   }

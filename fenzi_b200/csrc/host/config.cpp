@@ -1,5 +1,6 @@
 // .in run-file parser: the keyword set of ReadInput (src/prmread.cu:491-913),
 // case-insensitive, '#' comments, defaults from src/globals.cu:28-593.
+#include <algorithm>
 #include <cctype>
 #include <cstdio>
 #include <cstdlib>
@@ -33,8 +34,8 @@ std::string join_dir(const std::string& base_file, const std::string& rel) {
   return base_file.substr(0, p + 1) + rel;
 }
 
-static void copy_str(char* dst, const std::string& s) {
-  std::snprintf(dst, 512, "%s", s.c_str());
+static void copy_str(char* dst, const std::string& s, size_t cap = 512) {
+  std::snprintf(dst, cap, "%s", s.c_str());
 }
 
 }  // namespace fz
@@ -126,9 +127,18 @@ extern "C" fz_status fz_read_input(const char* in_path, fz_config* c) {
     else if (!cicompare(key, "pmegridsizez")) c->pme_grid[2] = (int)num();
     else if (!cicompare(key, "pmass")) c->pmass = num();
     else if (!cicompare(key, "pref")) c->pref = num();
-    else if (!cicompare(key, "consharm") || !cicompare(key, "consharmdist") || !cicompare(key, "consharmfc") ||
-             !cicompare(key, "consfix")) {
-      // restraints / fixed segments: parsed, not part of this build's step
+    else if (!cicompare(key, "consharm")) {
+      c->consharm = 1;
+      copy_str(c->consharm_seg[0], str(), sizeof c->consharm_seg[0]);
+      copy_str(c->consharm_seg[1], str(), sizeof c->consharm_seg[1]);
+    } else if (!cicompare(key, "consharmdist")) {
+      for (int d = 0; d < 3; ++d) c->consharm_dist[d] = num();
+    } else if (!cicompare(key, "consharmfc")) {
+      c->consharm_fc = num();
+    } else if (!cicompare(key, "consfix")) {
+      const int k = (int)num();
+      c->consfix_nseg = std::max(0, std::min(8, k));
+      for (int j = 0; j < c->consfix_nseg; ++j) copy_str(c->consfix_seg[j], str(), sizeof c->consfix_seg[j]);
     } else if (!cicompare(key, "shake")) {
       const std::string v = str();
       if (!cicompare(v, "on")) c->shake = 1;

@@ -253,4 +253,58 @@ void launch_bonded(const BondedArgs& a, bool energy, cudaStream_t st) {
     k_bonded<false><<<g, 256, 0, st>>>(a);
 }
 
+// ---------------------------------------------------------------- consharm restraint
+constexpr double kFixCom = 16777216.0;  // mass-centre sums, 2^24 per amu A
+
+// positions wrapped into [-L/2, L/2) (the reference's primary box), mass-weighted sums
+// per segment in fixed point (order independent)
+__global__ void __launch_bounds__(256) k_restraint_com(SysParams p, const float4* __restrict__ pos4,
+                                                       const int* __restrict__ seg, const float* __restrict__ mass,
+                                                       long long* acc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double w[6] = {0, 0, 0, 0, 0, 0};
+  if (i < p.n) {
+    const int sg = seg[i];
+    if (sg >= 0) {
+      const float4 r = pos4[i];
+      const double m = mass[i];
+      const double x = r.x - p.box.x * floorf(r.x * p.inv_box.x + 0.5f);
+      const double y = r.y - p.box.y * floorf(r.y * p.inv_box.y + 0.5f);
+      const double z = r.z - p.box.z * floorf(r.z * p.inv_box.z + 0.5f);
+      w[3 * sg] = m * x;
+      w[3 * sg + 1] = m * y;
+      w[3 * sg + 2] = m * z;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    long long v = __double2ll_rn(w[k] * kFixCom);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v != 0) red_add(acc + k, v);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_restraint_force(int n, const int* __restrict__ seg,
+                                                         const long long* __restrict__ acc, double inv_m0,
+                                                         double inv_m1, double dx, double dy, double dz, double fc,
+                                                         long long* facc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || seg[i] != 1) return;
+  const double s = 1.0 / kFixCom;
+  const double fx = fc * (dx + acc[0] * s * inv_m0 - acc[3] * s * inv_m1);
+  const double fy = fc * (dy + acc[1] * s * inv_m0 - acc[4] * s * inv_m1);
+  const double fz = fc * (dz + acc[2] * s * inv_m0 - acc[5] * s * inv_m1);
+  red_add(facc + i, to_fix_d(fx));
+  red_add(facc + n + i, to_fix_d(fy));
+  red_add(facc + 2 * n + i, to_fix_d(fz));
+}
+
+void launch_restraint(const SysParams& p, const float4* pos4, const int* seg, const float* mass, long long* acc,
+                      double inv_m0, double inv_m1, const double* dist, double fc, long long* facc, cudaStream_t st) {
+  const int g = (p.n + 255) / 256;
+  k_restraint_com<<<g, 256, 0, st>>>(p, pos4, seg, mass, acc);
+  k_restraint_force<<<g, 256, 0, st>>>(p.n, seg, acc, inv_m0, inv_m1, dist[0], dist[1], dist[2], fc, facc);
+}
+
 }  // namespace fzk

@@ -572,6 +572,7 @@ __global__ void __launch_bounds__(128) k_min_step(IntegrateArgs a) {
     } else {
       step = make_float3((float)F.x * a.min_fac, (float)F.y * a.min_fac, (float)F.z * a.min_fac);
     }
+    if (im[k] == 0.0) step = make_float3(0.f, 0.f, 0.f);  // fixed (consfix) atom
     rn[k][0] = r0[k][0] + step.x;
     rn[k][1] = r0[k][1] + step.y;
     rn[k][2] = r0[k][2] + step.z;

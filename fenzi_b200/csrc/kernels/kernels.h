@@ -164,6 +164,11 @@ void launch_kinetic(const IntegrateArgs& a, cudaStream_t st);
 void launch_reassign(const IntegrateArgs& a, double T, uint64_t seed, uint32_t counter, double inv_mtot,
                      long long* psum, cudaStream_t st);
 
+// consharm restraint (src/mdcuda.cu:481-516, src/cell_based_kernels.cu:715-877): every
+// atom of segment 1 gets fc (dist + R0 - R1), R the segments' mass centres
+void launch_restraint(const SysParams& p, const float4* pos4, const int* seg, const float* mass, long long* acc,
+                      double inv_m0, double inv_m1, const double* dist, double fc, long long* facc, cudaStream_t st);
+
 double measure_fp32_peak(int device);
 
 }  // namespace fzk

@@ -71,6 +71,15 @@ typedef struct fz_config {
   char checkpointformat;     /* 'a' ascii, 'b' binary, 0 unset */
   long long seed;
   int unknown_keywords;      /* count of unrecognised lines (the reference warns) */
+  /* restraints (src/prmread.cu:674-690): the mass centre of segment consharm_seg[1]
+   * pulled towards that of consharm_seg[0] + consharm_dist with consharm_fc */
+  int consharm;
+  char consharm_seg[2][64];
+  double consharm_dist[3];
+  double consharm_fc;
+  /* fixed segments (consfix, src/prmread.cu:697-723): their atoms never move */
+  int consfix_nseg;
+  char consfix_seg[8][64];
 } fz_config;
 
 /* Energies, the EvalProps table (src/evalprops.cu:248-308), kcal/mol, FP64. */
