@@ -57,11 +57,11 @@ def args_():
                          "(relaxes the seeded lattice start; untimed, before the warm-up)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ensemble", type=int, default=256,
-                    help="batched-ensemble measurement (BASELINE configs[2]) with this many boxes; 0 skips it")
+                    help="batched-ensemble measurement (256 uneven TIP3P boxes of 648-6,000 atoms) with this many boxes; 0 skips it")
     ap.add_argument("--served", type=int, default=32,
-                    help="served-job measurement (BASELINE configs[3]) with this many jobs; 0 skips it")
+                    help="served-job measurement (Poisson arrivals of 1.5k-30k-atom jobs) with this many jobs; 0 skips it")
     ap.add_argument("--precision", type=int, default=100000,
-                    help="precision study (BASELINE configs[4]): NVE steps of the 17,280-atom system; 0 skips it")
+                    help="precision study: NVE steps of the 17,280-atom system, then NPT; 0 skips it")
     ap.add_argument("--profile", action="store_true",
                     help="only run warm-up + steps (no timing/report): a clean target for ncu")
     return ap.parse_args()
@@ -516,7 +516,7 @@ def main():
                 "work": f"{FLOP_PER_PAIR} FLOP x {pairs} non-excluded pairs within rc per launch",
                 "peak_source": "measured FP32 FMA microbenchmark (fz_measure_fp32_peak); "
                                "MEASURED_PEAKS.json has no FP32 figure"}
-        # whole-step roofline (SURVEY 8d): T_ideal = W_nb/P_fp32 + (B_pme + B_int)/BW_hbm
+        # whole-step roofline: T_ideal = W_nb/P_fp32 + (B_pme + B_int)/BW_hbm
         hbm = None
         try:
             hbm = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]

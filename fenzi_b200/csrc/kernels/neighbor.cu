@@ -373,7 +373,14 @@ __global__ void __launch_bounds__(256, 6) k_prune(SysParams p, const int* __rest
   const float4 pi = xyzq_s[islot];
   const int ia = perm[islot];
   if (ia >= 0) pos_prune[ia] = pi;
-  ipos[lane] = pi;
+  // distances are taken about the block's first atom o (slot 0 of a block is always
+  // an atom): |r - q|^2 = |r - o|^2 + (|q - o|^2 - 2 (q - o).(r - o)), so each (i, j)
+  // test is three FMAs and a min on (-2(q - o), |q - o|^2) held in shared memory
+  const float4 o = xyzq_s[I * 32];
+  {
+    const float qx = pi.x - o.x, qy = pi.y - o.y, qz = pi.z - o.z;
+    ipos[lane] = make_float4(-2.f * qx, -2.f * qy, -2.f * qz, fmaf(qx, qx, fmaf(qy, qy, qz * qz)));
+  }
   // diagonal tile mask (exclusions inside the block)
   dmask[islot] = excl_mask(I, (uint32_t)islot, lane, msk, xn, xs, xmax);
   const uint32_t dummy = (uint32_t)(p.nslots - 1) | ((uint32_t)kNoShift << kSlotBits);
@@ -411,6 +418,7 @@ __global__ void __launch_bounds__(256, 6) k_prune(SysParams p, const int* __rest
   };
   // the next chunk's entries and positions are loaded before this chunk's distance
   // tests, so the gathers overlap the arithmetic
+  const float rp2_keep = rp2 + 1e-3f;
   uint32_t e_nx = lane < n ? src[lane] : dummy;
   float4 r_nx = xyzq_s[e_nx & kSlotMask];
   for (int c0 = 0; c0 < n; c0 += 32) {
@@ -428,19 +436,24 @@ __global__ void __launch_bounds__(256, 6) k_prune(SysParams p, const int* __rest
       r.y += sh.y;
       r.z += sh.z;
     }
+    r.x -= o.x;
+    r.y -= o.y;
+    r.z -= o.z;
+    const float rr = fmaf(r.x, r.x, fmaf(r.y, r.y, r.z * r.z));
     float m2[kNG];
 #pragma unroll
     for (int s = 0; s < kNG; ++s) m2[s] = 3e38f;
 #pragma unroll
     for (int k = 0; k < 32; ++k) {
       const float4 q = ipos[k];
-      const float dx = r.x - q.x, dy = r.y - q.y, dz = r.z - q.z;
-      m2[k / kIG] = fminf(m2[k / kIG], fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+      m2[k / kIG] = fminf(m2[k / kIG], fmaf(q.x, r.x, fmaf(q.y, r.y, fmaf(q.z, r.z, q.w))));
     }
 #pragma unroll
     for (int s = 0; s < kNG; ++s) {
       uint32_t* buf = buf_all[warp][s];
-      const bool keep = valid && m2[s] < rp2;
+      // rp2_keep exceeds (rc + delta)^2 by far more than the rounding of the expanded
+      // form (|r - o| <= ~20 A), so no entry the exact test keeps is dropped
+      const bool keep = valid && m2[s] + rr < rp2_keep;
       const unsigned b = __ballot_sync(0xffffffffu, keep);
       if (keep) buf[count[s] + __popc(b & ((1u << lane) - 1u))] = e;
       __syncwarp();

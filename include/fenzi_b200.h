@@ -228,7 +228,7 @@ fz_status fz_measure_fp32_peak(int device, double* tflops);
  * on the shared scratch and must be serialised by the caller. */
 fz_status fz_pme_reciprocal_static(int device, void* stream, const float* pos4, int n, const double* box,
                                    const int* K, double beta, long long* facc, double* energy_out);
-/* ---- batched ensemble --------------------------- */
+/* ---- batched ensemble ------------------------------------------------- */
 /* Independent uploaded systems (same device) advanced together: one MD step of every
  * system is one CUDA-graph launch whose branches are the systems' steps, so small
  * systems run concurrently on the GPU.  The batch does not own the systems; positions,
