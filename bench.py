@@ -189,6 +189,7 @@ def bench_ensemble(nsys, device, steps=30, dist=None):
         sy.SingleStep(seq_steps)
     torch.cuda.synchronize()
     ts = (time.perf_counter() - t0) / seq_steps
+    plain_rate, plain_atoms, plain_boxes = plain_one_at_a_time(systems, device)
     batch.close()
     for sy in systems:
         sy.close()
@@ -196,10 +197,61 @@ def bench_ensemble(nsys, device, steps=30, dist=None):
             "systems": nsys, "atoms": natoms, "ms_per_batched_step": tb * 1e3,
             "sequential_atom_steps_per_s": natoms / ts, "ms_per_sequential_sweep": ts * 1e3,
             "speedup_vs_one_at_a_time": ts / tb,
+            "plain_one_at_a_time_atom_steps_per_s": plain_rate,
+            "speedup_vs_plain_one_at_a_time": natoms / tb / plain_rate,
+            "plain_sample": f"{plain_boxes} of the {len(systems)} boxes (every 4th, {plain_atoms} atoms), each on "
+                            f"its own plain-path engine from its current state, 3 warm-up + 10 timed steps",
             "workload": f"{nsys} TIP3P boxes, 216-2000 waters each at 0.0334/A^3, grids 16^3-36^3 (smallest "
                         f"2^a3^b5^c >= L/1.2), rc 9 / ron 7.5, beta 0.34, SHAKE, NVE, 1 fs; seeded",
             "timing": "wall clock over 30 batched steps vs 10-step sweeps of the boxes one at a time, device "
                       "synchronised around each; working set > L2"}
+
+
+def plain_one_at_a_time(systems, device, every=4, steps=10, warm=3):
+    """Boxes one at a time on the plain path (every `every`-th box), each on its own
+    engine started from the box's current state.  The plain step synchronises with the
+    host every step, so each box is timed by wall clock.  Returns (atom-steps/s of the
+    sample run one after another, atoms in the sample, boxes in the sample)."""
+    from fenzi_b200.plain import Plain
+    atoms, secs, nb = 0, 0.0, 0
+    for sy in systems[::every]:
+        p = Plain(sy, device)
+        p.set_positions(sy.positions())
+        p.set_velocities(sy.velocities())
+        p.SingleStep(warm)
+        t0 = time.perf_counter()
+        p.SingleStep(steps)
+        secs += (time.perf_counter() - t0) / steps
+        atoms += sy.n
+        nb += 1
+        p.close()
+    return atoms / secs, atoms, nb
+
+
+def bench_plain_single(sysm, device, t_ideal_s, ms_ours, steps=60, warm=10):
+    """The 230,400-atom system on the plain path (FP32, the reference's method) from the
+    product path's current state: wall clock per step (it synchronises with the host
+    every step), its fraction of the step roofline, and the product path's speed-up."""
+    from fenzi_b200.plain import Plain
+    p = Plain(sysm, device, fp64=False)
+    p.set_positions(sysm.positions())
+    p.set_velocities(sysm.velocities())
+    p.SingleStep(warm)
+    c0 = p.counters()
+    t0 = time.perf_counter()
+    p.SingleStep(steps)
+    sec = (time.perf_counter() - t0) / steps
+    c1 = p.counters()
+    p.close()
+    return {"method": "plain path, FP32: cell list + per-atom full neighbour list (no Newton-3), thread-per-atom "
+                      "nonbonded, per-grid-point atom lists + gather-style spread, complex cuFFT, thread-per-atom "
+                      "gather, one launch per stage, host synchronisation every step",
+            "ms_per_step": sec * 1e3, "ns_per_day": 86.4 * sysm.cfg.timestep_ps * 1e3 / (sec * 1e3),
+            "atom_steps_per_s": sysm.n / sec, "step_roofline_frac": t_ideal_s / sec,
+            "product_speedup": sec * 1e3 / ms_ours,
+            "rebuilds_in_timed_steps": c1["rebuilds"] - c0["rebuilds"],
+            "launches_per_step": (c1["launches"] - c0["launches"]) / steps,
+            "list_entries": c1["list_entries"], "timing": f"wall clock over {steps} steps after {warm} warm-up"}
 
 
 def served_jobs(njobs, seed):
@@ -300,11 +352,49 @@ def bench_served(device, njobs=32, seed=4242, check=4):
                       "server's steady clock"}
 
 
-def bench_precision(device, nve_steps=100000, npt_steps=2000):
+def drift_fit(t_ns, etot, natom):
+    """Least-squares slope of the total energy (kcal/mol/ns/atom) and its standard error."""
+    t, e = np.asarray(t_ns, float), np.asarray(etot, float)
+    if len(t) < 2:
+        return 0.0, None
+    if len(t) < 4:
+        return float(np.polyfit(t, e, 1)[0]) / natom, None
+    c, cov = np.polyfit(t, e, 1, cov=True)
+    return float(c[0]) / natom, float(np.sqrt(cov[0, 0])) / natom
+
+
+def plain_fp64_drift(s, device, pos0, vel0, nsteps, chunk):
+    """NVE energy drift of the all-FP64 GPU variant (the plain path with every quantity
+    in FP64) from the given state: total energy every `chunk` steps, slope per ns per atom."""
+    from fenzi_b200.plain import Plain
+    p = Plain(s, device, fp64=True)
+    p.set_positions(pos0)
+    p.set_velocities(vel0)
+    t, tot = [], []
+    t0 = time.perf_counter()
+    for k in range(nsteps // chunk + 1):
+        if k:
+            p.SingleStep(chunk)
+        e = p.EvalProps()
+        t.append(k * chunk * s.cfg.timestep_ps * 1e-3)
+        tot.append(e["potential"] + e["kinetic"])
+    wall = time.perf_counter() - t0
+    p.close()
+    slope, err = drift_fit(t, tot, s.n)
+    return {"method": "plain path in FP64 (positions, velocities, forces, PME mesh and FFT, SHAKE/RATTLE)",
+            "nve_steps": nsteps, "nve_wall_s": wall, "nve_drift_kcal_per_mol_per_ns_per_atom": slope,
+            "nve_drift_stderr": err,
+            "nve_total_energy_std_kcal_per_mol": float(np.std(tot)), "t_ns": t}
+
+
+def bench_precision(device, nve_steps=100000, npt_steps=2000, fp64_steps=20000):
     """The 17,280-atom precision study: NVE energy drift per ns per atom over nve_steps
     (after 2,000 thermalised steps), total-force error against the FP64 oracle, run-to-
-    run bit-equality of the int64 force buffer (SHA-256 of two evaluations), then an
-    Andersen leg of npt_steps at 1 atm (conserved-quantity excursion, volume change)."""
+    run bit-equality of the int64 force buffer (SHA-256 of two evaluations), the drift
+    of the all-FP64 GPU variant over fp64_steps from the same state (the product path's
+    drift over the same span beside it), then an Andersen leg of npt_steps at 1 atm
+    (conserved-quantity excursion, volume change).  Drifts are least-squares slopes of
+    the total energy sampled every 1,000 steps, with their standard errors."""
     import hashlib
     import fenzi_b200 as fz
     from fenzi_b200 import gen_system
@@ -318,6 +408,7 @@ def bench_precision(device, nve_steps=100000, npt_steps=2000):
         s.SingleStep(100)
         s.InitVelocity(T=300.0, seed=2345, counter=k + 1)
     s.SingleStep(100)
+    pos0, vel0 = s.positions(), s.velocities()
     chunk = 1000
     t, tot = [], []
     t0 = time.perf_counter()
@@ -328,7 +419,11 @@ def bench_precision(device, nve_steps=100000, npt_steps=2000):
         t.append(k * chunk * s.cfg.timestep_ps * 1e-3)  # ns
         tot.append(e["potential"] + e["kinetic"])
     wall = time.perf_counter() - t0
-    slope = float(np.polyfit(np.array(t), np.array(tot), 1)[0])  # kcal/mol/ns
+    slope, slope_err = drift_fit(t, tot, s.n)
+    # the all-FP64 GPU variant (plain path, FP64 throughout) from the same state
+    fp64 = plain_fp64_drift(s, device, pos0, vel0, min(nve_steps, fp64_steps), chunk)
+    nspan = len(fp64["t_ns"])
+    slope_same, slope_same_err = drift_fit(t[:nspan], tot[:nspan], s.n)
     s.ComputeAccelGPU()
     a = s.forces_fixed()
     s.ComputeAccelGPU()
@@ -347,12 +442,14 @@ def bench_precision(device, nve_steps=100000, npt_steps=2000):
     out = {"workload": "chain17k: 5,360 TIP3P + 40 x 30-atom chains = 17,280 atoms, 56 A, 64^3, beta 0.34, rc 10, "
                        "SHAKE, 1 fs",
            "nve_steps": nve_steps, "nve_wall_s": wall,
-           "nve_drift_kcal_per_mol_per_ns_per_atom": slope / s.n,
+           "nve_drift_kcal_per_mol_per_ns_per_atom": slope, "nve_drift_stderr": slope_err,
            "nve_total_energy_std_kcal_per_mol": float(np.std(tot)),
            "force_rel_rms_vs_fp64_oracle": err,
            "force_sha256": [hashlib.sha256(a.tobytes()).hexdigest()[:16], hashlib.sha256(b.tobytes()).hexdigest()[:16]],
            "forces_bit_reproducible": bool(np.array_equal(a, b)),
-           "all_fp64_gpu_variant": None,
+           "nve_drift_same_span_kcal_per_mol_per_ns_per_atom": slope_same,
+           "nve_drift_same_span_stderr": slope_same_err,
+           "all_fp64_gpu_variant": {k: v for k, v in fp64.items() if k != "t_ns"},
            "npt": {"steps": npt_steps, "pref_atm": 1.0, "pmass": 1e-5,
                    "conserved_max_excursion_kcal_per_mol": float(np.abs(hs).max()),
                    "kinetic_kcal_per_mol": e0["kinetic"], "volume_change_max": float(np.abs(vs).max()),
@@ -530,6 +627,7 @@ def main():
             per, cores = cpu_baseline(path, 4)
             cpu = {"value": 86.4 * dt_fs / (per * 1e3), "unit": "ns/day", "cores": cores, "kind": "port",
                    "sample": "4 full MD steps of the 230,400-atom system (FP64 oracle, OpenMP, all host threads)"}
+        plain = bench_plain_single(sysm, local, t_ideal, ms_step) if world == 1 else None
         batched = batched_multi
         if a.ensemble > 0 and world == 1:
             batched = bench_ensemble(a.ensemble, local)
@@ -554,7 +652,7 @@ def main():
                 "pair_slots": sysm.counters()["pair_slots"],
                 "prunes_total": sysm.counters()["prunes"],
                 "pair_slot_efficiency": pairs / float(sysm.counters()["pair_slots"]),
-                "roofline": roof, "cpu_baseline": cpu,
+                "roofline": roof, "cpu_baseline": cpu, "plain_path": plain,
                 "e2e": {"value": e2e_nsd, "unit": "ns/day", "h2d_bytes_per_step": 24 * natom / a.chunk,
                         "d2h_bytes_per_step": 24 * natom / a.chunk, "h2d_bytes_per_call": 24 * natom,
                         "d2h_bytes_per_call": 24 * natom,

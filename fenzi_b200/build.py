@@ -1,4 +1,6 @@
-"""Builds the in-tree CUDA library fenzi_b200/libfenzi_b200.so for sm_100a.
+"""Builds the in-tree CUDA libraries for sm_100a: fenzi_b200/libfenzi_b200.so (the
+product) and fenzi_b200/libfenzi_plain.so (the plain comparator path, which links
+the product library and cuFFT).
 
 Usage: python -m fenzi_b200.build   (or fenzi_b200.build.build())
 """
@@ -12,6 +14,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libfenzi_b200.so")
+PLAIN_LIB = os.path.join(HERE, "libfenzi_plain.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -21,29 +24,30 @@ def sources():
                   + glob.glob(os.path.join(c, "host", "*.cpp")))
 
 
+def plain_sources():
+    return sorted(glob.glob(os.path.join(HERE, "csrc", "plain", "*.cu")))
+
+
 def headers():
     c = os.path.join(HERE, "csrc")
     return (glob.glob(os.path.join(c, "**", "*.h"), recursive=True)
             + glob.glob(os.path.join(c, "**", "*.cuh"), recursive=True)
-            + [os.path.join(ROOT, "include", "fenzi_b200.h")])
+            + glob.glob(os.path.join(ROOT, "include", "*.h")))
 
 
-def up_to_date():
-    if not os.path.exists(LIB):
+def up_to_date(lib=LIB, srcs=None):
+    if not os.path.exists(lib):
         return False
-    t = os.path.getmtime(LIB)
-    return all(os.path.getmtime(f) <= t for f in sources() + headers())
+    t = os.path.getmtime(lib)
+    return all(os.path.getmtime(f) <= t for f in (srcs or sources()) + headers())
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and up_to_date():
-        return LIB
+def _compile(srcs, objdir, verbose):
     nvcc = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
-    objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
     objs = []
     procs = []
-    for src in sources():
+    for src in srcs:
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
         objs.append(obj)
         cmd = [nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-O3",
@@ -59,7 +63,17 @@ def build(force: bool = False, verbose: bool = False) -> str:
         failed |= p.returncode != 0
     if failed:
         raise RuntimeError("nvcc failed")
-    subprocess.check_call([nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"])
+    return nvcc, objs
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if force or not up_to_date():
+        nvcc, objs = _compile(sources(), os.path.join(HERE, "_build"), verbose)
+        subprocess.check_call([nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"])
+    if force or not up_to_date(PLAIN_LIB, plain_sources()) or os.path.getmtime(PLAIN_LIB) < os.path.getmtime(LIB):
+        nvcc, objs = _compile(plain_sources(), os.path.join(HERE, "_build", "plain"), verbose)
+        subprocess.check_call([nvcc, *ARCH, "-shared", "-o", PLAIN_LIB, *objs, "-L", HERE, "-lfenzi_b200", "-lcufft",
+                               "-lcudart", "-Xlinker", "-rpath,$ORIGIN", "-Xlinker", "-rpath,/usr/local/cuda/lib64"])
     return LIB
 
 

@@ -54,3 +54,29 @@ def test_server_without_gpu_fails_cleanly():
         pytest.skip("a CUDA device is present")
     assert code in (3, 6)  # FZ_ERR_CUDA / FZ_ERR_ARG
     assert fz.last_error()
+
+
+def test_plain_header_symbols_exported():
+    """libfenzi_plain.so (the comparator path) exports every symbol of fenzi_plain.h."""
+    from fenzi_b200 import plain
+    txt = open(os.path.join(os.path.dirname(HDR), "fenzi_plain.h")).read()
+    names = sorted(set(re.findall(r"^\s*fz_status\s+(fz_plain_\w+)\s*\(", txt, re.M)))
+    assert len(names) == 10
+    L = plain.plib()
+    for n in names:
+        assert hasattr(L, n), n
+    assert set(names) == set(plain.PLAIN_EXPORTS)
+
+
+def test_plain_without_gpu_fails_cleanly():
+    from tests.helpers import system
+    from fenzi_b200.plain import Plain
+    _, path = system("tiny")
+    s = fz.FenZi.ReadInput(path).LoadSystem()
+    try:
+        p = Plain(s, 0)
+    except fz.FenZiError as e:
+        assert e.code == 3 and fz.last_error()
+        return
+    p.close()
+    pytest.skip("a CUDA device is present")
