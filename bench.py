@@ -276,8 +276,8 @@ def bench_served(device, njobs=32, seed=4242, check=4):
     """Served jobs through the serving loop (fz_server): each job is submitted at its
     Poisson arrival time, admitted by the 150 GB HBM budget, advanced with the running
     mix in the batch graph; latency = completion - submission on the server clock.
-    The one-at-a-time comparison times 200 steps of each job alone (its own CUDA graph)
-    and scales to the job's step count."""
+    The one-at-a-time comparisons time 200 steps of each job alone (its own CUDA graph)
+    and 30 steps of it alone on the plain path, each scaled to the job's step count."""
     import torch
     import fenzi_b200 as fz
     from fenzi_b200 import gen_system
@@ -298,7 +298,8 @@ def bench_served(device, njobs=32, seed=4242, check=4):
         return s.LoadSystem()
 
     # one at a time: 200 steps of each job alone, scaled to its length
-    seq_s, natoms = 0.0, []
+    from fenzi_b200.plain import Plain
+    seq_s, plain_s, natoms = 0.0, 0.0, []
     for i, j in enumerate(jobs):
         s = load(i)
         s.InitMem(device)
@@ -310,6 +311,15 @@ def bench_served(device, njobs=32, seed=4242, check=4):
         torch.cuda.synchronize()
         seq_s += (time.perf_counter() - t0) / 200 * j["steps"]
         natoms.append(s.n)
+        # the same job alone on the plain path (its own engine, from the same state)
+        pl = Plain(s, device)
+        pl.set_positions(s.positions())
+        pl.set_velocities(s.velocities())
+        pl.SingleStep(5)
+        t0 = time.perf_counter()
+        pl.SingleStep(30)
+        plain_s += (time.perf_counter() - t0) / 30 * j["steps"]
+        pl.close()
         s.close()
     systems = [load(i) for i in range(len(jobs))]
     total = sum(n * j["steps"] for n, j in zip(natoms, jobs))
@@ -343,6 +353,7 @@ def bench_served(device, njobs=32, seed=4242, check=4):
             "p99_s": float(np.percentile(lat, 99)), "unit": "s", "jobs": len(jobs),
             "aggregate_atom_steps_per_s": total / wall, "makespan_s": wall,
             "one_at_a_time_atom_steps_per_s": total / seq_s, "speedup_vs_one_at_a_time": seq_s / wall,
+            "plain_one_at_a_time_atom_steps_per_s": total / plain_s, "speedup_vs_plain_one_at_a_time": plain_s / wall,
             "peak_running_jobs": stats["peak_running"],
             "final_frame_force_rel_rms_vs_oracle": {"max": max(errs), "jobs_checked": len(errs)},
             "workload": f"{len(jobs)} jobs of a Poisson(200/s) stream (seed {seed}): 1.5k-30k atoms, 0-40 30-atom "
