@@ -96,7 +96,11 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
   if (rc >= 0.5 * lmin) return fail(FZ_ERR_ARG, "cutoff must be below half the smallest box edge");
   const double V = c.box[0] * c.box[1] * c.box[2];
   const double rho = n / V;
-  const double a = std::cbrt(32.0 / rho);
+  // column cross-section: a x a with a^3 holding `col_atoms` atoms (32: one sorted
+  // block is a near-cube; smaller values make narrower, taller blocks)
+  double col_atoms = 32.0;
+  if (const char* v = std::getenv("FZ_COL_ATOMS")) col_atoms = std::min(64.0, std::max(8.0, std::atof(v)));
+  const double a = std::cbrt(col_atoms / rho);
   int ncx = std::max(1, (int)std::floor(c.box[0] / a)), ncy = std::max(1, (int)std::floor(c.box[1] / a));
   while ((double)n / (ncx * ncy) > fzk::kColCap / 2 && (ncx < 4096 && ncy < 4096)) {
     ncx *= 2;
@@ -318,10 +322,51 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
         um.push_back(1);
         ud.push_back(make_float4(0.f, 0.f, 0.f, 0.f));
       }
+    // SETTLE applies to (3 atoms, 3 constraints) clusters that are symmetric triangles:
+    // an apex bonded to two base atoms of equal mass at equal lengths; those are stored
+    // apex first with constraints (0,1), (0,2), (1,2)
+    auto as_triangle = [&](const Cluster& cl, Cluster& out) {
+      if (cl.na != 3 || cl.nc != 3) return false;
+      for (int base = 0; base < 3; ++base) {  // constraint `base` joins the two base atoms
+        const int b = cl.ca[base], c = cl.cb[base], ap = 3 - b - c;
+        if (ap < 0 || ap > 2 || b == c) continue;
+        double dab = -1, dac = -1;
+        for (int k = 0; k < 3; ++k) {
+          if ((cl.ca[k] == ap && cl.cb[k] == b) || (cl.ca[k] == b && cl.cb[k] == ap)) dab = cl.d[k];
+          if ((cl.ca[k] == ap && cl.cb[k] == c) || (cl.ca[k] == c && cl.cb[k] == ap)) dac = cl.d[k];
+        }
+        const double mb = t.mass[cl.atom[b]], mc = t.mass[cl.atom[c]];
+        if (dab <= 0 || dac <= 0 || (float)dab != (float)dac || mb != mc || mb <= 0 || t.mass[cl.atom[ap]] <= 0)
+          continue;
+        if (fixed[cl.atom[ap]] || fixed[cl.atom[b]] || fixed[cl.atom[c]]) return false;
+        out = cl;
+        out.atom[0] = cl.atom[ap];
+        out.atom[1] = cl.atom[b];
+        out.atom[2] = cl.atom[c];
+        out.ca[0] = 0; out.cb[0] = 1; out.d[0] = dab;
+        out.ca[1] = 0; out.cb[1] = 2; out.d[1] = dac;
+        out.ca[2] = 1; out.cb[2] = 2; out.d[2] = cl.d[base];
+        return true;
+      }
+      return false;
+    };
+    {
+      int n33 = 0, ntri = 0;
+      Cluster tmp;
+      for (const auto& cl : t.clusters)
+        if (cl.na == 3 && cl.nc == 3 && in_cl[cl.atom[0]]) {
+          ++n33;
+          ntri += as_triangle(cl, tmp) ? 1 : 0;
+        }
+      e->settle = (n33 > 0 && ntri == n33) ? 1 : 0;
+      if (const char* v = std::getenv("FZ_SETTLE")) e->settle = e->settle && std::atoi(v) != 0;
+    }
     for (int na = 2; na <= 4; ++na)
       for (int nc = 1; nc <= 3; ++nc)
-        for (const auto& cl : t.clusters) {
-          if (cl.na != na || cl.nc != nc || !in_cl[cl.atom[0]]) continue;
+        for (const auto& cl0 : t.clusters) {
+          if (cl0.na != na || cl0.nc != nc || !in_cl[cl0.atom[0]]) continue;
+          Cluster cl = cl0;
+          if (e->settle && na == 3 && nc == 3) as_triangle(cl0, cl);
           open_class(na, nc);
           ua.push_back(make_int4(cl.atom[0], cl.atom[1], cl.atom[2], cl.atom[3]));
           int meta = cl.na | (cl.nc << 4);

@@ -85,6 +85,7 @@ struct Engine {
   bool forces_valid = false;
   long long step = 0;
   double self_energy = 0, inv_mtot = 0, dtu = 0, shake_tol = 1e-10;
+  int settle = 0;  // (3,3) units solved by SETTLE (all are symmetric triangles)
   double box_d[3] = {0, 0, 0};
   int ncons = 0;
   int temp_reset_every = 0;
@@ -333,6 +334,7 @@ struct Engine {
     }
     a.shake_tol = shake_tol;
     a.shake_maxit = 500;
+    a.settle = settle;
     a.lam = 1.0;
     a.vfric = 1.0;
     a.u_begin = 0;
@@ -430,15 +432,26 @@ struct Engine {
     if (e != cudaSuccess) capture_error = e;
   }
   // neighbour maintenance: conditional nodes inside a capture, else flag-checking kernels
-  void rebuild_step() {
+  bool capturing_conditional() {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    return cond_graph && st_cap && cudaStreamIsCapturing(st, &cs) == cudaSuccess &&
+           cs == cudaStreamCaptureStatusActive;
+  }
+  // list rebuild when due (it wraps the positions, so it precedes every reader)
+  void rebuild_build_step() {
     const fzk::RebuildArgs ra = rebuild_args();
-    if (cond_graph && st_cap && cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusActive) {
-      conditional(flag, [&](cudaStream_t s) { fzk::launch_rebuild_build(ra, s); });
-      conditional(flag_prune, [&](cudaStream_t s) { fzk::launch_rebuild_prune(ra, s); });
-    } else {
-      fzk::launch_rebuild(ra, st);
-    }
+    if (capturing_conditional()) conditional(flag, [&](cudaStream_t s) { fzk::launch_rebuild_build(ra, s); });
+    else fzk::launch_rebuild_build(ra, st);
+  }
+  // inner-list prune when due (reads the sorted positions, writes only list data)
+  void prune_step() {
+    const fzk::RebuildArgs ra = rebuild_args();
+    if (capturing_conditional()) conditional(flag_prune, [&](cudaStream_t s) { fzk::launch_rebuild_prune(ra, s); });
+    else fzk::launch_rebuild_prune(ra, st);
+  }
+  void rebuild_step() {
+    rebuild_build_step();
+    prune_step();
   }
   // kernels one captured step launches besides the conditional bodies
   long long graph_step_launches() const {
@@ -454,11 +467,13 @@ struct Engine {
     seen_pr_launch = cnt[fzk::CNT_PRUNES];
   }
   // forces with PME on st2, overlapping the pair and bonded kernels on st
+  // (PME needs only the positions, so it starts before the prune and overlaps it too)
   void forces_overlapped() {
-    rebuild_step();
+    rebuild_build_step();
     cudaEventRecord(ev_fork, st);
     cudaStreamWaitEvent(st2, ev_fork, 0);
     fzk::launch_pme(pme_args(), false, st2);
+    prune_step();
     fzk::launch_nonbonded(nb_args(), false, st);
     fzk::launch_bonded(bonded_args(), false, st);
     if (restraint) restraint_forces(st);

@@ -172,6 +172,100 @@ __device__ __forceinline__ int shake_unit(const Unit& U, const double rref[4][3]
   return it >= a.shake_maxit ? 1 : 0;
 }
 
+__device__ __forceinline__ void cross3d(const double* a, const double* b, double* c) {
+  c[0] = a[1] * b[2] - a[2] * b[1];
+  c[1] = a[2] * b[0] - a[0] * b[2];
+  c[2] = a[0] * b[1] - a[1] * b[0];
+}
+__device__ __forceinline__ double dot3d(const double* a, const double* b) {
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+__device__ __forceinline__ void unit3d(double* a) {
+  const double s = rsqrt(dot3d(a, a));
+  a[0] *= s;
+  a[1] *= s;
+  a[2] *= s;
+}
+
+// SETTLE (Miyamoto and Kollman, J. Comput. Chem. 13, 952 (1992)): the closed-form
+// solution of the SHAKE equations for a rigid triangle with an apex (atom 0) and two
+// base atoms of equal mass at equal distance from it, constraints ordered (0,1),
+// (0,2), (1,2).  The constraint displacements lie in the plane of r(t), so in a frame
+// with n0 normal to that plane every atom keeps its n0 coordinate and the triangle
+// is placed by three rotations (phi, psi, theta) solved in closed form; the result is
+// the converged SHAKE solution without iterations.  Works on offsets from the apex's
+// r(t) (min-imaged), so large coordinates do not enter; rn: unconstrained positions
+// in, constrained out.  Returns false when the step is too large for a solution.
+__device__ __forceinline__ bool settle_unit(const Unit& U, const double rref[4][3], double rn[4][3],
+                                            const double* im, const IntegrateArgs& a) {
+  const double mA = 1.0 / im[0], mB = 1.0 / im[1];
+  const double wA = mA / (mA + 2.0 * mB), wB = mB / (mA + 2.0 * mB);
+  const double rc = 0.5 * U.d[2];
+  const double h = sqrt(U.d[0] * U.d[0] - rc * rc);
+  const double ra = 2.0 * wB * h, rb = h - ra;
+  double b0[3], c0[3], a1[3], b1[3], c1[3], D[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    b0[c] = rref[1][c] - rref[0][c];
+    c0[c] = rref[2][c] - rref[0][c];
+  }
+  minimg3(b0, a);
+  minimg3(c0, a);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    a1[c] = rn[0][c] - rref[0][c];
+    b1[c] = b0[c] + (rn[1][c] - rref[1][c]);
+    c1[c] = c0[c] + (rn[2][c] - rref[2][c]);
+    D[c] = wA * a1[c] + wB * (b1[c] + c1[c]);
+    a1[c] -= D[c];
+    b1[c] -= D[c];
+    c1[c] -= D[c];
+  }
+  double n0[3], n1[3], n2[3];
+  cross3d(b0, c0, n0);
+  cross3d(a1, n0, n1);
+  cross3d(n0, n1, n2);
+  unit3d(n0);
+  unit3d(n1);
+  unit3d(n2);
+  const double b0x = dot3d(n1, b0), b0y = dot3d(n2, b0), c0x = dot3d(n1, c0), c0y = dot3d(n2, c0);
+  const double a1z = dot3d(n0, a1);
+  const double b1x = dot3d(n1, b1), b1y = dot3d(n2, b1), b1z = dot3d(n0, b1);
+  const double c1x = dot3d(n1, c1), c1y = dot3d(n2, c1), c1z = dot3d(n0, c1);
+  const double sinphi = a1z / ra;
+  const double cphi2 = 1.0 - sinphi * sinphi;
+  if (!(cphi2 > 0.0)) return false;
+  const double cosphi = sqrt(cphi2);
+  const double sinpsi = (b1z - c1z) / (2.0 * rc * cosphi);
+  const double cpsi2 = 1.0 - sinpsi * sinpsi;
+  if (!(cpsi2 > 0.0)) return false;
+  const double cospsi = sqrt(cpsi2);
+  const double ya2 = ra * cosphi, xb2 = -rc * cospsi;
+  const double t1 = -rb * cosphi, t2 = rc * sinpsi * sinphi;
+  const double yb2 = t1 - t2, yc2 = t1 + t2;
+  const double al = xb2 * (b0x - c0x) + b0y * yb2 + c0y * yc2;
+  const double be = xb2 * (c0y - b0y) + b0x * yb2 + c0x * yc2;
+  const double ga = b0x * b1y - b1x * b0y + c0x * c1y - c1x * c0y;
+  const double ab2 = al * al + be * be;
+  const double disc = ab2 - ga * ga;
+  if (!(disc >= 0.0) || !(ab2 > 0.0)) return false;
+  const double sinth = (al * ga - be * sqrt(disc)) / ab2;
+  const double costh = sqrt(fmax(0.0, 1.0 - sinth * sinth));
+  // final offsets from D in the (n1, n2, n0) frame, minus the r(t) offsets from the apex
+  const double p[3][3] = {{-ya2 * sinth, ya2 * costh, a1z},
+                          {xb2 * costh - yb2 * sinth, xb2 * sinth + yb2 * costh, b1z},
+                          {-xb2 * costh - yc2 * sinth, -xb2 * sinth + yc2 * costh, c1z}};
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const double x = D[c] + p[k][0] * n1[c] + p[k][1] * n2[c] + p[k][2] * n0[c];
+      const double x0 = k == 0 ? 0.0 : (k == 1 ? b0[c] : c0[c]);
+      rn[k][c] = rref[k][c] + (x - x0);
+    }
+  return true;
+}
+
 // RATTLE velocity stage: (v_a - v_b) . r_ab = 0, linear, solved directly
 __device__ __forceinline__ void rattle_unit(const Unit& U, const double r[4][3], double v[4][3], const double* im,
                                             const IntegrateArgs& a) {
@@ -248,7 +342,7 @@ __device__ __forceinline__ void scale_com_velocity(const Unit& U, double v[4][3]
 // NPT (Andersen barostat step with the integration units as scaling groups): the unit
 // moves rigidly with its mass centre scaled by a.lam about the origin (the box changed
 // by a.lam), and its centre-of-mass velocity is scaled by a.vfric before the kick.
-template <bool NPT, int NA, int NC>
+template <bool NPT, int NA, int NC, bool SETTLE = false>
 __global__ void __launch_bounds__(128) k_kick_drift(IntegrateArgs a) {
   const int u = a.u_begin + blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= a.u_end) return;
@@ -279,14 +373,14 @@ __global__ void __launch_bounds__(128) k_kick_drift(IntegrateArgs a) {
   for (int k = 0; k < 4; ++k) {
     if (k >= U.na) continue;
     const int i = U.atom[k];
-    const double3 F = force_of(a.facc, n, i);
+    const double3 Fk = force_of(a.facc, n, i);
     a.facc[i] = 0;
     a.facc[n + i] = 0;
     a.facc[2 * n + i] = 0;
     const double h = 0.5 * a.dtu * im[k];
-    v[k][0] += h * F.x;
-    v[k][1] += h * F.y;
-    v[k][2] += h * F.z;
+    v[k][0] += h * Fk.x;
+    v[k][1] += h * Fk.y;
+    v[k][2] += h * Fk.z;
   }
   if (NPT) {
     // Each atom moves by (lam - 1) x the unit's mass centre taken in the atom's own
@@ -320,7 +414,9 @@ __global__ void __launch_bounds__(128) k_kick_drift(IntegrateArgs a) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) rn[k][c] = r0[k][c] + a.dtu * v[k][c];
   if (U.nc > 0) {
-    const int st = shake_unit(U, r0, rn, im, a);
+    int st;
+    if constexpr (SETTLE) st = settle_unit(U, r0, rn, im, a) ? 0 : 1;
+    else st = shake_unit(U, r0, rn, im, a);
     if (st) atomicOr(a.status, ST_SHAKE_NOCONV);
     const double idt = 1.0 / a.dtu;
 #pragma unroll
@@ -344,8 +440,12 @@ __global__ void __launch_bounds__(128) k_kick_drift(IntegrateArgs a) {
     const float ex = np.x - pp.x, ey = np.y - pp.y, ez = np.z - pp.z;
     moved |= ex * ex + ey * ey + ez * ez > a.prune_half2;
   }
-  if (far) *a.flag = 1;
-  if (moved) *a.flag_prune = 1;
+  // one store per warp: on a step where many atoms cross the threshold, per-thread
+  // stores to the same word would queue at one L2 slice
+  const unsigned am = __activemask();
+  const bool lead = (threadIdx.x & 31) == __ffs(am) - 1;
+  if (__any_sync(am, far) && lead) *a.flag = 1;
+  if (__any_sync(am, moved) && lead) *a.flag_prune = 1;
 }
 
 // Group (unit) virial terms of a barostat step, after the forces: the centre-of-mass
@@ -594,8 +694,12 @@ __global__ void __launch_bounds__(128) k_min_step(IntegrateArgs a) {
     const float ex = np.x - pp.x, ey = np.y - pp.y, ez = np.z - pp.z;
     moved |= ex * ex + ey * ey + ez * ez > a.prune_half2;
   }
-  if (far) *a.flag = 1;
-  if (moved) *a.flag_prune = 1;
+  // one store per warp: on a step where many atoms cross the threshold, per-thread
+  // stores to the same word would queue at one L2 slice
+  const unsigned am = __activemask();
+  const bool lead = (threadIdx.x & 31) == __ffs(am) - 1;
+  if (__any_sync(am, far) && lead) *a.flag = 1;
+  if (__any_sync(am, moved) && lead) *a.flag_prune = 1;
 }
 
 // ---------------------------------------------------------------- velocity reassignment
@@ -690,17 +794,25 @@ void for_classes(const IntegrateArgs& a0, F f) {
 
 static int unit_grid(const IntegrateArgs& a) { return (a.u_end - a.u_begin + 127) / 128; }
 
-void launch_kick_drift(const IntegrateArgs& a, cudaStream_t st) {
+// (3, 3) units go to the SETTLE instantiation when every one of them is a symmetric
+// triangle (a.settle), which keeps its registers apart from the Newton solver's
+template <bool NPT>
+static void kick_drift_classes(const IntegrateArgs& a, cudaStream_t st) {
   for_classes(a, [&](const IntegrateArgs& x, auto na, auto nc) {
-    k_kick_drift<false, decltype(na)::value, decltype(nc)::value><<<unit_grid(x), 128, 0, st>>>(x);
+    constexpr int NA = decltype(na)::value, NC = decltype(nc)::value;
+    if constexpr (NA == 3 && NC == 3) {
+      if (x.settle) {
+        k_kick_drift<NPT, 3, 3, true><<<unit_grid(x), 128, 0, st>>>(x);
+        return;
+      }
+    }
+    k_kick_drift<NPT, NA, NC><<<unit_grid(x), 128, 0, st>>>(x);
   });
 }
 
-void launch_kick_drift_npt(const IntegrateArgs& a, cudaStream_t st) {
-  for_classes(a, [&](const IntegrateArgs& x, auto na, auto nc) {
-    k_kick_drift<true, decltype(na)::value, decltype(nc)::value><<<unit_grid(x), 128, 0, st>>>(x);
-  });
-}
+void launch_kick_drift(const IntegrateArgs& a, cudaStream_t st) { kick_drift_classes<false>(a, st); }
+
+void launch_kick_drift_npt(const IntegrateArgs& a, cudaStream_t st) { kick_drift_classes<true>(a, st); }
 
 void launch_unit_virial(const IntegrateArgs& a, cudaStream_t st) {
   for_classes(a, [&](const IntegrateArgs& x, auto na, auto nc) {

@@ -135,6 +135,7 @@ struct IntegrateArgs {
   double box_d[3], inv_box_d[3];
   double shake_tol;
   int shake_maxit;
+  int settle;  // every (3 atoms, 3 constraints) unit is a SETTLE triangle, apex first
   int u_begin, u_end;        // unit range of one launch (set by the launchers)
   int ncls;                  // unit classes: units [cls_begin[c], cls_begin[c+1]) have
   int cls_na[8], cls_nc[8];  //   cls_na[c] atoms and cls_nc[c] constraints
