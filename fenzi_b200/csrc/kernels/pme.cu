@@ -534,10 +534,16 @@ __device__ __forceinline__ void small_dft(float2* v) {
   }
 }
 
+// Threads per block of the compile-time FFT kernels (all are launched with 256) and
+// lines per block, both constants so the index arithmetic of every load, store and
+// butterfly loop folds to shifts and multiplies and the loops unroll.
+constexpr int kFftThreads = 256;
+__host__ __device__ constexpr int fft_lines_per_block(int n) { return n >= 256 ? 8 : (n >= 128 ? 16 : 32); }
+
 template <int N, int R, int NS, bool INV>
 __device__ __forceinline__ void fft_stage_t(const float2* x, float2* y, const float2* tw, int nl) {
   constexpr int NB = N / R, STEP = N / (NS * R), LD = N + 1;
-  for (int idx = threadIdx.x; idx < nl * NB; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < nl * NB; idx += kFftThreads) {
     const int l = idx / NB, j = idx - l * NB;
     const int k = j % NS;
     const float2* xl = x + l * LD;
@@ -573,7 +579,8 @@ __device__ __forceinline__ float2* fft_run_t(float2* a, float2* b, const float2*
 }
 
 template <int N>
-__global__ void __launch_bounds__(256) k_fft_x_r2c_t(PmeArgs a, int nl) {
+__global__ void __launch_bounds__(256) k_fft_x_r2c_t(PmeArgs a, int) {
+  constexpr int nl = fft_lines_per_block(N);
   extern __shared__ float2 sm[];
   constexpr int LD = N + 1, NH = N / 2 + 1;
   const int nrows = a.K[1] * a.K[2];
@@ -582,14 +589,14 @@ __global__ void __launch_bounds__(256) k_fft_x_r2c_t(PmeArgs a, int nl) {
   float2* B = A + nl * LD;
   load_tw(tw, a.tw[0], N);
   const int r0 = blockIdx.x * nl;
-  for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < nl * N; idx += kFftThreads) {
     const int l = idx / N, x = idx - l * N;
     const int row = r0 + l;
     A[l * LD + x] = make_float2(row < nrows ? a.grid[(size_t)row * N + x] : 0.f, 0.f);
   }
   __syncthreads();
   const float2* R = fft_run_t<N, 0, 1, false>(A, B, tw, nl);
-  for (int idx = threadIdx.x; idx < nl * NH; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < nl * NH; idx += kFftThreads) {
     const int l = idx / NH, m = idx - l * NH;
     const int row = r0 + l;
     if (row < nrows) a.cgrid[(size_t)row * NH + m] = R[l * LD + m];
@@ -597,7 +604,8 @@ __global__ void __launch_bounds__(256) k_fft_x_r2c_t(PmeArgs a, int nl) {
 }
 
 template <int N, bool INV>
-__global__ void __launch_bounds__(256) k_fft_y_t(PmeArgs a, int nl) {
+__global__ void __launch_bounds__(256) k_fft_y_t(PmeArgs a, int) {
+  constexpr int nl = fft_lines_per_block(N);
   extern __shared__ float2 sm[];
   constexpr int LD = N + 1;
   const int Kxh = a.K[0] / 2 + 1;
@@ -607,14 +615,14 @@ __global__ void __launch_bounds__(256) k_fft_y_t(PmeArgs a, int nl) {
   float2* A = sm + N;
   float2* B = A + nl * LD;
   load_tw(tw, a.tw[1], N);
-  for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < nl * N; idx += kFftThreads) {
     const int y = idx / nl, l = idx - y * nl;
     const int mx = mx0 + l;
     A[l * LD + y] = mx < Kxh ? a.cgrid[((size_t)z * N + y) * Kxh + mx] : make_float2(0.f, 0.f);
   }
   __syncthreads();
   const float2* R = fft_run_t<N, 0, 1, INV>(A, B, tw, nl);
-  for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < nl * N; idx += kFftThreads) {
     const int y = idx / nl, l = idx - y * nl;
     const int mx = mx0 + l;
     if (mx < Kxh) a.cgrid[((size_t)z * N + y) * Kxh + mx] = R[l * LD + y];
@@ -622,7 +630,8 @@ __global__ void __launch_bounds__(256) k_fft_y_t(PmeArgs a, int nl) {
 }
 
 template <int N, bool ENERGY>
-__global__ void __launch_bounds__(256) k_fft_z_conv_t(PmeArgs a, int nl) {
+__global__ void __launch_bounds__(256) k_fft_z_conv_t(PmeArgs a, int) {
+  constexpr int nl = fft_lines_per_block(N);
   extern __shared__ float2 sm[];
   constexpr int LD = N + 1;
   const int Kx = a.K[0], Ky = a.K[1], Kxh = Kx / 2 + 1;
@@ -632,7 +641,7 @@ __global__ void __launch_bounds__(256) k_fft_z_conv_t(PmeArgs a, int nl) {
   float2* A = sm + N;
   float2* B = A + nl * LD;
   load_tw(tw, a.tw[2], N);
-  for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < nl * N; idx += kFftThreads) {
     const int z = idx / nl, l = idx - z * nl;
     const int mx = mx0 + l;
     A[l * LD + z] = mx < Kxh ? a.cgrid[((size_t)z * Ky + y) * Kxh + mx] : make_float2(0.f, 0.f);
@@ -642,7 +651,7 @@ __global__ void __launch_bounds__(256) k_fft_z_conv_t(PmeArgs a, int nl) {
   float2* O = (R == A) ? B : A;
   double e = 0.0, w0 = 0.0, w1 = 0.0, w2 = 0.0;
   const float gy = a.gfac[1][y], fy2 = a.f2[1][y];
-  for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < nl * N; idx += kFftThreads) {
     const int l = idx / N, z = idx - l * N;
     const int mx = mx0 + l;
     float2 v = R[l * LD + z];
@@ -666,7 +675,7 @@ __global__ void __launch_bounds__(256) k_fft_z_conv_t(PmeArgs a, int nl) {
   }
   __syncthreads();
   const float2* Q = fft_run_t<N, 0, 1, true>(R, O, tw, nl);
-  for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < nl * N; idx += kFftThreads) {
     const int z = idx / nl, l = idx - z * nl;
     const int mx = mx0 + l;
     if (mx < Kxh) a.cgrid[((size_t)z * Ky + y) * Kxh + mx] = Q[l * LD + z];
@@ -680,7 +689,8 @@ __global__ void __launch_bounds__(256) k_fft_z_conv_t(PmeArgs a, int nl) {
 }
 
 template <int N>
-__global__ void __launch_bounds__(256) k_fft_x_c2r_t(PmeArgs a, int nl) {
+__global__ void __launch_bounds__(256) k_fft_x_c2r_t(PmeArgs a, int) {
+  constexpr int nl = fft_lines_per_block(N);
   extern __shared__ float2 sm[];
   constexpr int LD = N + 1, NH = N / 2 + 1;
   const int nrows = a.K[1] * a.K[2];
@@ -689,7 +699,7 @@ __global__ void __launch_bounds__(256) k_fft_x_c2r_t(PmeArgs a, int nl) {
   float2* B = A + nl * LD;
   load_tw(tw, a.tw[0], N);
   const int r0 = blockIdx.x * nl;
-  for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < nl * N; idx += kFftThreads) {
     const int l = idx / N, m = idx - l * N;
     const int row = r0 + l;
     float2 v = make_float2(0.f, 0.f);
@@ -704,7 +714,7 @@ __global__ void __launch_bounds__(256) k_fft_x_c2r_t(PmeArgs a, int nl) {
   }
   __syncthreads();
   const float2* R = fft_run_t<N, 0, 1, true>(A, B, tw, nl);
-  for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < nl * N; idx += kFftThreads) {
     const int l = idx / N, x = idx - l * N;
     const int row = r0 + l;
     if (row < nrows) a.grid[(size_t)row * N + x] = R[l * LD + x].x;
@@ -765,7 +775,7 @@ static FftPlan make_plan(int n) {
   return p;  // m == 1 checked by the caller (grid sizes are 2^a 3^b 5^c)
 }
 
-static int lines_for(int n) { return n >= 256 ? 8 : (n >= 128 ? 16 : 32); }
+static int lines_for(int n) { return fft_lines_per_block(n); }
 
 void launch_pme(const PmeArgs& a, bool energy, cudaStream_t st) {
   const int nbr = a.nb[0] * a.nb[1] * a.nb[2];
