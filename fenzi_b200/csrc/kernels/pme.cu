@@ -578,9 +578,12 @@ __device__ __forceinline__ float2* fft_run_t(float2* a, float2* b, const float2*
   }
 }
 
+// Real rows in pairs: rows 2p and 2p+1 of the block are the real and imaginary parts of
+// one complex line, so each complex FFT transforms two rows; with Z its transform,
+// X0(m) = (Z(m) + conj Z(N-m)) / 2 and X1(m) = (Z(m) - conj Z(N-m)) / 2i.
 template <int N>
 __global__ void __launch_bounds__(256) k_fft_x_r2c_t(PmeArgs a, int) {
-  constexpr int nl = fft_lines_per_block(N);
+  constexpr int nl = fft_lines_per_block(N);  // complex lines = row pairs per block
   extern __shared__ float2 sm[];
   constexpr int LD = N + 1, NH = N / 2 + 1;
   const int nrows = a.K[1] * a.K[2];
@@ -588,18 +591,21 @@ __global__ void __launch_bounds__(256) k_fft_x_r2c_t(PmeArgs a, int) {
   float2* A = sm + N;
   float2* B = A + nl * LD;
   load_tw(tw, a.tw[0], N);
-  const int r0 = blockIdx.x * nl;
+  const int r0 = blockIdx.x * 2 * nl;
   for (int idx = threadIdx.x; idx < nl * N; idx += kFftThreads) {
     const int l = idx / N, x = idx - l * N;
-    const int row = r0 + l;
-    A[l * LD + x] = make_float2(row < nrows ? a.grid[(size_t)row * N + x] : 0.f, 0.f);
+    const int row = r0 + 2 * l;
+    A[l * LD + x] = make_float2(row < nrows ? a.grid[(size_t)row * N + x] : 0.f,
+                                row + 1 < nrows ? a.grid[(size_t)(row + 1) * N + x] : 0.f);
   }
   __syncthreads();
   const float2* R = fft_run_t<N, 0, 1, false>(A, B, tw, nl);
   for (int idx = threadIdx.x; idx < nl * NH; idx += kFftThreads) {
     const int l = idx / NH, m = idx - l * NH;
-    const int row = r0 + l;
-    if (row < nrows) a.cgrid[(size_t)row * NH + m] = R[l * LD + m];
+    const int row = r0 + 2 * l;
+    const float2 z = R[l * LD + m], w = R[l * LD + (m == 0 ? 0 : N - m)];  // w = Z(N-m)
+    if (row < nrows) a.cgrid[(size_t)row * NH + m] = make_float2(0.5f * (z.x + w.x), 0.5f * (z.y - w.y));
+    if (row + 1 < nrows) a.cgrid[(size_t)(row + 1) * NH + m] = make_float2(0.5f * (z.y + w.y), 0.5f * (w.x - z.x));
   }
 }
 
@@ -688,6 +694,8 @@ __global__ void __launch_bounds__(256) k_fft_z_conv_t(PmeArgs a, int) {
   }
 }
 
+// Inverse of the pairing above: Z(m) = X0(m) + i X1(m) over the full line (Hermitian
+// extension for m > N/2) transforms back to row 2p + i row 2p+1.
 template <int N>
 __global__ void __launch_bounds__(256) k_fft_x_c2r_t(PmeArgs a, int) {
   constexpr int nl = fft_lines_per_block(N);
@@ -698,26 +706,29 @@ __global__ void __launch_bounds__(256) k_fft_x_c2r_t(PmeArgs a, int) {
   float2* A = sm + N;
   float2* B = A + nl * LD;
   load_tw(tw, a.tw[0], N);
-  const int r0 = blockIdx.x * nl;
+  const int r0 = blockIdx.x * 2 * nl;
   for (int idx = threadIdx.x; idx < nl * N; idx += kFftThreads) {
     const int l = idx / N, m = idx - l * N;
-    const int row = r0 + l;
-    float2 v = make_float2(0.f, 0.f);
-    if (row < nrows) {
-      if (m < NH) v = a.cgrid[(size_t)row * NH + m];
-      else {
-        v = a.cgrid[(size_t)row * NH + (N - m)];
-        v.y = -v.y;
-      }
+    const int row = r0 + 2 * l;
+    const bool lo = m < NH;
+    const int mm = lo ? m : N - m;
+    float2 x0 = make_float2(0.f, 0.f), x1 = make_float2(0.f, 0.f);
+    if (row < nrows) x0 = a.cgrid[(size_t)row * NH + mm];
+    if (row + 1 < nrows) x1 = a.cgrid[(size_t)(row + 1) * NH + mm];
+    if (!lo) {
+      x0.y = -x0.y;
+      x1.y = -x1.y;
     }
-    A[l * LD + m] = v;
+    A[l * LD + m] = make_float2(x0.x - x1.y, x0.y + x1.x);
   }
   __syncthreads();
   const float2* R = fft_run_t<N, 0, 1, true>(A, B, tw, nl);
   for (int idx = threadIdx.x; idx < nl * N; idx += kFftThreads) {
     const int l = idx / N, x = idx - l * N;
-    const int row = r0 + l;
-    if (row < nrows) a.grid[(size_t)row * N + x] = R[l * LD + x].x;
+    const int row = r0 + 2 * l;
+    const float2 v = R[l * LD + x];
+    if (row < nrows) a.grid[(size_t)row * N + x] = v.x;
+    if (row + 1 < nrows) a.grid[(size_t)(row + 1) * N + x] = v.y;
   }
 }
 
@@ -795,7 +806,8 @@ void launch_pme(const PmeArgs& a, bool energy, cudaStream_t st) {
   const size_t smz = (size_t)(Kz + 2 * lz * (Kz + 1)) * sizeof(float2);
   const dim3 gx((rows + lx - 1) / lx), gy(Kz * ((Kxh + ly - 1) / ly)), gz(Ky * ((Kxh + lz - 1) / lz));
   // compile-time-sized kernels where available, runtime plans otherwise
-  if (!fft_x_r2c_t(a, lx, gx, smx, st)) k_fft_x_r2c<<<gx, 256, smx, st>>>(a, px, lx);
+  const dim3 gx2((rows + 2 * lx - 1) / (2 * lx));  // compile-time x kernels: row pairs
+  if (!fft_x_r2c_t(a, lx, gx2, smx, st)) k_fft_x_r2c<<<gx, 256, smx, st>>>(a, px, lx);
   if (!fft_y_t(a, ly, false, gy, smy, st)) k_fft_y<<<gy, 256, smy, st>>>(a, py, ly, 0);
   if (!fft_z_t(a, lz, energy, gz, smz, st)) {
     if (energy)
@@ -804,7 +816,7 @@ void launch_pme(const PmeArgs& a, bool energy, cudaStream_t st) {
       k_fft_z_conv<false><<<gz, 256, smz, st>>>(a, pz, lz);
   }
   if (!fft_y_t(a, ly, true, gy, smy, st)) k_fft_y<<<gy, 256, smy, st>>>(a, py, ly, 1);
-  if (!fft_x_c2r_t(a, lx, gx, smx, st)) k_fft_x_c2r<<<gx, 256, smx, st>>>(a, px, lx);
+  if (!fft_x_c2r_t(a, lx, gx2, smx, st)) k_fft_x_c2r<<<gx, 256, smx, st>>>(a, px, lx);
   k_pme_gather<<<(a.n + 255) / 256, 256, 0, st>>>(a);
 }
 
