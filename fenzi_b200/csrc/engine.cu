@@ -386,7 +386,6 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
     if ((r = e->alloc(&e->brick_of, n)) || (r = e->alloc(&e->brick_count, nbr)) ||
         (r = e->alloc(&e->brick_cursor, nbr)) || (r = e->alloc(&e->brick_start, nbr + 1)) ||
         (r = e->alloc(&e->brick_atoms, n)) || (r = e->alloc(&e->grid, (size_t)Kx * Ky * Kz)) ||
-        (r = e->alloc(&e->stage, (size_t)nbr * (e->B[0] + 3) * (e->B[1] + 3) * (e->B[2] + 3))) ||
         (r = e->alloc(&e->cgrid, (size_t)Kz * Ky * (Kx / 2 + 1))))
       return r;
     const double b2 = c.kappa * c.kappa;

@@ -76,7 +76,6 @@ struct Engine {
   int *brick_of = nullptr, *brick_count = nullptr, *brick_cursor = nullptr, *brick_start = nullptr,
       *brick_atoms = nullptr;
   float* grid = nullptr;
-  int* stage = nullptr;
   float2* cgrid = nullptr;
   float2* tw[3] = {nullptr, nullptr, nullptr};
   float *gfac[3] = {nullptr, nullptr, nullptr}, *f2[3] = {nullptr, nullptr, nullptr};
@@ -271,7 +270,6 @@ struct Engine {
     a.brick_start = brick_start;
     a.brick_atoms = brick_atoms;
     a.grid = grid;
-    a.stage = stage;
     a.cgrid = cgrid;
     a.gscale = gscale;
     a.facc = facc;

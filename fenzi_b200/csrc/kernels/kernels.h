@@ -82,8 +82,7 @@ struct PmeArgs {
   int* brick_cursor;
   int* brick_start;  // [nbricks+1]
   int* brick_atoms;  // [n]
-  int* stage;        // per-brick charge regions (B+3)^3, int32 fixed point 2^24
-  float* grid;       // real grid Kz*Ky*Kx (charges, then potential)
+  float* grid;       // real grid Kz*Ky*Kx: int32 fixed-point charges, then the float potential
   float2* cgrid;     // complex half grid Kz*Ky*(Kx/2+1)
   const float2* tw[3];     // twiddles per dimension (forward, e^{-2 pi i m/K})
   const float* gfac[3];    // per-dim b^2 exp(-pi^2 f^2/beta^2)

@@ -4,13 +4,13 @@
 // pair and BCMultiply (src/mdcuda.cu:748,780, src/cell_based_kernels.cu:1770-1826)
 // and PMEForce_medium/_large (src/pme_kernels.cu:381-770).
 //
-// Spreading in two phases: the grid is cut into bricks and atoms are binned by the
-// brick of their base grid point every step; one CTA per brick spreads each of its
-// atoms once into a shared-memory region (the brick grown by the 3-point stencil
-// reach on its low side) with int32 fixed-point atomics and stores the region to its
-// staging slot; k_pme_reduce then sums, per grid point, the <= 8 regions covering it.
-// Integer sums are order independent, so the grid is bit-reproducible; there are no
-// global atomics and no per-grid-point lists.  B-splines are evaluated analytically
+// Spreading: the grid is cut into bricks and atoms are binned by the brick of their
+// base grid point every step; one CTA per brick spreads each of its atoms once into a
+// shared-memory region (the brick grown by the 3-point stencil reach on its low side)
+// with int32 fixed-point atomics, then adds the region into the int32 charge grid with
+// one global atomic add per nonzero point (a point gets <= 8 such adds, from the
+// regions covering it).  Integer sums are order independent, so the grid is
+// bit-reproducible; there are no per-grid-point lists.  B-splines are evaluated analytically
 // (the reference samples a 1001-point table with a truncating index).
 #include "common.cuh"
 #include "kernels.h"
@@ -118,13 +118,17 @@ __global__ void k_pme_scatter(PmeArgs a) {
 
 constexpr float kFixQ32 = 16777216.0f;  // charge grid fixed point, 2^24 per e
 
+// the grid buffer holds int32 fixed-point charges from the spread until the x pass
+// reads them, and the float potential from the inverse x pass until the gather
+__device__ __forceinline__ float charge_at(const PmeArgs& a, size_t i) {
+  return (float)reinterpret_cast<const int*>(a.grid)[i] * (1.0f / kFixQ32);
+}
+
 // One CTA per brick processes the atoms binned to that brick exactly once: their
 // 4x4x4 stencils (grid points k0-3..k0 per dimension) all fall inside the brick grown
 // by 3 points on the low side, accumulated in shared memory with int32 fixed-point
-// atomics (2^24 per e; values stay far below +-128 e).  The region is stored to the
-// brick's staging slot with plain stores; k_pme_reduce then sums, for every grid point,
-// the <= 8 regions that cover it.  No global atomics, integer sums are exact, so the
-// charge grid is bit-reproducible.
+// atomics (2^24 per e; values stay far below +-128 e).  The region is then added to
+// the int32 charge grid; integer sums are exact, so the grid is bit-reproducible.
 __global__ void __launch_bounds__(256) k_pme_spread(PmeArgs a) {
   extern __shared__ int acc[];
   const int Bx = a.B[0], By = a.B[1], Bz = a.B[2];
@@ -160,43 +164,21 @@ __global__ void __launch_bounds__(256) k_pme_spread(PmeArgs a) {
       }
   }
   __syncthreads();
-  int* stage = a.stage + (size_t)b * vol;
-  for (int k = threadIdx.x; k < vol; k += blockDim.x) stage[k] = acc[k];
+  // add the region into the int32 charge grid (zeroed before the spread); the low-side
+  // halo wraps periodically, the region never passes the grid's upper end
+  int* g = reinterpret_cast<int*>(a.grid);
+  for (int k = threadIdx.x; k < vol; k += blockDim.x) {
+    const int v = acc[k];
+    if (v == 0) continue;
+    const int rx = k % Ex, ry = (k / Ex) % Ey, rz = k / (Ex * Ey);
+    int gx = ox + rx, gy = oy + ry, gz = oz + rz;
+    gx += gx < 0 ? Kx : 0;
+    gy += gy < 0 ? Ky : 0;
+    gz += gz < 0 ? Kz : 0;
+    atomicAdd(g + ((size_t)gz * Ky + gy) * Kx + gx, v);
+  }
 }
 
-// charge grid point (x, y, z) = sum over the bricks whose grown region covers it: its
-// own brick and, within 3 points of the brick's upper faces, the next brick(s)
-__global__ void __launch_bounds__(256) k_pme_reduce(PmeArgs a) {
-  const int Kx = a.K[0], Ky = a.K[1], Kz = a.K[2];
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= Kx * Ky * Kz) return;
-  const int x = g % Kx, y = (g / Kx) % Ky, z = g / (Kx * Ky);
-  const int Bx = a.B[0], By = a.B[1], Bz = a.B[2];
-  const int Ex = Bx + 3, Ey = By + 3, Ez = Bz + 3;
-  const int nbx = a.nb[0], nby = a.nb[1], nbz = a.nb[2];
-  const int bx = x / Bx, by = y / By, bz = z / Bz;
-  const int lx = x - bx * Bx, ly = y - by * By, lz = z - bz * Bz;
-  const int vol = Ex * Ey * Ez;
-  int sum = 0;
-#pragma unroll
-  for (int dz = 0; dz < 2; ++dz) {
-    if (dz && lz < Bz - 3) continue;
-    const int cz = dz ? (bz + 1) % nbz : bz, rz = dz ? lz - Bz + 3 : lz + 3;
-#pragma unroll
-    for (int dy = 0; dy < 2; ++dy) {
-      if (dy && ly < By - 3) continue;
-      const int cy = dy ? (by + 1) % nby : by, ry = dy ? ly - By + 3 : ly + 3;
-#pragma unroll
-      for (int dx = 0; dx < 2; ++dx) {
-        if (dx && lx < Bx - 3) continue;
-        const int cx = dx ? (bx + 1) % nbx : bx, rx = dx ? lx - Bx + 3 : lx + 3;
-        const int brick = (cz * nby + cy) * nbx + cx;
-        sum += a.stage[(size_t)brick * vol + (rz * Ey + ry) * Ex + rx];
-      }
-    }
-  }
-  a.grid[g] = (float)sum * (1.0f / kFixQ32);
-}
 
 // ------------------------------------------------------------------ FFT
 // Stockham autosort FFT of nl lines of length n in shared memory (x at a[l*n + i]).
@@ -293,7 +275,7 @@ __global__ void __launch_bounds__(256) k_fft_x_r2c(PmeArgs a, FftPlan pl, int nl
   for (int idx = threadIdx.x; idx < nl * Kx; idx += blockDim.x) {
     const int l = idx / Kx, x = idx - l * Kx;
     const int row = r0 + l;
-    A[l * ld + x] = make_float2(row < nrows ? a.grid[(size_t)row * Kx + x] : 0.f, 0.f);
+    A[l * ld + x] = make_float2(row < nrows ? charge_at(a, (size_t)row * Kx + x) : 0.f, 0.f);
   }
   __syncthreads();
   const float2* R = fft_lines(A, B, tw, pl, nl, false);
@@ -595,8 +577,8 @@ __global__ void __launch_bounds__(256) k_fft_x_r2c_t(PmeArgs a, int) {
   for (int idx = threadIdx.x; idx < nl * N; idx += kFftThreads) {
     const int l = idx / N, x = idx - l * N;
     const int row = r0 + 2 * l;
-    A[l * LD + x] = make_float2(row < nrows ? a.grid[(size_t)row * N + x] : 0.f,
-                                row + 1 < nrows ? a.grid[(size_t)(row + 1) * N + x] : 0.f);
+    A[l * LD + x] = make_float2(row < nrows ? charge_at(a, (size_t)row * N + x) : 0.f,
+                                row + 1 < nrows ? charge_at(a, (size_t)(row + 1) * N + x) : 0.f);
   }
   __syncthreads();
   const float2* R = fft_run_t<N, 0, 1, false>(A, B, tw, nl);
@@ -795,8 +777,8 @@ void launch_pme(const PmeArgs& a, bool energy, cudaStream_t st) {
   k_pme_scan<<<1, 1024, 0, st>>>(a, nbr);
   k_pme_scatter<<<(a.n + 255) / 256, 256, 0, st>>>(a);
   const size_t sp = (size_t)(a.B[0] + 3) * (a.B[1] + 3) * (a.B[2] + 3) * sizeof(int);
+  cudaMemsetAsync(a.grid, 0, (size_t)a.K[0] * a.K[1] * a.K[2] * sizeof(float), st);
   k_pme_spread<<<nbr, 256, sp, st>>>(a);
-  k_pme_reduce<<<(a.K[0] * a.K[1] * a.K[2] + 255) / 256, 256, 0, st>>>(a);
   const int Kx = a.K[0], Ky = a.K[1], Kz = a.K[2], Kxh = Kx / 2 + 1;
   const FftPlan px = make_plan(Kx), py = make_plan(Ky), pz = make_plan(Kz);
   const int lx = lines_for(Kx), ly = lines_for(Ky), lz = lines_for(Kz);

@@ -31,8 +31,6 @@ constexpr int kSMaxBricks = 22 * 22 * 22;
 constexpr int kSMaxDev = 64;
 
 __device__ __align__(256) float s_grid[kSMaxK * kSMaxK * kSMaxK];
-constexpr int kSMaxStage = 1536 * 1024;  // per-brick charge regions, (K/B)^3 (B+3)^3 ints
-__device__ __align__(256) int s_stage[kSMaxStage];
 __device__ __align__(256) float2 s_cgrid[kSMaxK * kSMaxK * (kSMaxK / 2 + 1)];
 __device__ __align__(256) int s_brick_of[kSMaxAtoms];
 __device__ __align__(256) int s_brick_atoms[kSMaxAtoms];
@@ -47,7 +45,6 @@ __device__ __align__(256) int s_status[1];
 
 struct Scratch {
   float* grid;
-  int* stage;
   float2* cgrid;
   int *brick_of, *brick_atoms, *brick_count, *brick_cursor, *brick_start, *status;
   float2* tw;
@@ -67,7 +64,6 @@ fz_status setup(int device, Scratch** out) {
     float2* tw = nullptr;
     float *gf = nullptr, *f2 = nullptr;
     if ((e = cudaGetSymbolAddress((void**)&s.grid, s_grid)) != cudaSuccess ||
-        (e = cudaGetSymbolAddress((void**)&s.stage, s_stage)) != cudaSuccess ||
         (e = cudaGetSymbolAddress((void**)&s.cgrid, s_cgrid)) != cudaSuccess ||
         (e = cudaGetSymbolAddress((void**)&s.brick_of, s_brick_of)) != cudaSuccess ||
         (e = cudaGetSymbolAddress((void**)&s.brick_atoms, s_brick_atoms)) != cudaSuccess ||
@@ -156,11 +152,6 @@ extern "C" fz_status fz_pme_reciprocal_static(int device, void* stream, const fl
       (ce = cudaMemsetAsync(s->energy, 0, sizeof(long long) * fzk::EN_COUNT, st)) != cudaSuccess ||
       (ce = cudaMemsetAsync(facc, 0, sizeof(long long) * 3 * (size_t)n, st)) != cudaSuccess)
     return fail(FZ_ERR_CUDA, std::string("fz_pme_reciprocal_static: ") + cudaGetErrorString(ce));
-  {
-    long long need = 1;
-    for (int d = 0; d < 3; ++d) need *= (long long)(K[d] / brick_edge(K[d])) * (brick_edge(K[d]) + 3);
-    if (need > kSMaxStage) return fail(FZ_ERR_ARG, "fz_pme_reciprocal_static: grid too large for the static scratch");
-  }
   fzk::PmeArgs a{};
   a.p.box = make_float3((float)box[0], (float)box[1], (float)box[2]);
   a.p.inv_box = make_float3((float)(1.0 / box[0]), (float)(1.0 / box[1]), (float)(1.0 / box[2]));
@@ -183,7 +174,6 @@ extern "C" fz_status fz_pme_reciprocal_static(int device, void* stream, const fl
   a.brick_start = s->brick_start;
   a.brick_atoms = s->brick_atoms;
   a.grid = s->grid;
-  a.stage = s->stage;
   a.cgrid = s->cgrid;
   a.gscale = (float)(kCC / (M_PI * box[0] * box[1] * box[2]));
   a.facc = facc;
