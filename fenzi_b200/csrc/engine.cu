@@ -140,7 +140,10 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
   e->ocap = (int)std::ceil(std::max(256.0, 1.25 * rho * vm) / 32.0) * 32;
   e->mask_cap = (e->nslots / 32) * fzk::kNG * (e->ocap / 32);
   {
-    const double delta = std::min(0.3, plist - c.cutoff);
+    // inner-list buffer: a larger delta prunes less often but leaves more pairs
+    double want = 0.3;
+    if (const char* v = std::getenv("FZ_PRUNE_DELTA")) want = std::max(0.05, std::atof(v));
+    const double delta = std::min(want, plist - c.cutoff);
     e->rp2 = (float)((c.cutoff + delta) * (c.cutoff + delta));
     e->prune_half2 = (float)(0.25 * delta * delta);
     e->prune_delta = delta;

@@ -64,13 +64,13 @@ __device__ __forceinline__ float pair_force(const PairConst& c, float r2, float 
                                             float& ee) {
   const float rinv = rsqrt_a(r2);
   const float r2inv = rinv * rinv;
-  const float br = r2 * rinv * c.beta;                   // beta r
   const float ex = ex2_a(r2 * c.eb2);                    // exp(-beta^2 r^2)
-  const float tt = rcp_a(fmaf(kAS_p, br, 1.f));
+  const float tt = rcp_a(fmaf(c.p_b, r2 * rinv, 1.f));   // 1 / (1 + p beta r)
   const float poly = tt * fmaf(tt, fmaf(tt, fmaf(tt, fmaf(tt, kAS_a5, kAS_a4), kAS_a3), kAS_a2), kAS_a1);
-  const float qe = qq * ex * rinv;
-  // F_C r / r^2 = qq (erfc(br)/r + 2 beta/sqrt(pi) exp(-b^2 r^2)) / r^2
-  const float fc = qe * fmaf(c.c2b, r2 * rinv, poly) * r2inv;
+  // erfc(beta r) = poly exp(-beta^2 r^2), so F_C r / r^2 = qq (erfc(beta r)/r + 2 beta/sqrt(pi)
+  // exp(-beta^2 r^2)) / r^2 = qq exp(-beta^2 r^2) (poly / r + 2 beta/sqrt(pi)) / r^2
+  const float qex = qq * ex;
+  const float fc = qex * fmaf(poly, rinv, c.c2b) * r2inv;
   const float s2 = ls.y * r2inv;
   const float s6 = s2 * s2 * s2;
   const float a = ls.x * s6;
@@ -84,7 +84,7 @@ __device__ __forceinline__ float pair_force(const PairConst& c, float r2, float 
   float fr = fmaf(flj, sw, fmaf(elj, dsw, fc));
   if (ENERGY) {
     ev += ok ? elj * sw : 0.f;
-    ee += ok ? qe * poly : 0.f;
+    ee += ok ? qex * poly * rinv : 0.f;
   }
   return ok ? fr : 0.f;
 }
