@@ -168,7 +168,7 @@ extern "C" fz_status fz_batch_step(fz_batch* b, int nsteps) {
         FZ_CUDA(cudaStreamWaitEvent(e->st, b->ev_master, 0));
         fzk::launch_reassign(e->int_args(), e->temperature, e->seed, (uint32_t)(e->step / e->temp_reset_every),
                              e->inv_mtot, e->psum, e->st);
-        e->launches += 4;
+        e->launches += 3 + e->ncls;
         FZ_CUDA(cudaEventRecord(b->ev_done[i], e->st));
         FZ_CUDA(cudaStreamWaitEvent(b->master, b->ev_done[i], 0));
       }

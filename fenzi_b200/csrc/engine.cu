@@ -583,7 +583,7 @@ static fz_status npt_step(Engine* e) {
   ia = e->int_args();
   ia.vfric = std::exp(-0.5 * dt * e->Ldot / Ln);
   fzk::launch_kick_rattle(ia, false, true, e->st);
-  e->launches += 4 + 12 + 1 + ((e->nbond + e->nangle + e->nub + e->ndihe + e->nimpr + e->nexcl + e->n14 > 0) ? 1 : 0) + 12;
+  e->launches += 3 * e->ncls;  // kick/drift, unit virial, kick/RATTLE (forces() counts its own)
   return FZ_OK;
 }
 
@@ -652,13 +652,13 @@ extern "C" fz_status fz_step(fz_system* s, int nsteps) {
       fzk::launch_kick_rattle(ia, false, true, e->st);
       e->mark(6);
       if (e->timing) e->collect_step();
-      e->launches += 2;
+      e->launches += 2 * e->ncls;
     }
     e->step++;
     if (e->temp_reset_every > 0 && e->step % e->temp_reset_every == 0) {
       fzk::launch_reassign(e->npt ? e->int_args() : ia, e->temperature, e->seed, (uint32_t)(e->step / e->temp_reset_every), e->inv_mtot,
                            e->psum, e->st);
-      e->launches += 4;
+      e->launches += 3 + e->ncls;
     }
   }
   return e->check();

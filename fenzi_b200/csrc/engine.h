@@ -353,7 +353,7 @@ struct Engine {
   void forces(bool energies, int terms = FZ_TERM_ALL) {
     mark(1);
     fzk::launch_rebuild(rebuild_args(), st);
-    launches += 12;
+    launches += fzk::kRebuildBuildLaunches + fzk::kRebuildPruneLaunches;
     mark(2);
     if (terms & FZ_TERM_NONBONDED) {
       fzk::launch_nonbonded(nb_args(), energies, st);
@@ -362,13 +362,16 @@ struct Engine {
     mark(3);
     if (terms & FZ_TERM_BONDED) {
       fzk::launch_bonded(bonded_args(), energies, st);
-      launches += (nbond + nangle + nub + ndihe + nimpr + nexcl + n14 > 0) ? 1 : 0;
+      launches += bonded_launches();
     }
-    if ((terms & FZ_TERM_BONDED) && restraint) restraint_forces(st);
+    if ((terms & FZ_TERM_BONDED) && restraint) {
+      restraint_forces(st);
+      launches += 2;
+    }
     mark(4);
     if (terms & FZ_TERM_PME) {
       fzk::launch_pme(pme_args(), energies, st);
-      launches += 12;
+      launches += fzk::kPmeLaunches;
     }
     mark(5);
   }
@@ -392,9 +395,10 @@ struct Engine {
     cudaMemsetAsync(rs_acc, 0, 8 * sizeof(long long), s);
     fzk::launch_restraint(p, pos4, rs_seg, rs_mass, rs_acc, rs_inv_m[0], rs_inv_m[1], rs_dist, rs_fc, facc, s);
   }
-  // Adds to the capture on st an IF node that runs body(stream) when *dflag != 0.
+  // Adds to the capture on st an IF node that runs body(stream) when *dflag != 0 (or
+  // *dflag2 != 0 when given).
   template <class F>
-  void conditional(const int* dflag, F body) {
+  void conditional(const int* dflag, const int* dflag2, F body) {
     cudaStreamCaptureStatus cs;
     unsigned long long id;
     cudaGraph_t g = nullptr;
@@ -407,7 +411,7 @@ struct Engine {
       capture_error = e;
       return;
     }
-    fzk::launch_set_condition(h, dflag, st);
+    fzk::launch_set_condition(h, dflag, dflag2, st);
     e = cudaStreamGetCaptureInfo(st, &cs, &id, &g, &deps, &nd);
     cudaGraphNodeParams np{};
     np.type = cudaGraphNodeTypeConditional;
@@ -438,13 +442,15 @@ struct Engine {
   // list rebuild when due (it wraps the positions, so it precedes every reader)
   void rebuild_build_step() {
     const fzk::RebuildArgs ra = rebuild_args();
-    if (capturing_conditional()) conditional(flag, [&](cudaStream_t s) { fzk::launch_rebuild_build(ra, s); });
+    if (capturing_conditional()) conditional(flag, nullptr, [&](cudaStream_t s) { fzk::launch_rebuild_build(ra, s); });
     else fzk::launch_rebuild_build(ra, st);
   }
   // inner-list prune when due (reads the sorted positions, writes only list data)
   void prune_step() {
     const fzk::RebuildArgs ra = rebuild_args();
-    if (capturing_conditional()) conditional(flag_prune, [&](cudaStream_t s) { fzk::launch_rebuild_prune(ra, s); });
+    // a rebuild this step (flag still raised) always ends in a prune
+    if (capturing_conditional())
+      conditional(flag_prune, flag, [&](cudaStream_t s) { fzk::launch_rebuild_prune(ra, s); });
     else fzk::launch_rebuild_prune(ra, st);
   }
   void rebuild_step() {
@@ -453,13 +459,16 @@ struct Engine {
   }
   // kernels one captured step launches besides the conditional bodies
   long long graph_step_launches() const {
-    return 2 + (cond_graph ? 2 : 12) + 1 + ((nbond + nangle + nub + ndihe + nimpr + nexcl + n14 > 0) ? 1 : 0) + 12;
+    return 2 * ncls + (cond_graph ? 2 : fzk::kRebuildBuildLaunches + fzk::kRebuildPruneLaunches) + 1 +
+           bonded_launches() + fzk::kPmeLaunches + (restraint ? 2 : 0);
   }
-  // launches of the conditional bodies (9 per rebuild, 3 per prune) since the last
+  int bonded_launches() const { return (nbond + nangle + nub + ndihe + nimpr + nexcl + n14 > 0) ? 1 : 0; }
+  // launches of the conditional bodies (per rebuild and per prune) since the last
   // call, from the device counters; called after a synchronisation
   void account_conditional(const int* cnt) {
     if (cond_graph && graph_since_check)
-      launches += 9 * (cnt[fzk::CNT_REBUILDS] - seen_rb_launch) + 3 * (cnt[fzk::CNT_PRUNES] - seen_pr_launch);
+      launches += fzk::kRebuildBuildLaunches * (cnt[fzk::CNT_REBUILDS] - seen_rb_launch) +
+                  fzk::kRebuildPruneLaunches * (cnt[fzk::CNT_PRUNES] - seen_pr_launch);
     graph_since_check = false;
     seen_rb_launch = cnt[fzk::CNT_REBUILDS];
     seen_pr_launch = cnt[fzk::CNT_PRUNES];

@@ -5,7 +5,13 @@
 namespace fzk {
 
 constexpr int kColCap = 4096;  // atoms per column sorted in shared memory
-enum : int { CNT_TILES = 0, CNT_MASKS, CNT_SLOTS, CNT_REBUILDS, CNT_PRUNES, CNT_WORK, CNT_ITEMS, CNT_COUNT = 8 };
+enum : int {
+  CNT_TILES = 0, CNT_MASKS, CNT_SLOTS, CNT_REBUILDS, CNT_PRUNES, CNT_WORK, CNT_ITEMS, CNT_COUNT = 8
+};
+// kernels each launcher issues (the step's launch count)
+constexpr int kRebuildBuildLaunches = 6;  // launch_rebuild_build
+constexpr int kRebuildPruneLaunches = 3;  // launch_rebuild_prune
+constexpr int kPmeLaunches = 11;          // launch_pme
 
 struct RebuildArgs {
   SysParams p;
@@ -46,7 +52,8 @@ void launch_rebuild(const RebuildArgs& a, cudaStream_t st);
 void launch_rebuild_build(const RebuildArgs& a, cudaStream_t st);
 void launch_rebuild_prune(const RebuildArgs& a, cudaStream_t st);
 // one-thread kernel: graph conditional value = (*flag != 0)
-void launch_set_condition(cudaGraphConditionalHandle h, const int* flag, cudaStream_t st);
+// IF-node value = (*flag || (flag2 && *flag2))
+void launch_set_condition(cudaGraphConditionalHandle h, const int* flag, const int* flag2, cudaStream_t st);
 
 struct NonbondedArgs {
   SysParams p;

@@ -15,15 +15,6 @@
 
 namespace fzk {
 
-__global__ void k_rb_begin(const int* __restrict__ flag, int* col_count, int* col_cursor, int ncol, int* counters) {
-  if (!*flag) return;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncol; c += gridDim.x * blockDim.x) {
-    col_count[c] = 0;
-    col_cursor[c] = 0;
-  }
-
-}
-
 // wrap positions into [-L/2, L/2), record build positions, bin into columns
 __global__ void k_rb_bin(SysParams p, const int* __restrict__ flag, float4* pos4, float4* pos_build, int* col_of,
                          int* col_count, int* status) {
@@ -108,8 +99,8 @@ __device__ __forceinline__ uint32_t float_key(float f) {
 }
 
 // one block per column: bitonic sort by (z, atom id), then fill the sorted arrays
-__global__ void __launch_bounds__(256) k_rb_colsort(SysParams p, const int* __restrict__ flag,
-                                                    const int* __restrict__ col_count,
+__global__ void __launch_bounds__(256) k_rb_colsort(SysParams p, const int* __restrict__ flag, int* col_count,
+                                                    int* col_cursor,
                                                     const int* __restrict__ col_start, const int* __restrict__ col_tmp,
                                                     const float4* __restrict__ pos4, const int* __restrict__ type,
                                                     int* perm, int* inv_perm, float4* xyzq_s, int* typ_s, int* blk_col,
@@ -119,6 +110,12 @@ __global__ void __launch_bounds__(256) k_rb_colsort(SysParams p, const int* __re
   const int c = blockIdx.x;
   const int n = col_count[c];
   const int start = col_start[c];
+  // the column's count and cursor are spent: zero them for the next rebuild's binning
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    col_count[c] = 0;
+    col_cursor[c] = 0;
+  }
   const int padded = (n + 31) & ~31;
   if (start + padded > p.nslots - 32) return;  // slot overflow already flagged
   if (n > kColCap) {
@@ -167,34 +164,6 @@ __global__ void __launch_bounds__(256) k_rb_colsort(SysParams p, const int* __re
       xyzq_s[s] = make_float4(1.0e6f + (float)s, 1.0e6f, 1.0e6f, 0.f);
       typ_s[s] = p.ntypes;
     }
-  }
-}
-
-// per-block bounding boxes (warp per block)
-__global__ void k_rb_bbox(SysParams p, const int* __restrict__ flag, const int* __restrict__ counters,
-                          const int* __restrict__ perm, const float4* __restrict__ xyzq_s, float4* bb_lo,
-                          float4* bb_hi) {
-  if (!*flag) return;
-  const int nblk = counters[CNT_SLOTS] >> 5;
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (w >= nblk) return;
-  const int s = w * 32 + lane;
-  const bool ok = perm[s] >= 0;
-  const float4 r = xyzq_s[s];
-  float lx = ok ? r.x : 3e38f, ly = ok ? r.y : 3e38f, lz = ok ? r.z : 3e38f;
-  float hx = ok ? r.x : -3e38f, hy = ok ? r.y : -3e38f, hz = ok ? r.z : -3e38f;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    lx = fminf(lx, __shfl_xor_sync(0xffffffffu, lx, o));
-    ly = fminf(ly, __shfl_xor_sync(0xffffffffu, ly, o));
-    lz = fminf(lz, __shfl_xor_sync(0xffffffffu, lz, o));
-    hx = fmaxf(hx, __shfl_xor_sync(0xffffffffu, hx, o));
-    hy = fmaxf(hy, __shfl_xor_sync(0xffffffffu, hy, o));
-    hz = fmaxf(hz, __shfl_xor_sync(0xffffffffu, hz, o));
-  }
-  if (lane == 0) {
-    bb_lo[w] = make_float4(lx, ly, lz, 0.f);
-    bb_hi[w] = make_float4(hx, hy, hz, 0.f);
   }
 }
 
@@ -300,13 +269,15 @@ __global__ void __launch_bounds__(256) k_rb_outer(SysParams p, const int* __rest
   }
 }
 
-// partner slots of every slot's excluded atoms (1-2, 1-3, 1-4), for the prune's masks
-__global__ void k_rb_xslot(SysParams p, const int* __restrict__ flag, const int* __restrict__ perm,
-                           const int* __restrict__ inv_perm, const int* __restrict__ excl_off,
-                           const int* __restrict__ excl_idx, int* xn, int* xs, int xmax) {
+// Per slot: the partner slots of its excluded atoms (1-2, 1-3, 1-4), for the prune's
+// masks; per 32-slot block (one warp): the bounding box of its atoms
+__global__ void k_rb_slots(SysParams p, const int* __restrict__ flag, const int* __restrict__ counters,
+                           const int* __restrict__ perm, const int* __restrict__ inv_perm,
+                           const int* __restrict__ excl_off, const int* __restrict__ excl_idx, int* xn, int* xs,
+                           int xmax, const float4* __restrict__ xyzq_s, float4* bb_lo, float4* bb_hi) {
   if (!*flag) return;
   const int sl = blockIdx.x * blockDim.x + threadIdx.x;
-  if (sl >= p.nslots) return;
+  if (sl >= p.nslots) return;  // nslots is a multiple of 32: whole warps leave together
   const int a = perm[sl];
   int m = 0;
   if (a >= 0) {
@@ -315,9 +286,35 @@ __global__ void k_rb_xslot(SysParams p, const int* __restrict__ flag, const int*
     for (int k = 0; k < m; ++k) xs[(size_t)sl * xmax + k] = inv_perm[excl_idx[e0 + k]];
   }
   xn[sl] = m;
+  const int w = sl >> 5, lane = sl & 31;
+  if (w >= (counters[CNT_SLOTS] >> 5)) return;  // uniform per warp
+  const bool ok = a >= 0;
+  const float4 r = xyzq_s[sl];
+  float lx = ok ? r.x : 3e38f, ly = ok ? r.y : 3e38f, lz = ok ? r.z : 3e38f;
+  float hx = ok ? r.x : -3e38f, hy = ok ? r.y : -3e38f, hz = ok ? r.z : -3e38f;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lx = fminf(lx, __shfl_xor_sync(0xffffffffu, lx, o));
+    ly = fminf(ly, __shfl_xor_sync(0xffffffffu, ly, o));
+    lz = fminf(lz, __shfl_xor_sync(0xffffffffu, lz, o));
+    hx = fmaxf(hx, __shfl_xor_sync(0xffffffffu, hx, o));
+    hy = fmaxf(hy, __shfl_xor_sync(0xffffffffu, hy, o));
+    hz = fmaxf(hz, __shfl_xor_sync(0xffffffffu, hz, o));
+  }
+  if (lane == 0) {
+    bb_lo[w] = make_float4(lx, ly, lz, 0.f);
+    bb_hi[w] = make_float4(hx, hy, hz, 0.f);
+  }
 }
 
-__global__ void k_prune_begin(const int* __restrict__ flag_prune, int* counters) {
+// Closes a rebuild (counts it, lowers its flag, raises the prune flag: a new outer list
+// always gets a fresh inner list) and opens a prune (zeroes the list counters).
+__global__ void k_prune_begin(int* flag, int* flag_prune, int* counters) {
+  if (*flag) {
+    counters[CNT_REBUILDS] += 1;
+    *flag = 0;
+    *flag_prune = 1;
+  }
   if (!*flag_prune) return;
   counters[CNT_MASKS] = 0;
   counters[CNT_TILES] = 0;
@@ -500,22 +497,16 @@ __global__ void k_prune_end(int* flag_prune, int* counters) {
   *flag_prune = 0;
 }
 
-__global__ void k_rb_end(int* flag, int* flag_prune, int* counters) {
-  if (!*flag) return;
-  counters[CNT_REBUILDS] += 1;
-  *flag = 0;
-  *flag_prune = 1;  // a new outer list always gets a fresh inner list
-}
-
 // sets a graph conditional node's value from a device flag (the neighbour kernels run
 // inside an IF node only when their flag is raised)
-__global__ void k_set_condition(cudaGraphConditionalHandle h, const int* __restrict__ flag) {
-  cudaGraphSetConditional(h, *flag != 0 ? 1u : 0u);
+__global__ void k_set_condition(cudaGraphConditionalHandle h, const int* __restrict__ flag,
+                                const int* __restrict__ flag2) {
+  cudaGraphSetConditional(h, (*flag != 0 || (flag2 && *flag2 != 0)) ? 1u : 0u);
 }
 
 // ------------------------------------------------------------------ launchers
-void launch_set_condition(cudaGraphConditionalHandle h, const int* flag, cudaStream_t st) {
-  k_set_condition<<<1, 1, 0, st>>>(h, flag);
+void launch_set_condition(cudaGraphConditionalHandle h, const int* flag, const int* flag2, cudaStream_t st) {
+  k_set_condition<<<1, 1, 0, st>>>(h, flag, flag2);
 }
 
 void launch_rebuild(const RebuildArgs& a, cudaStream_t st) {
@@ -526,28 +517,25 @@ void launch_rebuild(const RebuildArgs& a, cudaStream_t st) {
 void launch_rebuild_build(const RebuildArgs& a, cudaStream_t st) {
   const SysParams& p = a.p;
   const int ncol = p.ncol[0] * p.ncol[1];
-  k_rb_begin<<<(ncol + 255) / 256, 256, 0, st>>>(a.flag, a.col_count, a.col_cursor, ncol, a.counters);
   k_rb_bin<<<(p.n + 255) / 256, 256, 0, st>>>(p, a.flag, a.pos4, a.pos_build, a.col_of, a.col_count, a.status);
   k_rb_scan<<<1, 1024, 0, st>>>(p, a.flag, a.col_count, a.col_start, ncol, a.counters, a.status);
   k_rb_scatter<<<(p.n + 255) / 256, 256, 0, st>>>(p, a.flag, a.col_of, a.col_start, a.col_cursor, a.col_tmp);
   k_rb_colsort<<<ncol, 256, kColCap * sizeof(unsigned long long), st>>>(
-      p, a.flag, a.col_count, a.col_start, a.col_tmp, a.pos4, a.type, a.perm, a.inv_perm, a.xyzq_s, a.typ_s,
-      a.blk_col, a.status);
-  k_rb_xslot<<<(p.nslots + 255) / 256, 256, 0, st>>>(p, a.flag, a.perm, a.inv_perm, a.excl_off, a.excl_idx, a.xn,
-                                                     a.xs, a.xmax);
+      p, a.flag, a.col_count, a.col_cursor, a.col_start, a.col_tmp, a.pos4, a.type, a.perm, a.inv_perm, a.xyzq_s,
+      a.typ_s, a.blk_col, a.status);
+  k_rb_slots<<<(p.nslots + 255) / 256, 256, 0, st>>>(p, a.flag, a.counters, a.perm, a.inv_perm, a.excl_off,
+                                                     a.excl_idx, a.xn, a.xs, a.xmax, a.xyzq_s, a.bb_lo, a.bb_hi);
   const int maxblk = (p.nslots) / 32;
-  k_rb_bbox<<<(maxblk * 32 + 255) / 256, 256, 0, st>>>(p, a.flag, a.counters, a.perm, a.xyzq_s, a.bb_lo, a.bb_hi);
   k_rb_outer<<<(maxblk + 7) / 8, 256, 0, st>>>(p, a.flag, a.counters, a.perm, a.xyzq_s, a.bb_lo, a.bb_hi, a.blk_col,
                                                a.col_start, a.dcx, a.dcy, a.all_images, a.outer, a.outer_n, a.ocap,
                                                a.xn, a.xs, a.xmax,
                                                a.status);
-  k_rb_end<<<1, 1, 0, st>>>(a.flag, a.flag_prune, a.counters);
 }
 
 void launch_rebuild_prune(const RebuildArgs& a, cudaStream_t st) {
   const SysParams& p = a.p;
   const int maxblk = (p.nslots) / 32;
-  k_prune_begin<<<1, 1, 0, st>>>(a.flag_prune, a.counters);
+  k_prune_begin<<<1, 1, 0, st>>>(a.flag, a.flag_prune, a.counters);
   k_prune<<<(maxblk + 7) / 8, 256, 0, st>>>(p, a.flag_prune, a.counters, a.perm, a.xn, a.xyzq_s, a.xs, a.xmax,
                                             a.outer, a.outer_n, a.inner, a.inner_nt, a.inner_m, a.masks,
                                             a.dmask, a.mask_cap, a.ocap, a.rp2, a.pos_prune, a.items, a.chunk,
