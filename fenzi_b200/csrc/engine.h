@@ -487,14 +487,40 @@ struct Engine {
     cudaEventRecord(ev_join, st2);
     cudaStreamWaitEvent(st, ev_join, 0);
   }
+  // One integrator pass over all unit classes; with a second stream the first class
+  // (free atoms) runs beside the others: classes touch disjoint atoms.
+  template <class L>
+  void integrate_classes(const fzk::IntegrateArgs& ia, L launch) {
+    if (!st2 || ia.ncls < 2) {
+      launch(ia, st);
+      return;
+    }
+    fzk::IntegrateArgs first = ia, rest = ia;
+    first.ncls = 1;
+    rest.ncls = ia.ncls - 1;
+    for (int c = 0; c < rest.ncls; ++c) {
+      rest.cls_na[c] = ia.cls_na[c + 1];
+      rest.cls_nc[c] = ia.cls_nc[c + 1];
+      rest.cls_begin[c] = ia.cls_begin[c + 1];
+    }
+    rest.cls_begin[rest.ncls] = ia.cls_begin[ia.ncls];
+    cudaEventRecord(ev_fork, st);
+    cudaStreamWaitEvent(st2, ev_fork, 0);
+    launch(first, st2);
+    launch(rest, st);
+    cudaEventRecord(ev_join, st2);
+    cudaStreamWaitEvent(st, ev_join, 0);
+  }
   void step_body() {
     const fzk::IntegrateArgs ia = int_args();
-    fzk::launch_kick_drift(ia, st);
+    integrate_classes(ia, [](const fzk::IntegrateArgs& a, cudaStream_t s) { fzk::launch_kick_drift(a, s); });
     if (st2)
       forces_overlapped();
     else
       forces(false);
-    fzk::launch_kick_rattle(ia, false, true, st);
+    integrate_classes(ia, [](const fzk::IntegrateArgs& a, cudaStream_t s) {
+      fzk::launch_kick_rattle(a, false, true, s);
+    });
   }
   fz_status graph_step() {
     if (!step_exec) {

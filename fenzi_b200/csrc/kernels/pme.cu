@@ -165,17 +165,23 @@ __global__ void __launch_bounds__(256) k_pme_spread(PmeArgs a) {
   }
   __syncthreads();
   // add the region into the int32 charge grid (zeroed before the spread); the low-side
-  // halo wraps periodically, the region never passes the grid's upper end
+  // halo wraps periodically, the region never passes the grid's upper end.  A point of
+  // the brick more than 3 below its upper faces (region index 3 .. B-1 on every axis)
+  // lies in no other brick's region, so it takes a plain store; the rest are shared
+  // with the neighbouring bricks' halos and take atomic adds.
   int* g = reinterpret_cast<int*>(a.grid);
   for (int k = threadIdx.x; k < vol; k += blockDim.x) {
     const int v = acc[k];
     if (v == 0) continue;
     const int rx = k % Ex, ry = (k / Ex) % Ey, rz = k / (Ex * Ey);
+    const bool own = rx >= 3 && rx < Bx && ry >= 3 && ry < By && rz >= 3 && rz < Bz;
     int gx = ox + rx, gy = oy + ry, gz = oz + rz;
     gx += gx < 0 ? Kx : 0;
     gy += gy < 0 ? Ky : 0;
     gz += gz < 0 ? Kz : 0;
-    atomicAdd(g + ((size_t)gz * Ky + gy) * Kx + gx, v);
+    int* dst = g + ((size_t)gz * Ky + gy) * Kx + gx;
+    if (own) *dst = v;
+    else atomicAdd(dst, v);
   }
 }
 
