@@ -62,6 +62,8 @@ def args_():
                     help="served-job measurement (Poisson arrivals of 1.5k-30k-atom jobs) with this many jobs; 0 skips it")
     ap.add_argument("--precision", type=int, default=100000,
                     help="precision study: NVE steps of the 17,280-atom system, then NPT; 0 skips it")
+    ap.add_argument("--small", type=int, default=2000,
+                    help="9,000-atom water box: timed product-path steps (plus plain path and CPU oracle); 0 skips it")
     ap.add_argument("--profile", action="store_true",
                     help="only run warm-up + steps (no timing/report): a clean target for ncu")
     return ap.parse_args()
@@ -125,6 +127,28 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def step_ideal_s(pairs, natom, K, peak_tflops, hbm_gbs):
+    """Step roofline time: 60 FLOP per pair within rc at the FP32 peak plus the PME and
+    integration bytes (56 N + 24 K^3 + 120 N) at the HBM bandwidth."""
+    return FLOP_PER_PAIR * pairs / (peak_tflops * 1e12) + (176.0 * natom + 24.0 * K[0] * K[1] * K[2]) / (hbm_gbs * 1e9)
+
+
+def measured_hbm_gbs():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"], "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def oracle_force_error(sy):
+    """Relative RMS of the system's GPU forces at its current positions against the FP64 oracle."""
+    from oracle.oracle import Oracle
+    sy.ComputeAccelGPU()
+    f = sy.forces()
+    f0, _ = Oracle(sy.topology()).forces(sy.positions())
+    return float(np.sqrt(((f - f0) ** 2).sum() / (f0 ** 2).sum()))
+
+
 def traffic_from_profiles(kernel_file):
     p = os.path.join(ROOT, "profiles", kernel_file)
     if not os.path.exists(p):
@@ -135,7 +159,7 @@ def traffic_from_profiles(kernel_file):
         return None
 
 
-def bench_ensemble(nsys, device, steps=30, dist=None):
+def bench_ensemble(nsys, device, steps=30, dist=None, peak_tflops=None):
     """Aggregate atom-steps/s of nsys independent water boxes advanced together (one
     graph launch per step) versus the same boxes stepped one at a time; wall clock with
     a device synchronisation on both sides of each timed region.  Under a process group
@@ -191,12 +215,38 @@ def bench_ensemble(nsys, device, steps=30, dist=None):
     ts = (time.perf_counter() - t0) / seq_steps
     plain_rate, plain_atoms, plain_boxes = plain_one_at_a_time(systems, device)
     batch.close()
+    # step roofline of the whole batch, oracle force error and the FP64 oracle one box
+    # at a time on the host cores (samples)
+    from oracle.oracle import Oracle
+    hbm, hbm_src = measured_hbm_gbs()
+    t_ideal = 0.0
+    for sy in systems:
+        orc = Oracle(sy.topology())
+        t_ideal += step_ideal_s(orc.count_pairs(sy.positions(), sy.cfg.cutoff), sy.n, list(sy.cfg.pme_grid),
+                                peak_tflops or 71.8, hbm)
+    errs = [oracle_force_error(sy) for sy in systems[:: max(1, len(systems) // 4)][:4]]
+    cpu_atoms, cpu_s = 0, 0.0
+    for sy in systems[:: max(1, len(systems) // 8)][:8]:
+        orc = Oracle(sy.topology())
+        p0, v0 = sy.positions(), sy.velocities()
+        orc.forces(p0)
+        t0 = time.perf_counter()
+        orc.md(p0, v0, 3, dt_ps=sy.cfg.timestep_ps, tol=1e-10, traces=False)
+        cpu_s += (time.perf_counter() - t0) / 3
+        cpu_atoms += sy.n
     for sy in systems:
         sy.close()
     return {"metric": "batched aggregate atom-steps/s", "value": natoms / tb, "unit": "atom-steps/s",
             "systems": nsys, "atoms": natoms, "ms_per_batched_step": tb * 1e3,
             "sequential_atom_steps_per_s": natoms / ts, "ms_per_sequential_sweep": ts * 1e3,
             "speedup_vs_one_at_a_time": ts / tb,
+            "step_roofline": {"t_ideal_ms": t_ideal * 1e3, "frac": t_ideal / tb,
+                              "model": "sum over boxes of 60 FLOP/pair / FP32 peak + (176 N + 24 K^3) B / HBM "
+                                       f"({hbm_src} HBM)"},
+            "force_rel_rms_vs_fp64_oracle": {"max": max(errs), "boxes_checked": len(errs)},
+            "cpu_baseline": {"value": cpu_atoms / cpu_s, "unit": "atom-steps/s", "cores": os.cpu_count(),
+                             "kind": "port", "sample": "FP64 oracle MD, 3 steps of each of 8 boxes one after "
+                                                       "another (all host threads inside each box)"},
             "plain_one_at_a_time_atom_steps_per_s": plain_rate,
             "speedup_vs_plain_one_at_a_time": natoms / tb / plain_rate,
             "plain_sample": f"{plain_boxes} of the {len(systems)} boxes (every 4th, {plain_atoms} atoms), each on "
@@ -205,6 +255,61 @@ def bench_ensemble(nsys, device, steps=30, dist=None):
                         f"2^a3^b5^c >= L/1.2), rc 9 / ron 7.5, beta 0.34, SHAKE, NVE, 1 fs; seeded",
             "timing": "wall clock over 30 batched steps vs 10-step sweeps of the boxes one at a time, device "
                       "synchronised around each; working set > L2"}
+
+
+def bench_small(device, peak_tflops, steps=2000):
+    """The 9,000-atom water box (3,000 TIP3P, 44.8 A, 48^3 PME, rc 10): the product path
+    (CUDA events around `steps` steps after 1,100 prepared ones), the plain path from the
+    same state, the FP64 oracle on the host cores, the step roofline and the force error
+    against the oracle."""
+    import torch
+    import fenzi_b200 as fz
+    from fenzi_b200.plain import Plain
+    from oracle.oracle import Oracle
+    _, path = build_inputs("water3000", 2345)
+    s = fz.FenZi.ReadInput(path).LoadSystem()
+    s.InitMem(device)
+    s.InitVelocity(T=300.0, seed=2345)
+    for k in range(10):
+        s.SingleStep(100)
+        s.InitVelocity(T=300.0, seed=2345, counter=k + 1)
+    s.SingleStep(100)
+    stream = torch.cuda.ExternalStream(s.stream(), device=f"cuda:{device}")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    s.SingleStep(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) * 1e-3 / steps
+    p = Plain(s, device)
+    p.set_positions(s.positions())
+    p.set_velocities(s.velocities())
+    p.SingleStep(20)
+    t0 = time.perf_counter()
+    p.SingleStep(300)
+    tp = (time.perf_counter() - t0) / 300
+    p.close()
+    orc = Oracle(s.topology())
+    pairs = orc.count_pairs(s.positions(), s.cfg.cutoff)
+    hbm, hbm_src = measured_hbm_gbs()
+    t_ideal = step_ideal_s(pairs, s.n, list(s.cfg.pme_grid), peak_tflops, hbm)
+    err = oracle_force_error(s)
+    per, cores = cpu_baseline(path, 10)
+    dt_fs = s.cfg.timestep_ps * 1000.0
+    out = {"workload": "water3000: 3,000 TIP3P = 9,000 atoms, 44.8 A, 48^3 PME, beta 0.34, rc 10 / ron 8, "
+                       "SHAKE, 1 fs (1,100 prepared steps with 300 K reassignment every 100)",
+           "ns_per_day": 86.4 * dt_fs / (t * 1e3), "ms_per_step": t * 1e3, "atom_steps_per_s": s.n / t,
+           "step_roofline": {"t_ideal_ms": t_ideal * 1e3, "frac": t_ideal / t, "hbm": hbm_src},
+           "force_rel_rms_vs_fp64_oracle": err,
+           "plain_path": {"ns_per_day": 86.4 * dt_fs / (tp * 1e3), "ms_per_step": tp * 1e3,
+                          "product_speedup": tp / t, "timing": "wall clock over 300 steps"},
+           "cpu_baseline": {"value": 86.4 * dt_fs / (per * 1e3), "unit": "ns/day", "cores": cores, "kind": "port",
+                            "sample": "10 MD steps of the same system, FP64 oracle, all host threads"},
+           "timing": f"CUDA events on the system's stream around {steps} steps (graph replay; the 2.2 us "
+                     "roofline step is launch-latency bound)"}
+    s.close()
+    return out
 
 
 def plain_one_at_a_time(systems, device, every=4, steps=10, warm=3):
@@ -420,6 +525,9 @@ def bench_precision(device, nve_steps=100000, npt_steps=2000, fp64_steps=20000):
         s.InitVelocity(T=300.0, seed=2345, counter=k + 1)
     s.SingleStep(100)
     pos0, vel0 = s.positions(), s.velocities()
+    per, cores = cpu_baseline(path, 3)
+    cpu = {"value": 86.4 * s.cfg.timestep_ps * 1e3 / (per * 1e3), "unit": "ns/day", "cores": cores, "kind": "port",
+           "sample": "3 MD steps of the same system, FP64 oracle, all host threads"}
     chunk = 1000
     t, tot = [], []
     t0 = time.perf_counter()
@@ -453,6 +561,8 @@ def bench_precision(device, nve_steps=100000, npt_steps=2000, fp64_steps=20000):
     out = {"workload": "chain17k: 5,360 TIP3P + 40 x 30-atom chains = 17,280 atoms, 56 A, 64^3, beta 0.34, rc 10, "
                        "SHAKE, 1 fs",
            "nve_steps": nve_steps, "nve_wall_s": wall,
+           "ns_per_day": 86.4 * s.cfg.timestep_ps * 1e3 / (wall / max(1, nve_steps) * 1e3),
+           "cpu_baseline": cpu,
            "nve_drift_kcal_per_mol_per_ns_per_atom": slope, "nve_drift_stderr": slope_err,
            "nve_total_energy_std_kcal_per_mol": float(np.std(tot)),
            "force_rel_rms_vs_fp64_oracle": err,
@@ -639,9 +749,10 @@ def main():
             cpu = {"value": 86.4 * dt_fs / (per * 1e3), "unit": "ns/day", "cores": cores, "kind": "port",
                    "sample": "4 full MD steps of the 230,400-atom system (FP64 oracle, OpenMP, all host threads)"}
         plain = bench_plain_single(sysm, local, t_ideal, ms_step) if world == 1 else None
+        small = bench_small(local, peak, a.small) if a.small > 0 and world == 1 else None
         batched = batched_multi
         if a.ensemble > 0 and world == 1:
-            batched = bench_ensemble(a.ensemble, local)
+            batched = bench_ensemble(a.ensemble, local, peak_tflops=peak)
         served = None
         if a.served > 0 and world == 1:
             served = bench_served(local, a.served)
@@ -663,7 +774,7 @@ def main():
                 "pair_slots": sysm.counters()["pair_slots"],
                 "prunes_total": sysm.counters()["prunes"],
                 "pair_slot_efficiency": pairs / float(sysm.counters()["pair_slots"]),
-                "roofline": roof, "cpu_baseline": cpu, "plain_path": plain,
+                "roofline": roof, "cpu_baseline": cpu, "plain_path": plain, "small_system": small,
                 "e2e": {"value": e2e_nsd, "unit": "ns/day", "h2d_bytes_per_step": 24 * natom / a.chunk,
                         "d2h_bytes_per_step": 24 * natom / a.chunk, "h2d_bytes_per_call": 24 * natom,
                         "d2h_bytes_per_call": 24 * natom,
