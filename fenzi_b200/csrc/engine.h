@@ -371,7 +371,7 @@ struct Engine {
     mark(4);
     if (terms & FZ_TERM_PME) {
       fzk::launch_pme(pme_args(), energies, st);
-      launches += fzk::kPmeLaunches;
+      launches += fzk::pme_launches(pme_args());
     }
     mark(5);
   }
@@ -460,7 +460,7 @@ struct Engine {
   // kernels one captured step launches besides the conditional bodies
   long long graph_step_launches() const {
     return 2 * ncls + (cond_graph ? 2 : fzk::kRebuildBuildLaunches + fzk::kRebuildPruneLaunches) + 1 +
-           bonded_launches() + fzk::kPmeLaunches + (restraint ? 2 : 0);
+           bonded_launches() + fzk::pme_launches(pme_args()) + (restraint ? 2 : 0);
   }
   int bonded_launches() const { return (nbond + nangle + nub + ndihe + nimpr + nexcl + n14 > 0) ? 1 : 0; }
   // launches of the conditional bodies (per rebuild and per prune) since the last

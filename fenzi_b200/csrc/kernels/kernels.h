@@ -11,7 +11,6 @@ enum : int {
 // kernels each launcher issues (the step's launch count)
 constexpr int kRebuildBuildLaunches = 6;  // launch_rebuild_build
 constexpr int kRebuildPruneLaunches = 3;  // launch_rebuild_prune
-constexpr int kPmeLaunches = 11;          // launch_pme
 
 struct RebuildArgs {
   SysParams p;
@@ -100,6 +99,7 @@ struct PmeArgs {
   int* status;
 };
 void launch_pme(const PmeArgs& a, bool energy, cudaStream_t st);
+int pme_launches(const PmeArgs& a);
 
 struct BondedArgs {
   SysParams p;

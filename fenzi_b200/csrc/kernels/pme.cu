@@ -720,6 +720,136 @@ __global__ void __launch_bounds__(256) k_fft_x_c2r_t(PmeArgs a, int) {
   }
 }
 
+// ------------------------------------------------------------------ plane FFTs
+// One CTA per z-plane of a grid with Kx = Ky = N: the x transform (two real rows per
+// complex line) and the y transform of the whole plane in shared memory, so the plane
+// is read and written once, in whole rows (the separate x and y passes each read and
+// wrote the complex grid).  The stage below is the Stockham stage above with compile-
+// time element stride ES and line stride LS; for strided lines (ES > 1) consecutive
+// threads take consecutive lines, so their shared-memory accesses are consecutive.
+constexpr int kPlaneThreads = 1024;
+
+template <int N, int R, int NS, bool INV, int ES, int LS, int NL>
+__device__ __forceinline__ void fft_stage_g(const float2* x, float2* y, const float2* tw) {
+  constexpr int NB = N / R, STEP = N / (NS * R);
+  for (int idx = threadIdx.x; idx < NL * NB; idx += kPlaneThreads) {
+    int l, j;
+    if constexpr (ES == 1) {
+      l = idx / NB;
+      j = idx - l * NB;
+    } else {
+      j = idx / NL;
+      l = idx - j * NL;
+    }
+    const int k = j % NS;
+    const float2* xl = x + l * LS;
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = xl[(j + r * NB) * ES];
+    if constexpr (NS > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        float2 w = tw[r * k * STEP];
+        if (INV) w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+    }
+    small_dft<R, INV>(v);
+    float2* yl = y + l * LS;
+    const int o = (j / NS) * NS * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) yl[(o + r * NS) * ES] = v[r];
+  }
+}
+
+template <int N, int S, int NS, bool INV, int ES, int LS, int NL>
+__device__ __forceinline__ float2* fft_run_g(float2* a, float2* b, const float2* tw) {
+  if constexpr (S == nstages(N)) {
+    return a;
+  } else {
+    constexpr int R = radix_at(N, S);
+    fft_stage_g<N, R, NS, INV, ES, LS, NL>(a, b, tw);
+    __syncthreads();
+    return fft_run_g<N, S + 1, NS * R, INV, ES, LS, NL>(b, a, tw);
+  }
+}
+
+template <int N>
+constexpr size_t plane_smem_bytes() {
+  constexpr int NH = N / 2 + 1, LD = N + 1;
+  constexpr int words = (N * NH > (N / 2) * LD) ? N * NH : (N / 2) * LD;
+  return (size_t)(N + 2 * words) * sizeof(float2);
+}
+
+// forward: real plane z -> half spectrum along x, full spectrum along y, cgrid[z][y][mx]
+template <int N>
+__global__ void __launch_bounds__(kPlaneThreads) k_fft_xy_plane(PmeArgs a) {
+  extern __shared__ float2 sm[];
+  constexpr int LD = N + 1, NH = N / 2 + 1, NP = N / 2;
+  constexpr int words = (N * NH > NP * LD) ? N * NH : NP * LD;
+  float2* tw = sm;
+  float2* A = sm + N;
+  float2* B = A + words;
+  load_tw(tw, a.tw[0], N);
+  const int z = blockIdx.x;
+  const size_t row0 = (size_t)z * N;
+  for (int idx = threadIdx.x; idx < NP * N; idx += kPlaneThreads) {
+    const int l = idx / N, x = idx - l * N;
+    A[l * LD + x] = make_float2(charge_at(a, (row0 + 2 * l) * N + x), charge_at(a, (row0 + 2 * l + 1) * N + x));
+  }
+  __syncthreads();
+  float2* R = fft_run_g<N, 0, 1, false, 1, LD, NP>(A, B, tw);
+  float2* P = (R == A) ? B : A;  // plane [y][mx], row length NH
+  for (int idx = threadIdx.x; idx < NP * NH; idx += kPlaneThreads) {
+    const int l = idx / NH, m = idx - l * NH;
+    const float2 u = R[l * LD + m], w = R[l * LD + (m == 0 ? 0 : N - m)];
+    P[(2 * l) * NH + m] = make_float2(0.5f * (u.x + w.x), 0.5f * (u.y - w.y));
+    P[(2 * l + 1) * NH + m] = make_float2(0.5f * (u.y + w.y), 0.5f * (w.x - u.x));
+  }
+  __syncthreads();
+  // the y twiddles equal the x twiddles (Kx = Ky)
+  const float2* Q = fft_run_g<N, 0, 1, false, NH, 1, NH>(P, R, tw);
+  for (int idx = threadIdx.x; idx < N * NH; idx += kPlaneThreads) a.cgrid[row0 * NH + idx] = Q[idx];
+}
+
+// inverse: cgrid[z][y][mx] -> inverse y, then two rows per complex line through the
+// inverse x transform -> real potential plane z
+template <int N>
+__global__ void __launch_bounds__(kPlaneThreads) k_fft_yx_plane(PmeArgs a) {
+  extern __shared__ float2 sm[];
+  constexpr int LD = N + 1, NH = N / 2 + 1, NP = N / 2;
+  constexpr int words = (N * NH > NP * LD) ? N * NH : NP * LD;
+  float2* tw = sm;
+  float2* A = sm + N;
+  float2* B = A + words;
+  load_tw(tw, a.tw[0], N);
+  const int z = blockIdx.x;
+  const size_t row0 = (size_t)z * N;
+  for (int idx = threadIdx.x; idx < N * NH; idx += kPlaneThreads) A[idx] = a.cgrid[row0 * NH + idx];
+  __syncthreads();
+  float2* Q = fft_run_g<N, 0, 1, true, NH, 1, NH>(A, B, tw);
+  float2* L = (Q == A) ? B : A;  // complex lines of row pairs, length N, stride LD
+  for (int idx = threadIdx.x; idx < NP * N; idx += kPlaneThreads) {
+    const int l = idx / N, m = idx - l * N;
+    const bool lo = m < NH;
+    const int mm = lo ? m : N - m;
+    float2 x0 = Q[(2 * l) * NH + mm], x1 = Q[(2 * l + 1) * NH + mm];
+    if (!lo) {
+      x0.y = -x0.y;
+      x1.y = -x1.y;
+    }
+    L[l * LD + m] = make_float2(x0.x - x1.y, x0.y + x1.x);
+  }
+  __syncthreads();
+  const float2* R = fft_run_g<N, 0, 1, true, 1, LD, NP>(L, Q, tw);
+  for (int idx = threadIdx.x; idx < NP * N; idx += kPlaneThreads) {
+    const int l = idx / N, x = idx - l * N;
+    const float2 v = R[l * LD + x];
+    a.grid[(row0 + 2 * l) * N + x] = v.x;
+    a.grid[(row0 + 2 * l + 1) * N + x] = v.y;
+  }
+}
+
 #define FZ_FFT_SIZES(X) X(16) X(18) X(20) X(24) X(25) X(27) X(30) X(32) X(36) X(40) X(48) X(64) X(80) X(96) X(128)
 
 static bool fft_x_r2c_t(const PmeArgs& a, int nl, dim3 g, size_t sm, cudaStream_t st) {
@@ -754,6 +884,38 @@ static bool fft_z_t(const PmeArgs& a, int nl, bool energy, dim3 g, size_t sm, cu
   }
   return false;
 }
+// plane kernels for cubic-in-xy grids of even size (row pairs); false if not available
+#define FZ_PLANE_SIZES(X) X(16) X(18) X(20) X(24) X(30) X(32) X(36) X(40) X(48) X(64) X(80) X(96) X(128)
+static bool use_plane_fft(const PmeArgs& a) {
+  static const bool on = !std::getenv("FZ_PLANE_FFT") || std::atoi(std::getenv("FZ_PLANE_FFT")) != 0;
+  if (!on || a.K[0] != a.K[1]) return false;
+  switch (a.K[0]) {
+#define FZ_C(N) case N: return true;
+    FZ_PLANE_SIZES(FZ_C)
+#undef FZ_C
+  }
+  return false;
+}
+static void fft_plane(const PmeArgs& a, bool inverse, cudaStream_t st) {
+  switch (a.K[0]) {
+#define FZ_C(N)                                                                                        \
+  case N: {                                                                                            \
+    constexpr size_t sm = plane_smem_bytes<N>();                                                       \
+    static const bool attr = [] {                                                                      \
+      cudaFuncSetAttribute(k_fft_xy_plane<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);   \
+      cudaFuncSetAttribute(k_fft_yx_plane<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);   \
+      return true;                                                                                     \
+    }();                                                                                               \
+    (void)attr;                                                                                        \
+    if (inverse) k_fft_yx_plane<N><<<a.K[2], kPlaneThreads, sm, st>>>(a);                              \
+    else k_fft_xy_plane<N><<<a.K[2], kPlaneThreads, sm, st>>>(a);                                      \
+    return;                                                                                            \
+  }
+    FZ_PLANE_SIZES(FZ_C)
+#undef FZ_C
+  }
+}
+
 static bool fft_x_c2r_t(const PmeArgs& a, int nl, dim3 g, size_t sm, cudaStream_t st) {
   switch (a.K[0]) {
 #define FZ_C(N) case N: k_fft_x_c2r_t<N><<<g, 256, sm, st>>>(a, nl); return true;
@@ -776,6 +938,9 @@ static FftPlan make_plan(int n) {
 
 static int lines_for(int n) { return fft_lines_per_block(n); }
 
+// zero, bin, scan, scatter, spread, 3 or 5 FFT kernels, gather
+int pme_launches(const PmeArgs& a) { return 5 + (use_plane_fft(a) ? 3 : 5) + 1; }
+
 void launch_pme(const PmeArgs& a, bool energy, cudaStream_t st) {
   const int nbr = a.nb[0] * a.nb[1] * a.nb[2];
   k_pme_zero<<<(nbr + 255) / 256, 256, 0, st>>>(a.brick_count, a.brick_cursor, nbr);
@@ -795,16 +960,25 @@ void launch_pme(const PmeArgs& a, bool energy, cudaStream_t st) {
   const dim3 gx((rows + lx - 1) / lx), gy(Kz * ((Kxh + ly - 1) / ly)), gz(Ky * ((Kxh + lz - 1) / lz));
   // compile-time-sized kernels where available, runtime plans otherwise
   const dim3 gx2((rows + 2 * lx - 1) / (2 * lx));  // compile-time x kernels: row pairs
-  if (!fft_x_r2c_t(a, lx, gx2, smx, st)) k_fft_x_r2c<<<gx, 256, smx, st>>>(a, px, lx);
-  if (!fft_y_t(a, ly, false, gy, smy, st)) k_fft_y<<<gy, 256, smy, st>>>(a, py, ly, 0);
+  const bool plane = use_plane_fft(a);
+  if (plane) {
+    fft_plane(a, false, st);
+  } else {
+    if (!fft_x_r2c_t(a, lx, gx2, smx, st)) k_fft_x_r2c<<<gx, 256, smx, st>>>(a, px, lx);
+    if (!fft_y_t(a, ly, false, gy, smy, st)) k_fft_y<<<gy, 256, smy, st>>>(a, py, ly, 0);
+  }
   if (!fft_z_t(a, lz, energy, gz, smz, st)) {
     if (energy)
       k_fft_z_conv<true><<<gz, 256, smz, st>>>(a, pz, lz);
     else
       k_fft_z_conv<false><<<gz, 256, smz, st>>>(a, pz, lz);
   }
-  if (!fft_y_t(a, ly, true, gy, smy, st)) k_fft_y<<<gy, 256, smy, st>>>(a, py, ly, 1);
-  if (!fft_x_c2r_t(a, lx, gx2, smx, st)) k_fft_x_c2r<<<gx, 256, smx, st>>>(a, px, lx);
+  if (plane) {
+    fft_plane(a, true, st);
+  } else {
+    if (!fft_y_t(a, ly, true, gy, smy, st)) k_fft_y<<<gy, 256, smy, st>>>(a, py, ly, 1);
+    if (!fft_x_c2r_t(a, lx, gx2, smx, st)) k_fft_x_c2r<<<gx, 256, smx, st>>>(a, px, lx);
+  }
   k_pme_gather<<<(a.n + 255) / 256, 256, 0, st>>>(a);
 }
 
