@@ -32,6 +32,39 @@
 using namespace fz;
 
 // ====================================================================== batched ensemble
+// Batched kernels: one launch per kernel of the step covers every member.  The members'
+// kernel arguments live in device arrays, and a block table per grid shape maps each
+// launched block to (member, block of that member's own grid, grid size).
+struct BatchKernels {
+  std::vector<void*> allocs;
+  fzk::RebuildArgs* rb = nullptr;
+  fzk::NonbondedArgs* nb = nullptr;
+  fzk::BondedArgs* bd = nullptr;
+  fzk::PmeArgs* pme = nullptr;
+  fzk::BatchTables t{};
+  std::vector<fzk::ClassBatch> classes;
+  std::vector<fzk::PmeSizeBatch> sizes;
+  size_t spread_smem = 0;
+  int max_ntypes = 0;
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  long long launches = 0;  // kernels one batched step launches
+  ~BatchKernels() {
+    for (void* p : allocs) cudaFree(p);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (aux) cudaStreamDestroy(aux);
+  }
+  template <class X> fz_status upload(const std::vector<X>& v, X** out) {
+    void* p = nullptr;
+    FZ_CUDA(cudaMalloc(&p, std::max<size_t>(1, v.size()) * sizeof(X)));
+    allocs.push_back(p);
+    if (!v.empty()) FZ_CUDA(cudaMemcpy(p, v.data(), v.size() * sizeof(X), cudaMemcpyHostToDevice));
+    *out = (X*)p;
+    return FZ_OK;
+  }
+};
+
 struct fz_batch {
   std::vector<fz_system*> systems;
   int dev = -1;
@@ -42,7 +75,9 @@ struct fz_batch {
   cudaGraphExec_t exec = nullptr;
   int* pinned_status = nullptr;
   long long steps = 0;
+  std::unique_ptr<BatchKernels> bk;
   void drop_graph() {
+    bk.reset();
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     exec = nullptr;
@@ -97,6 +132,136 @@ extern "C" fz_status fz_batch_remove(fz_batch* b, fz_system* s) {
   return FZ_OK;
 }
 
+// whether every member can run in the batched kernels (otherwise each member's step is
+// its own branch of the batch graph)
+static bool batched_kernels_ok(const fz_batch* b) {
+  const char* v = std::getenv("FZ_BATCH_KERNELS");
+  if (v && std::atoi(v) == 0) return false;
+  for (const fz_system* s : b->systems) {
+    const Engine* e = s->eng;
+    if (e->cond_graph || e->restraint || e->npt || !fzk::pme_batchable(e->pme_args())) return false;
+  }
+  return true;
+}
+
+static void add_blocks(std::vector<int4>& tab, int arg, int nblocks) {
+  for (int k = 0; k < nblocks; ++k) tab.push_back(make_int4(arg, k, nblocks, 0));
+}
+
+static fz_status build_batch_kernels(fz_batch* b) {
+  auto bk = std::make_unique<BatchKernels>();
+  const int ns = (int)b->systems.size();
+  std::vector<fzk::RebuildArgs> rb;
+  std::vector<fzk::NonbondedArgs> nb;
+  std::vector<fzk::BondedArgs> bd;
+  std::vector<fzk::PmeArgs> pme;
+  std::vector<std::vector<int4>> tabs(fzk::BT_COUNT);
+  // unit classes keyed by (atoms, constraints, SETTLE); PME grids keyed by size
+  struct ClassAcc { int na, nc, settle; std::vector<fzk::IntegrateArgs> args; std::vector<int4> tab; };
+  std::vector<ClassAcc> cls;
+  struct SizeAcc { int N; std::vector<int4> plane, z; };
+  std::vector<SizeAcc> sizes;
+  for (int i = 0; i < ns; ++i) {
+    Engine* e = b->systems[i]->eng;
+    rb.push_back(e->rebuild_args());
+    nb.push_back(e->nb_args());
+    bd.push_back(e->bonded_args());
+    pme.push_back(e->pme_args());
+    const fzk::SysParams& p = rb.back().p;
+    const fzk::PmeArgs& pa = pme.back();
+    const int nbr = pa.nb[0] * pa.nb[1] * pa.nb[2];
+    const long long kt = (long long)pa.K[0] * pa.K[1] * pa.K[2];
+    add_blocks(tabs[fzk::BT_ONE], i, 1);
+    add_blocks(tabs[fzk::BT_ATOMS256], i, (p.n + 255) / 256);
+    add_blocks(tabs[fzk::BT_COLUMNS], i, p.ncol[0] * p.ncol[1]);
+    add_blocks(tabs[fzk::BT_SLOTS256], i, (p.nslots + 255) / 256);
+    add_blocks(tabs[fzk::BT_BLOCKS8], i, (p.nslots / 32 + 7) / 8);
+    add_blocks(tabs[fzk::BT_NB], i, std::max(1, std::min(e->nb_grid, (p.n + 2047) / 2048)));
+    add_blocks(tabs[fzk::BT_BONDED], i, fzk::bonded_blocks(bd.back()));
+    add_blocks(tabs[fzk::BT_BRICKS256], i, (nbr + 255) / 256);
+    add_blocks(tabs[fzk::BT_BRICKS], i, nbr);
+    add_blocks(tabs[fzk::BT_GRID256], i, (int)std::min<long long>(64, (kt + 255) / 256));
+    bk->spread_smem = std::max(bk->spread_smem, fzk::pme_spread_smem(pa));
+    bk->max_ntypes = std::max(bk->max_ntypes, p.ntypes);
+    const fzk::IntegrateArgs ia = e->int_args();
+    for (int c = 0; c < ia.ncls; ++c) {
+      fzk::IntegrateArgs x = ia;
+      x.u_begin = ia.cls_begin[c];
+      x.u_end = ia.cls_begin[c + 1];
+      const int na = ia.cls_na[c], ncn = ia.cls_nc[c], st = (na == 3 && ncn == 3 && ia.settle) ? 1 : 0;
+      ClassAcc* acc = nullptr;
+      for (auto& q : cls)
+        if (q.na == na && q.nc == ncn && q.settle == st) acc = &q;
+      if (!acc) {
+        cls.push_back(ClassAcc{na, ncn, st, {}, {}});
+        acc = &cls.back();
+      }
+      add_blocks(acc->tab, (int)acc->args.size(), (x.u_end - x.u_begin + 127) / 128);
+      acc->args.push_back(x);
+    }
+    SizeAcc* sa = nullptr;
+    for (auto& q : sizes)
+      if (q.N == pa.K[0]) sa = &q;
+    if (!sa) {
+      sizes.push_back(SizeAcc{pa.K[0], {}, {}});
+      sa = &sizes.back();
+    }
+    add_blocks(sa->plane, i, pa.K[2]);
+    add_blocks(sa->z, i, fzk::pme_z_groups(pa));
+  }
+  fz_status r;
+  if ((r = bk->upload(rb, &bk->rb)) || (r = bk->upload(nb, &bk->nb)) || (r = bk->upload(bd, &bk->bd)) ||
+      (r = bk->upload(pme, &bk->pme)))
+    return r;
+  for (int k = 0; k < fzk::BT_COUNT; ++k) {
+    int4* d = nullptr;
+    if ((r = bk->upload(tabs[k], &d))) return r;
+    bk->t.tab[k] = d;
+    bk->t.n[k] = (int)tabs[k].size();
+  }
+  for (auto& q : cls) {
+    fzk::ClassBatch c{q.na, q.nc, q.settle, nullptr, nullptr, (int)q.tab.size()};
+    fzk::IntegrateArgs* da = nullptr;
+    int4* dt = nullptr;
+    if ((r = bk->upload(q.args, &da)) || (r = bk->upload(q.tab, &dt))) return r;
+    c.args = da;
+    c.tab = dt;
+    bk->classes.push_back(c);
+  }
+  for (auto& q : sizes) {
+    fzk::PmeSizeBatch s{q.N, nullptr, (int)q.plane.size(), nullptr, (int)q.z.size()};
+    int4 *dp = nullptr, *dz = nullptr;
+    if ((r = bk->upload(q.plane, &dp)) || (r = bk->upload(q.z, &dz))) return r;
+    s.plane_tab = dp;
+    s.z_tab = dz;
+    bk->sizes.push_back(s);
+  }
+  FZ_CUDA(cudaStreamCreateWithFlags(&bk->aux, cudaStreamNonBlocking));
+  FZ_CUDA(cudaEventCreateWithFlags(&bk->ev_fork, cudaEventDisableTiming));
+  FZ_CUDA(cudaEventCreateWithFlags(&bk->ev_join, cudaEventDisableTiming));
+  bk->launches = 2 * (long long)bk->classes.size() + fzk::kRebuildBuildLaunches + fzk::kRebuildPruneLaunches +
+                 1 + (bk->t.n[fzk::BT_BONDED] > 0 ? 1 : 0) + 7 + 3 * (long long)bk->sizes.size();
+  b->bk = std::move(bk);
+  return FZ_OK;
+}
+
+// the batched step: kick/drift (one launch per unit class), outer-list rebuild, then PME
+// on a second stream beside prune, pair and bonded kernels, then kick/RATTLE
+static void batched_step_body(fz_batch* b, cudaStream_t st) {
+  BatchKernels& k = *b->bk;
+  for (const auto& c : k.classes) fzk::launch_kick_drift_b(c, st);
+  fzk::launch_rebuild_build_b(k.rb, k.t, st);
+  cudaEventRecord(k.ev_fork, st);
+  cudaStreamWaitEvent(k.aux, k.ev_fork, 0);
+  fzk::launch_pme_b(k.pme, k.t, k.sizes.data(), (int)k.sizes.size(), k.spread_smem, k.aux);
+  fzk::launch_rebuild_prune_b(k.rb, k.t, st);
+  fzk::launch_nonbonded_b(k.nb, k.t, k.max_ntypes, st);
+  fzk::launch_bonded_b(k.bd, k.t, st);
+  cudaEventRecord(k.ev_join, k.aux);
+  cudaStreamWaitEvent(st, k.ev_join, 0);
+  for (const auto& c : k.classes) fzk::launch_kick_rattle_b(c, st);
+}
+
 static fz_status capture(fz_batch* b) {
   const int ns = (int)b->systems.size();
   fz_status r;
@@ -117,6 +282,16 @@ static fz_status capture(fz_batch* b) {
   b->ev_done.resize(ns, nullptr);
   for (auto& e : b->ev_done) FZ_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   FZ_CUDA(cudaMallocHost(&b->pinned_status, sizeof(int) * ns));
+  if (batched_kernels_ok(b)) {
+    if ((r = build_batch_kernels(b))) return r;
+    // the members' pending work (initial forces) precedes the first batched step
+    for (fz_system* s : b->systems) FZ_CUDA(cudaStreamSynchronize(s->eng->st));
+    FZ_CUDA(cudaStreamBeginCapture(b->master, cudaStreamCaptureModeThreadLocal));
+    batched_step_body(b, b->master);
+    FZ_CUDA(cudaStreamEndCapture(b->master, &b->graph));
+    FZ_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
+    return FZ_OK;
+  }
   FZ_CUDA(cudaStreamBeginCapture(b->master, cudaStreamCaptureModeThreadLocal));
   FZ_CUDA(cudaEventRecord(b->ev_start, b->master));
   cudaError_t cap = cudaSuccess;

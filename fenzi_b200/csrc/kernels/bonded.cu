@@ -55,8 +55,8 @@ __device__ __forceinline__ bool dihedral_geom(float4 ri, float4 rj, float4 rk, f
 }
 
 template <bool ENERGY>
-__global__ void __launch_bounds__(256) k_bonded(BondedArgs a) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void bonded_body(const BondedArgs& a, int bid) {
+  const int t = bid * blockDim.x + threadIdx.x;
   const int n = a.p.n;
   const SysParams& p = a.p;
   double e[7] = {0, 0, 0, 0, 0, 0, 0};  // bond angle ub dihed impr ewexcl (vdw14, elec14 below)
@@ -243,6 +243,15 @@ __global__ void __launch_bounds__(256) k_bonded(BondedArgs a) {
   }
 }
 
+template <bool ENERGY>
+__global__ void __launch_bounds__(256) k_bonded(BondedArgs a) { bonded_body<ENERGY>(a, blockIdx.x); }
+
+__global__ void __launch_bounds__(256) k_bonded_b(const BondedArgs* __restrict__ args, const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  const BondedArgs a = args[t.x];
+  bonded_body<false>(a, t.y);
+}
+
 void launch_bonded(const BondedArgs& a, bool energy, cudaStream_t st) {
   const int tot = a.nbond + a.nangle + a.nub + a.ndihe + a.nimpr + a.nexcl + a.n14;
   if (tot == 0) return;
@@ -251,6 +260,14 @@ void launch_bonded(const BondedArgs& a, bool energy, cudaStream_t st) {
     k_bonded<true><<<g, 256, 0, st>>>(a);
   else
     k_bonded<false><<<g, 256, 0, st>>>(a);
+}
+
+int bonded_blocks(const BondedArgs& a) {
+  return (a.nbond + a.nangle + a.nub + a.ndihe + a.nimpr + a.nexcl + a.n14 + 255) / 256;
+}
+
+void launch_bonded_b(const BondedArgs* args, const BatchTables& t, cudaStream_t st) {
+  if (t.n[BT_BONDED] > 0) k_bonded_b<<<t.n[BT_BONDED], 256, 0, st>>>(args, t.tab[BT_BONDED]);
 }
 
 // ---------------------------------------------------------------- consharm restraint

@@ -342,9 +342,9 @@ __device__ __forceinline__ void scale_com_velocity(const Unit& U, double v[4][3]
 // NPT (Andersen barostat step with the integration units as scaling groups): the unit
 // moves rigidly with its mass centre scaled by a.lam about the origin (the box changed
 // by a.lam), and its centre-of-mass velocity is scaled by a.vfric before the kick.
-template <bool NPT, int NA, int NC, bool SETTLE = false>
-__global__ void __launch_bounds__(128) k_kick_drift(IntegrateArgs a) {
-  const int u = a.u_begin + blockIdx.x * blockDim.x + threadIdx.x;
+template <bool NPT, int NA, int NC, bool SETTLE>
+__device__ __forceinline__ void kick_drift_body(const IntegrateArgs& a, int bid) {
+  const int u = a.u_begin + bid * blockDim.x + threadIdx.x;
   if (u >= a.u_end) return;
   const Unit U = load_unit<NA, NC>(a, u);
   const int n = a.p.n;
@@ -448,6 +448,16 @@ __global__ void __launch_bounds__(128) k_kick_drift(IntegrateArgs a) {
   if (__any_sync(am, moved) && lead) *a.flag_prune = 1;
 }
 
+template <bool NPT, int NA, int NC, bool SETTLE = false>
+__global__ void __launch_bounds__(128) k_kick_drift(IntegrateArgs a) { kick_drift_body<NPT, NA, NC, SETTLE>(a, blockIdx.x); }
+
+template <int NA, int NC, bool SETTLE>
+__global__ void __launch_bounds__(128) k_kick_drift_b(const IntegrateArgs* __restrict__ args, const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  const IntegrateArgs a = args[t.x];
+  kick_drift_body<false, NA, NC, SETTLE>(a, t.y);
+}
+
 // Group (unit) virial terms of a barostat step, after the forces: the centre-of-mass
 // kinetic energy of the half-step velocities into EN_KIN_HALF and, into the virial
 // slots, minus the intra-unit part sum_a (r_a - R_unit) . F_a, which turns the atomic
@@ -501,8 +511,8 @@ __global__ void __launch_bounds__(128) k_unit_virial(IntegrateArgs a) {
 }
 
 template <bool KIN, int NA, int NC>
-__global__ void __launch_bounds__(128) k_kick_rattle(IntegrateArgs a, int kick) {
-  const int u = a.u_begin + blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void kick_rattle_body(const IntegrateArgs& a, int kick, int bid) {
+  const int u = a.u_begin + bid * blockDim.x + threadIdx.x;
   double ke = 0.0;
   if (u < a.u_end) {
     const Unit U = load_unit<NA, NC>(a, u);
@@ -544,6 +554,16 @@ __global__ void __launch_bounds__(128) k_kick_rattle(IntegrateArgs a, int kick) 
     }
   }
   if (KIN) energy_add(a.energy + EN_KIN, ke);
+}
+
+template <bool KIN, int NA, int NC>
+__global__ void __launch_bounds__(128) k_kick_rattle(IntegrateArgs a, int kick) { kick_rattle_body<KIN, NA, NC>(a, kick, blockIdx.x); }
+
+template <int NA, int NC>
+__global__ void __launch_bounds__(128) k_kick_rattle_b(const IntegrateArgs* __restrict__ args, const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  const IntegrateArgs a = args[t.x];
+  kick_rattle_body<false, NA, NC>(a, 1, t.y);
 }
 
 __global__ void __launch_bounds__(256) k_kinetic(IntegrateArgs a) {
@@ -811,6 +831,38 @@ static void kick_drift_classes(const IntegrateArgs& a, cudaStream_t st) {
 }
 
 void launch_kick_drift(const IntegrateArgs& a, cudaStream_t st) { kick_drift_classes<false>(a, st); }
+
+// batched: one launch per unit class over every system's units of that class
+template <class F>
+static void class_dispatch(int na, int nc, F f) {
+  if (na == 1 && nc == 0) f(IC<1>(), IC<0>());
+  else if (na == 2 && nc == 1) f(IC<2>(), IC<1>());
+  else if (na == 3 && nc == 2) f(IC<3>(), IC<2>());
+  else if (na == 3 && nc == 3) f(IC<3>(), IC<3>());
+  else if (na == 4 && nc == 3) f(IC<4>(), IC<3>());
+  else f(IC<0>(), IC<0>());
+}
+
+void launch_kick_drift_b(const ClassBatch& c, cudaStream_t st) {
+  if (c.nblocks <= 0) return;
+  class_dispatch(c.na, c.nc, [&](auto na, auto nc) {
+    constexpr int NA = decltype(na)::value, NC = decltype(nc)::value;
+    if constexpr (NA == 3 && NC == 3) {
+      if (c.settle) {
+        k_kick_drift_b<3, 3, true><<<c.nblocks, 128, 0, st>>>(c.args, c.tab);
+        return;
+      }
+    }
+    k_kick_drift_b<NA, NC, false><<<c.nblocks, 128, 0, st>>>(c.args, c.tab);
+  });
+}
+
+void launch_kick_rattle_b(const ClassBatch& c, cudaStream_t st) {
+  if (c.nblocks <= 0) return;
+  class_dispatch(c.na, c.nc, [&](auto na, auto nc) {
+    k_kick_rattle_b<decltype(na)::value, decltype(nc)::value><<<c.nblocks, 128, 0, st>>>(c.args, c.tab);
+  });
+}
 
 void launch_kick_drift_npt(const IntegrateArgs& a, cudaStream_t st) { kick_drift_classes<true>(a, st); }
 

@@ -12,6 +12,28 @@ enum : int {
 constexpr int kRebuildBuildLaunches = 6;  // launch_rebuild_build
 constexpr int kRebuildPruneLaunches = 3;  // launch_rebuild_prune
 
+// Batched launches: one kernel launch covers many systems.  A block table holds one
+// int4 per launched block: (index into the launch's argument array, the block's index
+// in that system's own grid, that grid's size, 0).  Tables are built on the host from
+// the systems' sizes, one per per-system grid shape.
+enum : int {
+  BT_ONE = 0,     // one block per system
+  BT_ATOMS256,    // (n + 255) / 256
+  BT_COLUMNS,     // x-y columns of the neighbour sort
+  BT_SLOTS256,    // (sorted slots + 255) / 256
+  BT_BLOCKS8,     // (32-slot blocks + 7) / 8
+  BT_NB,          // pair-kernel CTAs
+  BT_BONDED,      // bonded-term blocks
+  BT_BRICKS256,   // (PME bricks + 255) / 256
+  BT_BRICKS,      // one block per PME brick
+  BT_GRID256,     // (K^3 + 255) / 256
+  BT_COUNT
+};
+struct BatchTables {
+  const int4* tab[BT_COUNT];
+  int n[BT_COUNT];
+};
+
 struct RebuildArgs {
   SysParams p;
   int* flag;
@@ -50,6 +72,8 @@ void launch_rebuild(const RebuildArgs& a, cudaStream_t st);
 // the two halves of launch_rebuild: the outer-list build (flag) and the prune (flag_prune)
 void launch_rebuild_build(const RebuildArgs& a, cudaStream_t st);
 void launch_rebuild_prune(const RebuildArgs& a, cudaStream_t st);
+void launch_rebuild_build_b(const RebuildArgs* args, const BatchTables& t, cudaStream_t st);
+void launch_rebuild_prune_b(const RebuildArgs* args, const BatchTables& t, cudaStream_t st);
 // one-thread kernel: graph conditional value = (*flag != 0)
 // IF-node value = (*flag || (flag2 && *flag2))
 void launch_set_condition(cudaGraphConditionalHandle h, const int* flag, const int* flag2, cudaStream_t st);
@@ -75,6 +99,7 @@ struct NonbondedArgs {
   int minb;  // CTAs per SM the kernel is built for (3 or 4)
 };
 void launch_nonbonded(const NonbondedArgs& a, bool energy, cudaStream_t st);
+void launch_nonbonded_b(const NonbondedArgs* args, const BatchTables& t, int max_ntypes, cudaStream_t st);
 
 struct PmeArgs {
   SysParams p;
@@ -99,6 +124,19 @@ struct PmeArgs {
   int* status;
 };
 void launch_pme(const PmeArgs& a, bool energy, cudaStream_t st);
+// batched PME: the systems of one grid size share the FFT launches
+struct PmeSizeBatch {
+  int N;                  // Kx = Ky (plane kernels), Kz compiled
+  const int4* plane_tab;  // (system, z plane, Kz)
+  int nplane;
+  const int4* z_tab;      // (system, z-pass group, groups)
+  int nz;
+};
+bool pme_batchable(const PmeArgs& a);
+size_t pme_spread_smem(const PmeArgs& a);
+int pme_z_groups(const PmeArgs& a);
+void launch_pme_b(const PmeArgs* args, const BatchTables& t, const PmeSizeBatch* sizes, int nsizes,
+                  size_t spread_smem, cudaStream_t st);
 int pme_launches(const PmeArgs& a);
 
 struct BondedArgs {
@@ -118,6 +156,8 @@ struct BondedArgs {
   long long* energy;
 };
 void launch_bonded(const BondedArgs& a, bool energy, cudaStream_t st);
+int bonded_blocks(const BondedArgs& a);
+void launch_bonded_b(const BondedArgs* args, const BatchTables& t, cudaStream_t st);
 
 struct IntegrateArgs {
   SysParams p;
@@ -154,6 +194,16 @@ struct IntegrateArgs {
   double vfric;  // barostat step: centre-of-mass velocity scale of the half kicks (1 = none)
 };
 // kick (F/2) + drift + SHAKE, zeroes the force accumulator, scatters sorted positions
+// the units of one class (atoms, constraints, SETTLE) across the systems of a batch:
+// args holds one IntegrateArgs per (system, class) with u_begin/u_end of that class
+struct ClassBatch {
+  int na, nc, settle;
+  const IntegrateArgs* args;
+  const int4* tab;
+  int nblocks;
+};
+void launch_kick_drift_b(const ClassBatch& c, cudaStream_t st);
+void launch_kick_rattle_b(const ClassBatch& c, cudaStream_t st);
 void launch_kick_drift(const IntegrateArgs& a, cudaStream_t st);
 // the same for a barostat step (rigid unit scaling by lam, centre-of-mass velocity
 // scale vfric)

@@ -16,10 +16,17 @@
 namespace fzk {
 
 // wrap positions into [-L/2, L/2), record build positions, bin into columns
-__global__ void k_rb_bin(SysParams p, const int* __restrict__ flag, float4* pos4, float4* pos_build, int* col_of,
-                         int* col_count, int* status) {
+__device__ __forceinline__ void rb_bin_body(const RebuildArgs& A, int bid, int nbid) {
+  const SysParams p = A.p;
+  const int* __restrict__ flag = A.flag;
+  float4* pos4 = A.pos4;
+  float4* pos_build = A.pos_build;
+  int* col_of = A.col_of;
+  int* col_count = A.col_count;
+  int* status = A.status;
+
   if (!*flag) return;
-  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  const int a = bid * blockDim.x + threadIdx.x;
   if (a >= p.n) return;
   float4 r = pos4[a];
   if (!(fabsf(r.x) < 1e7f && fabsf(r.y) < 1e7f && fabsf(r.z) < 1e7f)) {
@@ -45,9 +52,24 @@ __global__ void k_rb_bin(SysParams p, const int* __restrict__ flag, float4* pos4
   if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&col_count[c], __popc(peers));
 }
 
+__global__ void k_rb_bin(RebuildArgs a) { rb_bin_body(a, blockIdx.x, gridDim.x); }
+__global__ void k_rb_bin_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  const RebuildArgs a = args[t.x];
+  rb_bin_body(a, t.y, t.z);
+}
+
+
 // exclusive scan of the 32-padded column sizes (one block)
-__global__ void k_rb_scan(SysParams p, const int* __restrict__ flag, const int* __restrict__ col_count, int* col_start,
-                          int ncol, int* counters, int* status) {
+__device__ __forceinline__ void rb_scan_body(const RebuildArgs& A, int bid, int nbid) {
+  const SysParams p = A.p;
+  const int* __restrict__ flag = A.flag;
+  const int* __restrict__ col_count = A.col_count;
+  int* col_start = A.col_start;
+  const int ncol = A.p.ncol[0] * A.p.ncol[1];
+  int* counters = A.counters;
+  int* status = A.status;
+
   if (!*flag) return;
   __shared__ int part[1024];
   const int t = threadIdx.x, nt = blockDim.x;
@@ -77,10 +99,24 @@ __global__ void k_rb_scan(SysParams p, const int* __restrict__ flag, const int* 
   }
 }
 
-__global__ void k_rb_scatter(SysParams p, const int* __restrict__ flag, const int* __restrict__ col_of,
-                             const int* __restrict__ col_start, int* col_cursor, int* col_tmp) {
+__global__ void k_rb_scan(RebuildArgs a) { rb_scan_body(a, blockIdx.x, gridDim.x); }
+__global__ void k_rb_scan_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  const RebuildArgs a = args[t.x];
+  rb_scan_body(a, t.y, t.z);
+}
+
+
+__device__ __forceinline__ void rb_scatter_body(const RebuildArgs& A, int bid, int nbid) {
+  const SysParams p = A.p;
+  const int* __restrict__ flag = A.flag;
+  const int* __restrict__ col_of = A.col_of;
+  const int* __restrict__ col_start = A.col_start;
+  int* col_cursor = A.col_cursor;
+  int* col_tmp = A.col_tmp;
+
   if (!*flag) return;
-  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  const int a = bid * blockDim.x + threadIdx.x;
   if (a >= p.n) return;
   const int c = col_of[a];
   const unsigned peers = __match_any_sync(__activemask(), c);
@@ -93,21 +129,39 @@ __global__ void k_rb_scatter(SysParams p, const int* __restrict__ flag, const in
   if (s < p.nslots - 32) col_tmp[s] = a;
 }
 
+__global__ void k_rb_scatter(RebuildArgs a) { rb_scatter_body(a, blockIdx.x, gridDim.x); }
+__global__ void k_rb_scatter_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  const RebuildArgs a = args[t.x];
+  rb_scatter_body(a, t.y, t.z);
+}
+
+
 __device__ __forceinline__ uint32_t float_key(float f) {
   const uint32_t u = __float_as_uint(f);
   return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
 }
 
 // one block per column: bitonic sort by (z, atom id), then fill the sorted arrays
-__global__ void __launch_bounds__(256) k_rb_colsort(SysParams p, const int* __restrict__ flag, int* col_count,
-                                                    int* col_cursor,
-                                                    const int* __restrict__ col_start, const int* __restrict__ col_tmp,
-                                                    const float4* __restrict__ pos4, const int* __restrict__ type,
-                                                    int* perm, int* inv_perm, float4* xyzq_s, int* typ_s, int* blk_col,
-                                                    int* status) {
+__device__ __forceinline__ void rb_colsort_body(const RebuildArgs& A, int bid, int nbid) {
+  const SysParams p = A.p;
+  const int* __restrict__ flag = A.flag;
+  int* col_count = A.col_count;
+  int* col_cursor = A.col_cursor;
+  const int* __restrict__ col_start = A.col_start;
+  const int* __restrict__ col_tmp = A.col_tmp;
+  const float4* __restrict__ pos4 = A.pos4;
+  const int* __restrict__ type = A.type;
+  int* perm = A.perm;
+  int* inv_perm = A.inv_perm;
+  float4* xyzq_s = A.xyzq_s;
+  int* typ_s = A.typ_s;
+  int* blk_col = A.blk_col;
+  int* status = A.status;
+
   if (!*flag) return;
   extern __shared__ unsigned long long keys[];
-  const int c = blockIdx.x;
+  const int c = bid;
   const int n = col_count[c];
   const int start = col_start[c];
   // the column's count and cursor are spent: zero them for the next rebuild's binning
@@ -167,6 +221,14 @@ __global__ void __launch_bounds__(256) k_rb_colsort(SysParams p, const int* __re
   }
 }
 
+__global__ void __launch_bounds__(256) k_rb_colsort(RebuildArgs a) { rb_colsort_body(a, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(256) k_rb_colsort_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  const RebuildArgs a = args[t.x];
+  rb_colsort_body(a, t.y, t.z);
+}
+
+
 // squared distance between two boxes given center offset d and half extents
 __device__ __forceinline__ float box_gap2(float3 d, float3 h) {
   const float gx = fmaxf(0.f, fabsf(d.x) - h.x);
@@ -179,18 +241,31 @@ __device__ __forceinline__ float box_gap2(float3 d, float3 h) {
 // at every periodic image, whose position lies within rlist of block I's bounding box.
 // The diagonal block (J == I, no image) is implicit and not stored.  Entries append to
 // the block's own region outer[I * ocap ...] in a fixed order (deterministic).
-__global__ void __launch_bounds__(256) k_rb_outer(SysParams p, const int* __restrict__ flag,
-                                                  const int* __restrict__ counters, const int* __restrict__ perm,
-                                                  const float4* __restrict__ xyzq_s, const float4* __restrict__ bb_lo,
-                                                  const float4* __restrict__ bb_hi, const int* __restrict__ blk_col,
-                                                  const int* __restrict__ col_start, int dcx, int dcy, int all_images,
-                                                  uint32_t* outer, int* outer_n, int ocap,
-                                                  const int* __restrict__ xn, const int* __restrict__ xs, int xmax,
-                                                  int* status) {
+__device__ __forceinline__ void rb_outer_body(const RebuildArgs& A, int bid, int nbid) {
+  const SysParams p = A.p;
+  const int* __restrict__ flag = A.flag;
+  const int* __restrict__ counters = A.counters;
+  const int* __restrict__ perm = A.perm;
+  const float4* __restrict__ xyzq_s = A.xyzq_s;
+  const float4* __restrict__ bb_lo = A.bb_lo;
+  const float4* __restrict__ bb_hi = A.bb_hi;
+  const int* __restrict__ blk_col = A.blk_col;
+  const int* __restrict__ col_start = A.col_start;
+  int dcx = A.dcx;
+  int dcy = A.dcy;
+  int all_images = A.all_images;
+  uint32_t* outer = A.outer;
+  int* outer_n = A.outer_n;
+  int ocap = A.ocap;
+  const int* __restrict__ xn = A.xn;
+  const int* __restrict__ xs = A.xs;
+  int xmax = A.xmax;
+  int* status = A.status;
+
   if (!*flag) return;
   const int nblk = counters[CNT_SLOTS] >> 5;
   const int lane = threadIdx.x & 31;
-  const int I = blockIdx.x * 8 + (threadIdx.x >> 5);
+  const int I = bid * 8 + (threadIdx.x >> 5);
   if (I >= nblk) return;
   const float4 li = bb_lo[I], hi4 = bb_hi[I];
   const float3 ci = make_float3(0.5f * (li.x + hi4.x), 0.5f * (li.y + hi4.y), 0.5f * (li.z + hi4.z));
@@ -269,14 +344,33 @@ __global__ void __launch_bounds__(256) k_rb_outer(SysParams p, const int* __rest
   }
 }
 
+__global__ void __launch_bounds__(256) k_rb_outer(RebuildArgs a) { rb_outer_body(a, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(256) k_rb_outer_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  const RebuildArgs a = args[t.x];
+  rb_outer_body(a, t.y, t.z);
+}
+
+
 // Per slot: the partner slots of its excluded atoms (1-2, 1-3, 1-4), for the prune's
 // masks; per 32-slot block (one warp): the bounding box of its atoms
-__global__ void k_rb_slots(SysParams p, const int* __restrict__ flag, const int* __restrict__ counters,
-                           const int* __restrict__ perm, const int* __restrict__ inv_perm,
-                           const int* __restrict__ excl_off, const int* __restrict__ excl_idx, int* xn, int* xs,
-                           int xmax, const float4* __restrict__ xyzq_s, float4* bb_lo, float4* bb_hi) {
+__device__ __forceinline__ void rb_slots_body(const RebuildArgs& A, int bid, int nbid) {
+  const SysParams p = A.p;
+  const int* __restrict__ flag = A.flag;
+  const int* __restrict__ counters = A.counters;
+  const int* __restrict__ perm = A.perm;
+  const int* __restrict__ inv_perm = A.inv_perm;
+  const int* __restrict__ excl_off = A.excl_off;
+  const int* __restrict__ excl_idx = A.excl_idx;
+  int* xn = A.xn;
+  int* xs = A.xs;
+  int xmax = A.xmax;
+  const float4* __restrict__ xyzq_s = A.xyzq_s;
+  float4* bb_lo = A.bb_lo;
+  float4* bb_hi = A.bb_hi;
+
   if (!*flag) return;
-  const int sl = blockIdx.x * blockDim.x + threadIdx.x;
+  const int sl = bid * blockDim.x + threadIdx.x;
   if (sl >= p.nslots) return;  // nslots is a multiple of 32: whole warps leave together
   const int a = perm[sl];
   int m = 0;
@@ -307,9 +401,21 @@ __global__ void k_rb_slots(SysParams p, const int* __restrict__ flag, const int*
   }
 }
 
+__global__ void k_rb_slots(RebuildArgs a) { rb_slots_body(a, blockIdx.x, gridDim.x); }
+__global__ void k_rb_slots_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  const RebuildArgs a = args[t.x];
+  rb_slots_body(a, t.y, t.z);
+}
+
+
 // Closes a rebuild (counts it, lowers its flag, raises the prune flag: a new outer list
 // always gets a fresh inner list) and opens a prune (zeroes the list counters).
-__global__ void k_prune_begin(int* flag, int* flag_prune, int* counters) {
+__device__ __forceinline__ void prune_begin_body(const RebuildArgs& A, int bid, int nbid) {
+  int* flag = A.flag;
+  int* flag_prune = A.flag_prune;
+  int* counters = A.counters;
+
   if (*flag) {
     counters[CNT_REBUILDS] += 1;
     *flag = 0;
@@ -320,6 +426,14 @@ __global__ void k_prune_begin(int* flag, int* flag_prune, int* counters) {
   counters[CNT_TILES] = 0;
   counters[CNT_ITEMS] = 0;
 }
+
+__global__ void k_prune_begin(RebuildArgs a) { prune_begin_body(a, blockIdx.x, gridDim.x); }
+__global__ void k_prune_begin_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  const RebuildArgs a = args[t.x];
+  prune_begin_body(a, t.y, t.z);
+}
+
 
 // Exclusion masks of one tile (this lane holding j entry je): the lane walks the
 // excluded partners (1-2, 1-3, 1-4) of its own j slot (xs/xn: partner slots per slot,
@@ -349,20 +463,37 @@ __device__ __forceinline__ uint32_t excl_mask(int I, uint32_t je, int lane, uint
 // into full 32-entry tiles with their exclusion masks, and records the positions the
 // list was made at.  Run after every rebuild and whenever an atom has moved more than
 // delta/2 since the last prune, so no pair within rc is ever missed.
-__global__ void __launch_bounds__(256, 6) k_prune(SysParams p, const int* __restrict__ flag_prune, int* counters,
-                                               const int* __restrict__ perm, const int* __restrict__ xn,
-                                               const float4* __restrict__ xyzq_s, const int* __restrict__ xs,
-                                               int xmax, const uint32_t* __restrict__ outer,
-                                               const int* __restrict__ outer_n, uint32_t* inner, int* inner_nt,
-                                               int* inner_m, uint32_t* masks, uint32_t* dmask, int mask_cap, int ocap,
-                                               float rp2, float4* pos_prune, int2* items, int chunk, int* status) {
+__device__ __forceinline__ void prune_body(const RebuildArgs& A, int bid, int nbid) {
+  const SysParams p = A.p;
+  const int* __restrict__ flag_prune = A.flag_prune;
+  int* counters = A.counters;
+  const int* __restrict__ perm = A.perm;
+  const int* __restrict__ xn = A.xn;
+  const float4* __restrict__ xyzq_s = A.xyzq_s;
+  const int* __restrict__ xs = A.xs;
+  int xmax = A.xmax;
+  const uint32_t* __restrict__ outer = A.outer;
+  const int* __restrict__ outer_n = A.outer_n;
+  uint32_t* inner = A.inner;
+  int* inner_nt = A.inner_nt;
+  int* inner_m = A.inner_m;
+  uint32_t* masks = A.masks;
+  uint32_t* dmask = A.dmask;
+  int mask_cap = A.mask_cap;
+  int ocap = A.ocap;
+  float rp2 = A.rp2;
+  float4* pos_prune = A.pos_prune;
+  int2* items = A.items;
+  int chunk = A.chunk;
+  int* status = A.status;
+
   if (!*flag_prune) return;
   __shared__ float4 ipos_all[8][32];
   __shared__ uint32_t buf_all[8][kNG][64];
   __shared__ uint32_t msk_all[8][32];
   const int nblk = counters[CNT_SLOTS] >> 5;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int I = blockIdx.x * 8 + warp;
+  const int I = bid * 8 + warp;
   if (I >= nblk) return;
   float4* ipos = ipos_all[warp];
   uint32_t* msk = msk_all[warp];
@@ -491,11 +622,31 @@ __global__ void __launch_bounds__(256, 6) k_prune(SysParams p, const int* __rest
   }
 }
 
-__global__ void k_prune_end(int* flag_prune, int* counters) {
+__global__ void __launch_bounds__(256, 6) k_prune(RebuildArgs a) { prune_body(a, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(256, 6) k_prune_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  const RebuildArgs a = args[t.x];
+  prune_body(a, t.y, t.z);
+}
+
+
+__device__ __forceinline__ void prune_end_body(const RebuildArgs& A, int bid, int nbid) {
+  int* flag_prune = A.flag_prune;
+  int* counters = A.counters;
+
+  counters[CNT_WORK] = 0;  // the pair kernel's item counter (it always follows)
   if (!*flag_prune) return;
   counters[CNT_PRUNES] += 1;
   *flag_prune = 0;
 }
+
+__global__ void k_prune_end(RebuildArgs a) { prune_end_body(a, blockIdx.x, gridDim.x); }
+__global__ void k_prune_end_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  const RebuildArgs a = args[t.x];
+  prune_end_body(a, t.y, t.z);
+}
+
 
 // sets a graph conditional node's value from a device flag (the neighbour kernels run
 // inside an IF node only when their flag is raised)
@@ -517,30 +668,48 @@ void launch_rebuild(const RebuildArgs& a, cudaStream_t st) {
 void launch_rebuild_build(const RebuildArgs& a, cudaStream_t st) {
   const SysParams& p = a.p;
   const int ncol = p.ncol[0] * p.ncol[1];
-  k_rb_bin<<<(p.n + 255) / 256, 256, 0, st>>>(p, a.flag, a.pos4, a.pos_build, a.col_of, a.col_count, a.status);
-  k_rb_scan<<<1, 1024, 0, st>>>(p, a.flag, a.col_count, a.col_start, ncol, a.counters, a.status);
-  k_rb_scatter<<<(p.n + 255) / 256, 256, 0, st>>>(p, a.flag, a.col_of, a.col_start, a.col_cursor, a.col_tmp);
-  k_rb_colsort<<<ncol, 256, kColCap * sizeof(unsigned long long), st>>>(
-      p, a.flag, a.col_count, a.col_cursor, a.col_start, a.col_tmp, a.pos4, a.type, a.perm, a.inv_perm, a.xyzq_s,
-      a.typ_s, a.blk_col, a.status);
-  k_rb_slots<<<(p.nslots + 255) / 256, 256, 0, st>>>(p, a.flag, a.counters, a.perm, a.inv_perm, a.excl_off,
-                                                     a.excl_idx, a.xn, a.xs, a.xmax, a.xyzq_s, a.bb_lo, a.bb_hi);
   const int maxblk = (p.nslots) / 32;
-  k_rb_outer<<<(maxblk + 7) / 8, 256, 0, st>>>(p, a.flag, a.counters, a.perm, a.xyzq_s, a.bb_lo, a.bb_hi, a.blk_col,
-                                               a.col_start, a.dcx, a.dcy, a.all_images, a.outer, a.outer_n, a.ocap,
-                                               a.xn, a.xs, a.xmax,
-                                               a.status);
+  k_rb_bin<<<(p.n + 255) / 256, 256, 0, st>>>(a);
+  k_rb_scan<<<1, 1024, 0, st>>>(a);
+  k_rb_scatter<<<(p.n + 255) / 256, 256, 0, st>>>(a);
+  k_rb_colsort<<<ncol, 256, kColCap * sizeof(unsigned long long), st>>>(a);
+  k_rb_slots<<<(p.nslots + 255) / 256, 256, 0, st>>>(a);
+  k_rb_outer<<<(maxblk + 7) / 8, 256, 0, st>>>(a);
 }
 
 void launch_rebuild_prune(const RebuildArgs& a, cudaStream_t st) {
   const SysParams& p = a.p;
   const int maxblk = (p.nslots) / 32;
-  k_prune_begin<<<1, 1, 0, st>>>(a.flag, a.flag_prune, a.counters);
-  k_prune<<<(maxblk + 7) / 8, 256, 0, st>>>(p, a.flag_prune, a.counters, a.perm, a.xn, a.xyzq_s, a.xs, a.xmax,
-                                            a.outer, a.outer_n, a.inner, a.inner_nt, a.inner_m, a.masks,
-                                            a.dmask, a.mask_cap, a.ocap, a.rp2, a.pos_prune, a.items, a.chunk,
-                                            a.status);
-  k_prune_end<<<1, 1, 0, st>>>(a.flag_prune, a.counters);
+  k_prune_begin<<<1, 1, 0, st>>>(a);
+  k_prune<<<(maxblk + 7) / 8, 256, 0, st>>>(a);
+  k_prune_end<<<1, 1, 0, st>>>(a);
+}
+
+// ------------------------------------------------------------------ batched launchers
+// One launch per kernel over many systems: block b of the launch runs block t.y (of
+// t.z) of system t.x, t = tab[b]; the per-system grids are those of the launchers above.
+void rebuild_grids(const RebuildArgs& a, int* g6) {
+  const SysParams& p = a.p;
+  const int maxblk = p.nslots / 32;
+  g6[0] = (p.n + 255) / 256;          // bin, scatter
+  g6[1] = p.ncol[0] * p.ncol[1];      // colsort
+  g6[2] = (p.nslots + 255) / 256;     // slots
+  g6[3] = (maxblk + 7) / 8;           // outer, prune
+}
+
+void launch_rebuild_build_b(const RebuildArgs* args, const BatchTables& t, cudaStream_t st) {
+  k_rb_bin_b<<<t.n[BT_ATOMS256], 256, 0, st>>>(args, t.tab[BT_ATOMS256]);
+  k_rb_scan_b<<<t.n[BT_ONE], 1024, 0, st>>>(args, t.tab[BT_ONE]);
+  k_rb_scatter_b<<<t.n[BT_ATOMS256], 256, 0, st>>>(args, t.tab[BT_ATOMS256]);
+  k_rb_colsort_b<<<t.n[BT_COLUMNS], 256, kColCap * sizeof(unsigned long long), st>>>(args, t.tab[BT_COLUMNS]);
+  k_rb_slots_b<<<t.n[BT_SLOTS256], 256, 0, st>>>(args, t.tab[BT_SLOTS256]);
+  k_rb_outer_b<<<t.n[BT_BLOCKS8], 256, 0, st>>>(args, t.tab[BT_BLOCKS8]);
+}
+
+void launch_rebuild_prune_b(const RebuildArgs* args, const BatchTables& t, cudaStream_t st) {
+  k_prune_begin_b<<<t.n[BT_ONE], 1, 0, st>>>(args, t.tab[BT_ONE]);
+  k_prune_b<<<t.n[BT_BLOCKS8], 256, 0, st>>>(args, t.tab[BT_BLOCKS8]);
+  k_prune_end_b<<<t.n[BT_ONE], 1, 0, st>>>(args, t.tab[BT_ONE]);
 }
 
 }  // namespace fzk

@@ -58,6 +58,20 @@ struct PairConst {
   float dsw_k;            // 12 / (rc^2 - ron^2)
 };
 
+__host__ __device__ inline PairConst pair_const(const SysParams& p) {
+  PairConst c;
+  c.rc2 = p.rc2;
+  c.beta = p.beta;
+  c.eb2 = -p.beta * p.beta * kLog2e;
+  c.p_b = kAS_p * p.beta;
+  c.c2b = kTwoOverSqrtPi * p.beta;
+  const float d = p.rc2 - p.ron2;
+  c.sw_a = d > 0.f ? 1.f / d : 0.f;
+  c.sw_b = d > 0.f ? -p.ron2 / d : 0.f;
+  c.dsw_k = d > 0.f ? 12.f / d : 0.f;
+  return c;
+}
+
 // force/r for one pair (FP32); returns 0 outside the cutoff or when masked
 template <bool ENERGY>
 __device__ __forceinline__ float pair_force(const PairConst& c, float r2, float qq, float2 ls, bool ok, float& ev,
@@ -181,14 +195,12 @@ __device__ __forceinline__ void run_tile(const PairConst& c, const SysParams& p,
 
 // Warp per i-block (blocks taken from a dynamic counter): the diagonal tile, then the
 // block's inner tiles; the i force stays in registers across tiles and is flushed once.
-template <bool ENERGY, int MINB>
-__global__ void __launch_bounds__(256, MINB)
-    k_nonbonded(SysParams p, PairConst c, const float4* __restrict__ xyzq, const int* __restrict__ typ,
-                const int* __restrict__ perm, const uint32_t* __restrict__ inner, const int* __restrict__ inner_nt,
-                const int* __restrict__ inner_m, const uint32_t* __restrict__ dmask,
-                const uint32_t* __restrict__ masks, int* __restrict__ counters, const int2* __restrict__ items,
-                int chunk, const float2* __restrict__ ljtab, long long* __restrict__ facc,
-                long long* __restrict__ energy, int ocap) {
+template <bool ENERGY>
+__device__ __forceinline__ void nonbonded_body(const SysParams& p, const PairConst& c, const float4* __restrict__ xyzq, const int* __restrict__ typ,
+    const int* __restrict__ perm, const uint32_t* __restrict__ inner, const int* __restrict__ inner_nt,
+    const int* __restrict__ inner_m, const uint32_t* __restrict__ dmask, const uint32_t* __restrict__ masks,
+    int* __restrict__ counters, const int2* __restrict__ items, int chunk, const float2* __restrict__ ljtab,
+    long long* __restrict__ facc, long long* __restrict__ energy, int ocap) {
   extern __shared__ float2 lj[];
   __shared__ float4 jx_all[kWarps][64];
   __shared__ int jt_all[kWarps][64];
@@ -278,25 +290,44 @@ __global__ void __launch_bounds__(256, MINB)
   }
 }
 
+template <bool ENERGY, int MINB>
+__global__ void __launch_bounds__(256, MINB)
+    k_nonbonded(SysParams p, PairConst c, const float4* __restrict__ xyzq, const int* __restrict__ typ,
+                const int* __restrict__ perm, const uint32_t* __restrict__ inner, const int* __restrict__ inner_nt,
+                const int* __restrict__ inner_m, const uint32_t* __restrict__ dmask,
+                const uint32_t* __restrict__ masks, int* __restrict__ counters, const int2* __restrict__ items,
+                int chunk, const float2* __restrict__ ljtab, long long* __restrict__ facc,
+                long long* __restrict__ energy, int ocap) {
+  nonbonded_body<ENERGY>(p, c, xyzq, typ, perm, inner, inner_nt, inner_m, dmask, masks, counters, items, chunk, ljtab,
+                         facc, energy, ocap);
+}
+
+// batched: every CTA serves one system's work queue (force variant only)
+__global__ void __launch_bounds__(256, 4) k_nonbonded_b(const NonbondedArgs* __restrict__ args,
+                                                        const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  const NonbondedArgs a = args[t.x];
+  const PairConst c = pair_const(a.p);
+  nonbonded_body<false>(a.p, c, a.xyzq_s, a.typ_s, a.perm, a.inner, a.inner_nt, a.inner_m, a.dmask, a.masks,
+                        a.counters, a.items, a.chunk, a.ljtab, a.facc, a.energy, a.ocap);
+}
+
 void launch_nonbonded(const NonbondedArgs& a, bool energy, cudaStream_t st) {
   const int nt1 = a.p.ntypes + 1;
   const size_t smem = (size_t)nt1 * nt1 * sizeof(float2);
-  PairConst c;
-  c.rc2 = a.p.rc2;
-  c.beta = a.p.beta;
-  c.eb2 = -a.p.beta * a.p.beta * kLog2e;
-  c.p_b = kAS_p * a.p.beta;
-  c.c2b = kTwoOverSqrtPi * a.p.beta;
-  const float d = a.p.rc2 - a.p.ron2;
-  c.sw_a = d > 0.f ? 1.f / d : 0.f;
-  c.sw_b = d > 0.f ? -a.p.ron2 / d : 0.f;
-  c.dsw_k = d > 0.f ? 12.f / d : 0.f;
+  const PairConst c = pair_const(a.p);
   cudaMemsetAsync(a.counters + CNT_WORK, 0, sizeof(int), st);
   // 3 CTAs per SM fit 80 registers a thread; the 4-CTA build is held to 64
   auto k = energy ? (a.minb >= 4 ? k_nonbonded<true, 4> : k_nonbonded<true, 3>)
                   : (a.minb >= 4 ? k_nonbonded<false, 4> : k_nonbonded<false, 3>);
   k<<<a.grid, kWarps * 32, smem, st>>>(a.p, c, a.xyzq_s, a.typ_s, a.perm, a.inner, a.inner_nt, a.inner_m, a.dmask,
                                        a.masks, a.counters, a.items, a.chunk, a.ljtab, a.facc, a.energy, a.ocap);
+}
+
+// the work counters are zeroed by the prune's last kernel every step in batched steps
+void launch_nonbonded_b(const NonbondedArgs* args, const BatchTables& t, int max_ntypes, cudaStream_t st) {
+  const size_t smem = (size_t)(max_ntypes + 1) * (max_ntypes + 1) * sizeof(float2);
+  k_nonbonded_b<<<t.n[BT_NB], kWarps * 32, smem, st>>>(args, t.tab[BT_NB]);
 }
 
 }  // namespace fzk

@@ -58,15 +58,26 @@ __device__ __forceinline__ void bsp4(float t, float* w, float* dw) {
   }
 }
 
-__global__ void k_pme_zero(int* cnt, int* cur, int nb) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
+__device__ __forceinline__ void pme_zero_body(const PmeArgs& a, int bid, int nbid) {
+  int* cnt = a.brick_count;
+  int* cur = a.brick_cursor;
+  const int nb = a.nb[0] * a.nb[1] * a.nb[2];
+  for (int i = bid * blockDim.x + threadIdx.x; i < nb; i += nbid * blockDim.x) {
     cnt[i] = 0;
     cur[i] = 0;
   }
 }
 
-__global__ void k_pme_bin(PmeArgs a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void k_pme_zero(PmeArgs a) { pme_zero_body(a, blockIdx.x, gridDim.x); }
+__global__ void k_pme_zero_b(const PmeArgs* __restrict__ args, const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  const PmeArgs a = args[t.x];
+  pme_zero_body(a, t.y, t.z);
+}
+
+
+__device__ __forceinline__ void pme_bin_body(const PmeArgs& a, int bid, int nbid) {
+  const int i = bid * blockDim.x + threadIdx.x;
   if (i >= a.n) return;
   const float4 r = a.pos4[i];
   float t;
@@ -80,7 +91,16 @@ __global__ void k_pme_bin(PmeArgs a) {
   if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&a.brick_count[b], __popc(peers));
 }
 
-__global__ void k_pme_scan(PmeArgs a, int nbr) {
+__global__ void k_pme_bin(PmeArgs a) { pme_bin_body(a, blockIdx.x, gridDim.x); }
+__global__ void k_pme_bin_b(const PmeArgs* __restrict__ args, const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  const PmeArgs a = args[t.x];
+  pme_bin_body(a, t.y, t.z);
+}
+
+
+__device__ __forceinline__ void pme_scan_body(const PmeArgs& a, int bid, int nbid) {
+  const int nbr = a.nb[0] * a.nb[1] * a.nb[2];
   __shared__ int part[1024];
   const int t = threadIdx.x, nt = blockDim.x;
   const int per = (nbr + nt - 1) / nt;
@@ -103,8 +123,16 @@ __global__ void k_pme_scan(PmeArgs a, int nbr) {
   if (t == nt - 1) a.brick_start[nbr] = part[t];
 }
 
-__global__ void k_pme_scatter(PmeArgs a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void k_pme_scan(PmeArgs a) { pme_scan_body(a, blockIdx.x, gridDim.x); }
+__global__ void k_pme_scan_b(const PmeArgs* __restrict__ args, const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  const PmeArgs a = args[t.x];
+  pme_scan_body(a, t.y, t.z);
+}
+
+
+__device__ __forceinline__ void pme_scatter_body(const PmeArgs& a, int bid, int nbid) {
+  const int i = bid * blockDim.x + threadIdx.x;
   if (i >= a.n) return;
   const int b = a.brick_of[i];
   const unsigned peers = __match_any_sync(__activemask(), b);
@@ -115,6 +143,14 @@ __global__ void k_pme_scatter(PmeArgs a) {
   const int k = base + __popc(peers & ((1u << (threadIdx.x & 31)) - 1u));
   a.brick_atoms[a.brick_start[b] + k] = i;
 }
+
+__global__ void k_pme_scatter(PmeArgs a) { pme_scatter_body(a, blockIdx.x, gridDim.x); }
+__global__ void k_pme_scatter_b(const PmeArgs* __restrict__ args, const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  const PmeArgs a = args[t.x];
+  pme_scatter_body(a, t.y, t.z);
+}
+
 
 constexpr float kFixQ32 = 16777216.0f;  // charge grid fixed point, 2^24 per e
 
@@ -129,12 +165,12 @@ __device__ __forceinline__ float charge_at(const PmeArgs& a, size_t i) {
 // by 3 points on the low side, accumulated in shared memory with int32 fixed-point
 // atomics (2^24 per e; values stay far below +-128 e).  The region is then added to
 // the int32 charge grid; integer sums are exact, so the grid is bit-reproducible.
-__global__ void __launch_bounds__(256) k_pme_spread(PmeArgs a) {
+__device__ __forceinline__ void pme_spread_body(const PmeArgs& a, int bid, int nbid) {
   extern __shared__ int acc[];
   const int Bx = a.B[0], By = a.B[1], Bz = a.B[2];
   const int Ex = Bx + 3, Ey = By + 3, Ez = Bz + 3;
   const int nbx = a.nb[0], nby = a.nb[1];
-  const int b = blockIdx.x;
+  const int b = bid;
   const int bx = b % nbx, by = (b / nbx) % nby, bz = b / (nbx * nby);
   const int vol = Ex * Ey * Ez;
   for (int k = threadIdx.x; k < vol; k += blockDim.x) acc[k] = 0;
@@ -184,6 +220,14 @@ __global__ void __launch_bounds__(256) k_pme_spread(PmeArgs a) {
     else atomicAdd(dst, v);
   }
 }
+
+__global__ void __launch_bounds__(256) k_pme_spread(PmeArgs a) { pme_spread_body(a, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(256) k_pme_spread_b(const PmeArgs* __restrict__ args, const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  const PmeArgs a = args[t.x];
+  pme_spread_body(a, t.y, t.z);
+}
+
 
 
 // ------------------------------------------------------------------ FFT
@@ -413,8 +457,8 @@ __global__ void __launch_bounds__(256) k_fft_x_c2r(PmeArgs a, FftPlan pl, int nl
 }
 
 // one thread per atom, atoms taken in brick order so a warp reads neighbouring grid lines
-__global__ void __launch_bounds__(256) k_pme_gather(PmeArgs a) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void pme_gather_body(const PmeArgs& a, int bid, int nbid) {
+  const int t = bid * blockDim.x + threadIdx.x;
   if (t >= a.n) return;
   const int i = a.brick_atoms[t];
   const int Kx = a.K[0], Ky = a.K[1], Kz = a.K[2];
@@ -456,6 +500,14 @@ __global__ void __launch_bounds__(256) k_pme_gather(PmeArgs a) {
   red_add(a.facc + n + i, to_fix(-q * gy * (float)Ky * a.p.inv_box.y));
   red_add(a.facc + 2 * n + i, to_fix(-q * gz * (float)Kz * a.p.inv_box.z));
 }
+
+__global__ void __launch_bounds__(256) k_pme_gather(PmeArgs a) { pme_gather_body(a, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(256) k_pme_gather_b(const PmeArgs* __restrict__ args, const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  const PmeArgs a = args[t.x];
+  pme_gather_body(a, t.y, t.z);
+}
+
 
 // ------------------------------------------------------------------ compile-time FFT
 // The same Stockham autosort algorithm with the line length N a template parameter:
@@ -624,13 +676,13 @@ __global__ void __launch_bounds__(256) k_fft_y_t(PmeArgs a, int) {
 }
 
 template <int N, bool ENERGY>
-__global__ void __launch_bounds__(256) k_fft_z_conv_t(PmeArgs a, int) {
+__device__ __forceinline__ void fft_z_conv_body(const PmeArgs& a, int bid) {
   constexpr int nl = fft_lines_per_block(N);
   extern __shared__ float2 sm[];
   constexpr int LD = N + 1;
   const int Kx = a.K[0], Ky = a.K[1], Kxh = Kx / 2 + 1;
   const int ng = (Kxh + nl - 1) / nl;
-  const int y = blockIdx.x / ng, mx0 = (blockIdx.x % ng) * nl;
+  const int y = bid / ng, mx0 = (bid % ng) * nl;
   float2* tw = sm;
   float2* A = sm + N;
   float2* B = A + nl * LD;
@@ -681,6 +733,16 @@ __global__ void __launch_bounds__(256) k_fft_z_conv_t(PmeArgs a, int) {
     energy_add(a.energy + EN_VIR_Z, w2);
   }
 }
+
+template <int N, bool ENERGY>
+__global__ void __launch_bounds__(256) k_fft_z_conv_t(PmeArgs a, int) { fft_z_conv_body<N, ENERGY>(a, blockIdx.x); }
+template <int N>
+__global__ void __launch_bounds__(256) k_fft_z_conv_b(const PmeArgs* __restrict__ args, const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  const PmeArgs a = args[t.x];
+  fft_z_conv_body<N, false>(a, t.y);
+}
+
 
 // Inverse of the pairing above: Z(m) = X0(m) + i X1(m) over the full line (Hermitian
 // extension for m > N/2) transforms back to row 2p + i row 2p+1.
@@ -774,28 +836,31 @@ __device__ __forceinline__ float2* fft_run_g(float2* a, float2* b, const float2*
   }
 }
 
+// rows pair up as (2l, 2l+1); an odd N leaves the last line with one row and a zero
+template <int N>
+__host__ __device__ constexpr int plane_words() {
+  constexpr int NH = N / 2 + 1, LD = N + 1, NP = (N + 1) / 2;
+  return (N * NH > NP * LD) ? N * NH : NP * LD;
+}
 template <int N>
 constexpr size_t plane_smem_bytes() {
-  constexpr int NH = N / 2 + 1, LD = N + 1;
-  constexpr int words = (N * NH > (N / 2) * LD) ? N * NH : (N / 2) * LD;
-  return (size_t)(N + 2 * words) * sizeof(float2);
+  return (size_t)(N + 2 * plane_words<N>()) * sizeof(float2);
 }
 
 // forward: real plane z -> half spectrum along x, full spectrum along y, cgrid[z][y][mx]
 template <int N>
-__global__ void __launch_bounds__(kPlaneThreads) k_fft_xy_plane(PmeArgs a) {
+__device__ __forceinline__ void fft_xy_plane_body(const PmeArgs& a, int z) {
   extern __shared__ float2 sm[];
-  constexpr int LD = N + 1, NH = N / 2 + 1, NP = N / 2;
-  constexpr int words = (N * NH > NP * LD) ? N * NH : NP * LD;
+  constexpr int LD = N + 1, NH = N / 2 + 1, NP = (N + 1) / 2, W = plane_words<N>();
   float2* tw = sm;
   float2* A = sm + N;
-  float2* B = A + words;
+  float2* B = A + W;
   load_tw(tw, a.tw[0], N);
-  const int z = blockIdx.x;
   const size_t row0 = (size_t)z * N;
   for (int idx = threadIdx.x; idx < NP * N; idx += kPlaneThreads) {
     const int l = idx / N, x = idx - l * N;
-    A[l * LD + x] = make_float2(charge_at(a, (row0 + 2 * l) * N + x), charge_at(a, (row0 + 2 * l + 1) * N + x));
+    A[l * LD + x] = make_float2(charge_at(a, (row0 + 2 * l) * N + x),
+                                2 * l + 1 < N ? charge_at(a, (row0 + 2 * l + 1) * N + x) : 0.f);
   }
   __syncthreads();
   float2* R = fft_run_g<N, 0, 1, false, 1, LD, NP>(A, B, tw);
@@ -804,7 +869,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fft_xy_plane(PmeArgs a) {
     const int l = idx / NH, m = idx - l * NH;
     const float2 u = R[l * LD + m], w = R[l * LD + (m == 0 ? 0 : N - m)];
     P[(2 * l) * NH + m] = make_float2(0.5f * (u.x + w.x), 0.5f * (u.y - w.y));
-    P[(2 * l + 1) * NH + m] = make_float2(0.5f * (u.y + w.y), 0.5f * (w.x - u.x));
+    if (2 * l + 1 < N) P[(2 * l + 1) * NH + m] = make_float2(0.5f * (u.y + w.y), 0.5f * (w.x - u.x));
   }
   __syncthreads();
   // the y twiddles equal the x twiddles (Kx = Ky)
@@ -815,15 +880,13 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fft_xy_plane(PmeArgs a) {
 // inverse: cgrid[z][y][mx] -> inverse y, then two rows per complex line through the
 // inverse x transform -> real potential plane z
 template <int N>
-__global__ void __launch_bounds__(kPlaneThreads) k_fft_yx_plane(PmeArgs a) {
+__device__ __forceinline__ void fft_yx_plane_body(const PmeArgs& a, int z) {
   extern __shared__ float2 sm[];
-  constexpr int LD = N + 1, NH = N / 2 + 1, NP = N / 2;
-  constexpr int words = (N * NH > NP * LD) ? N * NH : NP * LD;
+  constexpr int LD = N + 1, NH = N / 2 + 1, NP = (N + 1) / 2, W = plane_words<N>();
   float2* tw = sm;
   float2* A = sm + N;
-  float2* B = A + words;
+  float2* B = A + W;
   load_tw(tw, a.tw[0], N);
-  const int z = blockIdx.x;
   const size_t row0 = (size_t)z * N;
   for (int idx = threadIdx.x; idx < N * NH; idx += kPlaneThreads) A[idx] = a.cgrid[row0 * NH + idx];
   __syncthreads();
@@ -833,7 +896,8 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fft_yx_plane(PmeArgs a) {
     const int l = idx / N, m = idx - l * N;
     const bool lo = m < NH;
     const int mm = lo ? m : N - m;
-    float2 x0 = Q[(2 * l) * NH + mm], x1 = Q[(2 * l + 1) * NH + mm];
+    float2 x0 = Q[(2 * l) * NH + mm];
+    float2 x1 = 2 * l + 1 < N ? Q[(2 * l + 1) * NH + mm] : make_float2(0.f, 0.f);
     if (!lo) {
       x0.y = -x0.y;
       x1.y = -x1.y;
@@ -846,8 +910,27 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fft_yx_plane(PmeArgs a) {
     const int l = idx / N, x = idx - l * N;
     const float2 v = R[l * LD + x];
     a.grid[(row0 + 2 * l) * N + x] = v.x;
-    a.grid[(row0 + 2 * l + 1) * N + x] = v.y;
+    if (2 * l + 1 < N) a.grid[(row0 + 2 * l + 1) * N + x] = v.y;
   }
+}
+
+template <int N>
+__global__ void __launch_bounds__(kPlaneThreads) k_fft_xy_plane(PmeArgs a) { fft_xy_plane_body<N>(a, blockIdx.x); }
+template <int N>
+__global__ void __launch_bounds__(kPlaneThreads) k_fft_yx_plane(PmeArgs a) { fft_yx_plane_body<N>(a, blockIdx.x); }
+template <int N>
+__global__ void __launch_bounds__(kPlaneThreads) k_fft_xy_plane_b(const PmeArgs* __restrict__ args,
+                                                                  const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  const PmeArgs a = args[t.x];
+  fft_xy_plane_body<N>(a, t.y);
+}
+template <int N>
+__global__ void __launch_bounds__(kPlaneThreads) k_fft_yx_plane_b(const PmeArgs* __restrict__ args,
+                                                                  const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  const PmeArgs a = args[t.x];
+  fft_yx_plane_body<N>(a, t.y);
 }
 
 #define FZ_FFT_SIZES(X) X(16) X(18) X(20) X(24) X(25) X(27) X(30) X(32) X(36) X(40) X(48) X(64) X(80) X(96) X(128)
@@ -884,8 +967,8 @@ static bool fft_z_t(const PmeArgs& a, int nl, bool energy, dim3 g, size_t sm, cu
   }
   return false;
 }
-// plane kernels for cubic-in-xy grids of even size (row pairs); false if not available
-#define FZ_PLANE_SIZES(X) X(16) X(18) X(20) X(24) X(30) X(32) X(36) X(40) X(48) X(64) X(80) X(96) X(128)
+// plane kernels for grids with Kx = Ky of the compiled sizes; false if not available
+#define FZ_PLANE_SIZES(X) X(16) X(18) X(20) X(24) X(25) X(27) X(30) X(32) X(36) X(40) X(48) X(64) X(80) X(96) X(128)
 static bool use_plane_fft(const PmeArgs& a) {
   static const bool on = !std::getenv("FZ_PLANE_FFT") || std::atoi(std::getenv("FZ_PLANE_FFT")) != 0;
   if (!on || a.K[0] != a.K[1]) return false;
@@ -916,6 +999,15 @@ static void fft_plane(const PmeArgs& a, bool inverse, cudaStream_t st) {
   }
 }
 
+static bool fft_size_compiled(int n) {
+  switch (n) {
+#define FZ_C(N) case N: return true;
+    FZ_FFT_SIZES(FZ_C)
+#undef FZ_C
+  }
+  return false;
+}
+
 static bool fft_x_c2r_t(const PmeArgs& a, int nl, dim3 g, size_t sm, cudaStream_t st) {
   switch (a.K[0]) {
 #define FZ_C(N) case N: k_fft_x_c2r_t<N><<<g, 256, sm, st>>>(a, nl); return true;
@@ -943,9 +1035,9 @@ int pme_launches(const PmeArgs& a) { return 5 + (use_plane_fft(a) ? 3 : 5) + 1; 
 
 void launch_pme(const PmeArgs& a, bool energy, cudaStream_t st) {
   const int nbr = a.nb[0] * a.nb[1] * a.nb[2];
-  k_pme_zero<<<(nbr + 255) / 256, 256, 0, st>>>(a.brick_count, a.brick_cursor, nbr);
+  k_pme_zero<<<(nbr + 255) / 256, 256, 0, st>>>(a);
   k_pme_bin<<<(a.n + 255) / 256, 256, 0, st>>>(a);
-  k_pme_scan<<<1, 1024, 0, st>>>(a, nbr);
+  k_pme_scan<<<1, 1024, 0, st>>>(a);
   k_pme_scatter<<<(a.n + 255) / 256, 256, 0, st>>>(a);
   const size_t sp = (size_t)(a.B[0] + 3) * (a.B[1] + 3) * (a.B[2] + 3) * sizeof(int);
   cudaMemsetAsync(a.grid, 0, (size_t)a.K[0] * a.K[1] * a.K[2] * sizeof(float), st);
@@ -980,6 +1072,60 @@ void launch_pme(const PmeArgs& a, bool energy, cudaStream_t st) {
     if (!fft_x_c2r_t(a, lx, gx2, smx, st)) k_fft_x_c2r<<<gx, 256, smx, st>>>(a, px, lx);
   }
   k_pme_gather<<<(a.n + 255) / 256, 256, 0, st>>>(a);
+}
+
+// ------------------------------------------------------------------ batched PME
+// zeroes the int32 charge grid of each system (the memset of the single-system path)
+__global__ void k_grid_zero_b(const PmeArgs* __restrict__ args, const int4* __restrict__ tab) {
+  const int4 t = tab[blockIdx.x];
+  const PmeArgs a = args[t.x];
+  const size_t kt = (size_t)a.K[0] * a.K[1] * a.K[2];
+  int* g = reinterpret_cast<int*>(a.grid);
+  for (size_t i = (size_t)t.y * blockDim.x + threadIdx.x; i < kt; i += (size_t)t.z * blockDim.x) g[i] = 0;
+}
+
+size_t pme_spread_smem(const PmeArgs& a) {
+  return (size_t)(a.B[0] + 3) * (a.B[1] + 3) * (a.B[2] + 3) * sizeof(int);
+}
+int pme_z_groups(const PmeArgs& a) {
+  const int nl = fft_lines_per_block(a.K[2]);
+  return a.K[1] * ((a.K[0] / 2 + 1 + nl - 1) / nl);
+}
+bool pme_batchable(const PmeArgs& a) { return use_plane_fft(a) && a.K[2] == a.K[0]; }
+
+void launch_pme_b(const PmeArgs* args, const BatchTables& t, const PmeSizeBatch* sizes, int nsizes,
+                  size_t spread_smem, cudaStream_t st) {
+  k_pme_zero_b<<<t.n[BT_BRICKS256], 256, 0, st>>>(args, t.tab[BT_BRICKS256]);
+  k_pme_bin_b<<<t.n[BT_ATOMS256], 256, 0, st>>>(args, t.tab[BT_ATOMS256]);
+  k_pme_scan_b<<<t.n[BT_ONE], 1024, 0, st>>>(args, t.tab[BT_ONE]);
+  k_pme_scatter_b<<<t.n[BT_ATOMS256], 256, 0, st>>>(args, t.tab[BT_ATOMS256]);
+  k_grid_zero_b<<<t.n[BT_GRID256], 256, 0, st>>>(args, t.tab[BT_GRID256]);
+  k_pme_spread_b<<<t.n[BT_BRICKS], 256, spread_smem, st>>>(args, t.tab[BT_BRICKS]);
+  for (int pass = 0; pass < 3; ++pass)
+    for (int k = 0; k < nsizes; ++k) {
+      const PmeSizeBatch& b = sizes[k];
+      switch (b.N) {
+#define FZ_C(N)                                                                                        \
+  case N: {                                                                                            \
+    constexpr size_t sm = plane_smem_bytes<N>();                                                       \
+    static const bool attr = [] {                                                                      \
+      cudaFuncSetAttribute(k_fft_xy_plane_b<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
+      cudaFuncSetAttribute(k_fft_yx_plane_b<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
+      return true;                                                                                     \
+    }();                                                                                               \
+    (void)attr;                                                                                        \
+    constexpr int nl = fft_lines_per_block(N);                                                         \
+    constexpr size_t smz = (size_t)(N + 2 * nl * (N + 1)) * sizeof(float2);                           \
+    if (pass == 0) k_fft_xy_plane_b<N><<<b.nplane, kPlaneThreads, sm, st>>>(args, b.plane_tab);       \
+    if (pass == 1) k_fft_z_conv_b<N><<<b.nz, 256, smz, st>>>(args, b.z_tab);                           \
+    if (pass == 2) k_fft_yx_plane_b<N><<<b.nplane, kPlaneThreads, sm, st>>>(args, b.plane_tab);       \
+    break;                                                                                             \
+  }
+        FZ_PLANE_SIZES(FZ_C)
+#undef FZ_C
+      }
+    }
+  k_pme_gather_b<<<t.n[BT_ATOMS256], 256, 0, st>>>(args, t.tab[BT_ATOMS256]);
 }
 
 }  // namespace fzk
