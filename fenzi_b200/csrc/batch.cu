@@ -35,8 +35,22 @@ using namespace fz;
 // Batched kernels: one launch per kernel of the step covers every member.  The members'
 // kernel arguments live in device arrays, and a block table per grid shape maps each
 // launched block to (member, block of that member's own grid, grid size).
+// Device storage of the arrays lives in a grow-only arena of the batch (members join and
+// leave often in serving: no allocation, free or synchronisation per membership change);
+// the host images are staged in pinned memory and copied with one asynchronous copy.
+struct BatchArena {
+  void* dev = nullptr;
+  void* host = nullptr;  // pinned
+  size_t cap = 0;
+  ~BatchArena() {
+    if (dev) cudaFree(dev);
+    if (host) cudaFreeHost(host);
+  }
+};
+
 struct BatchKernels {
-  std::vector<void*> allocs;
+  std::vector<char> image;                        // host image of every array
+  std::vector<std::pair<size_t, void**>> fixups;  // (offset, pointer to set) per array
   fzk::RebuildArgs* rb = nullptr;
   fzk::NonbondedArgs* nb = nullptr;
   fzk::BondedArgs* bd = nullptr;
@@ -46,21 +60,33 @@ struct BatchKernels {
   std::vector<fzk::PmeSizeBatch> sizes;
   size_t spread_smem = 0;
   int max_ntypes = 0;
-  cudaStream_t aux = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   long long launches = 0;  // kernels one batched step launches
-  ~BatchKernels() {
-    for (void* p : allocs) cudaFree(p);
-    if (ev_fork) cudaEventDestroy(ev_fork);
-    if (ev_join) cudaEventDestroy(ev_join);
-    if (aux) cudaStreamDestroy(aux);
-  }
+  // appends v to the image (256-byte aligned); *out is set once the arena is known
   template <class X> fz_status upload(const std::vector<X>& v, X** out) {
-    void* p = nullptr;
-    FZ_CUDA(cudaMalloc(&p, std::max<size_t>(1, v.size()) * sizeof(X)));
-    allocs.push_back(p);
-    if (!v.empty()) FZ_CUDA(cudaMemcpy(p, v.data(), v.size() * sizeof(X), cudaMemcpyHostToDevice));
-    *out = (X*)p;
+    const size_t off = (image.size() + 255) & ~(size_t)255;
+    image.resize(off + std::max<size_t>(1, v.size()) * sizeof(X));
+    if (!v.empty()) std::memcpy(image.data() + off, v.data(), v.size() * sizeof(X));
+    fixups.push_back({off, (void**)out});
+    return FZ_OK;
+  }
+  // places the image in the arena (growing it if needed) and queues its copy on st
+  fz_status place(BatchArena& ar, cudaStream_t st) {
+    if (image.size() > ar.cap) {
+      FZ_CUDA(cudaStreamSynchronize(st));
+      if (ar.dev) FZ_CUDA(cudaFree(ar.dev));
+      if (ar.host) FZ_CUDA(cudaFreeHost(ar.host));
+      ar.dev = ar.host = nullptr;
+      ar.cap = 0;
+      const size_t cap = image.size() + image.size() / 2 + 4096;
+      FZ_CUDA(cudaMalloc(&ar.dev, cap));
+      FZ_CUDA(cudaMallocHost(&ar.host, cap));
+      ar.cap = cap;
+    } else {
+      FZ_CUDA(cudaStreamSynchronize(st));  // the previous image's copy has been read
+    }
+    std::memcpy(ar.host, image.data(), image.size());
+    FZ_CUDA(cudaMemcpyAsync(ar.dev, ar.host, image.size(), cudaMemcpyHostToDevice, st));
+    for (auto& f : fixups) *f.second = (char*)ar.dev + f.first;
     return FZ_OK;
   }
 };
@@ -76,6 +102,9 @@ struct fz_batch {
   int* pinned_status = nullptr;
   long long steps = 0;
   std::unique_ptr<BatchKernels> bk;
+  BatchArena arena;
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   void drop_graph() {
     bk.reset();
     if (exec) cudaGraphExecDestroy(exec);
@@ -90,6 +119,9 @@ struct fz_batch {
   ~fz_batch() {
     if (master) cudaStreamSynchronize(master);
     drop_graph();
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (aux) cudaStreamDestroy(aux);
     if (ev_start) cudaEventDestroy(ev_start);
     if (ev_master) cudaEventDestroy(ev_master);
     if (master) cudaStreamDestroy(master);
@@ -161,6 +193,10 @@ static fz_status build_batch_kernels(fz_batch* b) {
   std::vector<ClassAcc> cls;
   struct SizeAcc { int N; std::vector<int4> plane, z; };
   std::vector<SizeAcc> sizes;
+  // pair-kernel CTAs: the batch's total is that of one large system (nb_grid, ~4 per
+  // SM), shared out in proportion to the members' atoms, at least one each
+  long long natoms = 0;
+  for (const fz_system* s : b->systems) natoms += s->top.n;
   for (int i = 0; i < ns; ++i) {
     Engine* e = b->systems[i]->eng;
     rb.push_back(e->rebuild_args());
@@ -176,7 +212,8 @@ static fz_status build_batch_kernels(fz_batch* b) {
     add_blocks(tabs[fzk::BT_COLUMNS], i, p.ncol[0] * p.ncol[1]);
     add_blocks(tabs[fzk::BT_SLOTS256], i, (p.nslots + 255) / 256);
     add_blocks(tabs[fzk::BT_BLOCKS8], i, (p.nslots / 32 + 7) / 8);
-    add_blocks(tabs[fzk::BT_NB], i, std::max(1, std::min(e->nb_grid, (p.n + 2047) / 2048)));
+    add_blocks(tabs[fzk::BT_NB], i,
+               std::max(1, (int)std::lround((double)e->nb_grid * p.n / (double)std::max(1LL, natoms))));
     add_blocks(tabs[fzk::BT_BONDED], i, fzk::bonded_blocks(bd.back()));
     add_blocks(tabs[fzk::BT_BRICKS256], i, (nbr + 255) / 256);
     add_blocks(tabs[fzk::BT_BRICKS], i, nbr);
@@ -214,31 +251,33 @@ static fz_status build_batch_kernels(fz_batch* b) {
       (r = bk->upload(pme, &bk->pme)))
     return r;
   for (int k = 0; k < fzk::BT_COUNT; ++k) {
-    int4* d = nullptr;
-    if ((r = bk->upload(tabs[k], &d))) return r;
-    bk->t.tab[k] = d;
+    if ((r = bk->upload(tabs[k], const_cast<int4**>(&bk->t.tab[k])))) return r;
     bk->t.n[k] = (int)tabs[k].size();
   }
-  for (auto& q : cls) {
-    fzk::ClassBatch c{q.na, q.nc, q.settle, nullptr, nullptr, (int)q.tab.size()};
-    fzk::IntegrateArgs* da = nullptr;
-    int4* dt = nullptr;
-    if ((r = bk->upload(q.args, &da)) || (r = bk->upload(q.tab, &dt))) return r;
-    c.args = da;
-    c.tab = dt;
-    bk->classes.push_back(c);
+  // the pointers in these structs are set when the image is placed: their addresses
+  // must stay put, so the vectors are sized first
+  bk->classes.resize(cls.size());
+  for (size_t k = 0; k < cls.size(); ++k) {
+    const auto& q = cls[k];
+    bk->classes[k] = fzk::ClassBatch{q.na, q.nc, q.settle, nullptr, nullptr, (int)q.tab.size()};
+    if ((r = bk->upload(q.args, const_cast<fzk::IntegrateArgs**>(&bk->classes[k].args))) ||
+        (r = bk->upload(q.tab, const_cast<int4**>(&bk->classes[k].tab))))
+      return r;
   }
-  for (auto& q : sizes) {
-    fzk::PmeSizeBatch s{q.N, nullptr, (int)q.plane.size(), nullptr, (int)q.z.size()};
-    int4 *dp = nullptr, *dz = nullptr;
-    if ((r = bk->upload(q.plane, &dp)) || (r = bk->upload(q.z, &dz))) return r;
-    s.plane_tab = dp;
-    s.z_tab = dz;
-    bk->sizes.push_back(s);
+  bk->sizes.resize(sizes.size());
+  for (size_t k = 0; k < sizes.size(); ++k) {
+    const auto& q = sizes[k];
+    bk->sizes[k] = fzk::PmeSizeBatch{q.N, nullptr, (int)q.plane.size(), nullptr, (int)q.z.size()};
+    if ((r = bk->upload(q.plane, const_cast<int4**>(&bk->sizes[k].plane_tab))) ||
+        (r = bk->upload(q.z, const_cast<int4**>(&bk->sizes[k].z_tab))))
+      return r;
   }
-  FZ_CUDA(cudaStreamCreateWithFlags(&bk->aux, cudaStreamNonBlocking));
-  FZ_CUDA(cudaEventCreateWithFlags(&bk->ev_fork, cudaEventDisableTiming));
-  FZ_CUDA(cudaEventCreateWithFlags(&bk->ev_join, cudaEventDisableTiming));
+  if (!b->aux) {
+    FZ_CUDA(cudaStreamCreateWithFlags(&b->aux, cudaStreamNonBlocking));
+    FZ_CUDA(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+    FZ_CUDA(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
+  }
+  if ((r = bk->place(b->arena, b->master))) return r;
   bk->launches = 2 * (long long)bk->classes.size() + fzk::kRebuildBuildLaunches + fzk::kRebuildPruneLaunches +
                  1 + (bk->t.n[fzk::BT_BONDED] > 0 ? 1 : 0) + 7 + 3 * (long long)bk->sizes.size();
   b->bk = std::move(bk);
@@ -251,14 +290,14 @@ static void batched_step_body(fz_batch* b, cudaStream_t st) {
   BatchKernels& k = *b->bk;
   for (const auto& c : k.classes) fzk::launch_kick_drift_b(c, st);
   fzk::launch_rebuild_build_b(k.rb, k.t, st);
-  cudaEventRecord(k.ev_fork, st);
-  cudaStreamWaitEvent(k.aux, k.ev_fork, 0);
-  fzk::launch_pme_b(k.pme, k.t, k.sizes.data(), (int)k.sizes.size(), k.spread_smem, k.aux);
+  cudaEventRecord(b->ev_fork, st);
+  cudaStreamWaitEvent(b->aux, b->ev_fork, 0);
+  fzk::launch_pme_b(k.pme, k.t, k.sizes.data(), (int)k.sizes.size(), k.spread_smem, b->aux);
   fzk::launch_rebuild_prune_b(k.rb, k.t, st);
   fzk::launch_nonbonded_b(k.nb, k.t, k.max_ntypes, st);
   fzk::launch_bonded_b(k.bd, k.t, st);
-  cudaEventRecord(k.ev_join, k.aux);
-  cudaStreamWaitEvent(st, k.ev_join, 0);
+  cudaEventRecord(b->ev_join, b->aux);
+  cudaStreamWaitEvent(st, b->ev_join, 0);
   for (const auto& c : k.classes) fzk::launch_kick_rattle_b(c, st);
 }
 
@@ -284,8 +323,6 @@ static fz_status capture(fz_batch* b) {
   FZ_CUDA(cudaMallocHost(&b->pinned_status, sizeof(int) * ns));
   if (batched_kernels_ok(b)) {
     if ((r = build_batch_kernels(b))) return r;
-    // the members' pending work (initial forces) precedes the first batched step
-    for (fz_system* s : b->systems) FZ_CUDA(cudaStreamSynchronize(s->eng->st));
     FZ_CUDA(cudaStreamBeginCapture(b->master, cudaStreamCaptureModeThreadLocal));
     batched_step_body(b, b->master);
     FZ_CUDA(cudaStreamEndCapture(b->master, &b->graph));

@@ -933,7 +933,9 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fft_yx_plane_b(const PmeArgs*
   fft_yx_plane_body<N>(a, t.y);
 }
 
-#define FZ_FFT_SIZES(X) X(16) X(18) X(20) X(24) X(25) X(27) X(30) X(32) X(36) X(40) X(48) X(64) X(80) X(96) X(128)
+#define FZ_FFT_SIZES(X) \
+  X(16) X(18) X(20) X(24) X(25) X(27) X(30) X(32) X(36) X(40) X(45) X(48) X(50) X(54) X(60) X(64) X(72) X(80) \
+  X(90) X(96) X(100) X(108) X(120) X(128)
 
 static bool fft_x_r2c_t(const PmeArgs& a, int nl, dim3 g, size_t sm, cudaStream_t st) {
   switch (a.K[0]) {
@@ -968,7 +970,7 @@ static bool fft_z_t(const PmeArgs& a, int nl, bool energy, dim3 g, size_t sm, cu
   return false;
 }
 // plane kernels for grids with Kx = Ky of the compiled sizes; false if not available
-#define FZ_PLANE_SIZES(X) X(16) X(18) X(20) X(24) X(25) X(27) X(30) X(32) X(36) X(40) X(48) X(64) X(80) X(96) X(128)
+#define FZ_PLANE_SIZES(X) FZ_FFT_SIZES(X)
 static bool use_plane_fft(const PmeArgs& a) {
   static const bool on = !std::getenv("FZ_PLANE_FFT") || std::atoi(std::getenv("FZ_PLANE_FFT")) != 0;
   if (!on || a.K[0] != a.K[1]) return false;

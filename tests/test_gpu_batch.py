@@ -35,3 +35,36 @@ def test_batch_matches_each_system_alone():
     b.close()
     for s in alone + mixed:
         s.close()
+
+
+def test_batched_kernels_match_per_system_branches():
+    """The batched kernels (one launch per kernel over all members) and the graph of
+    per-member branches give bit-identical trajectories, on members with chains (free-
+    atom and bonded-term classes besides rigid water) and odd grid sizes (25, 27)."""
+    specs = [dict(nw=300, nchains=2, chain_len=10, box=24.0, kgrid=25),
+             dict(nw=420, nchains=0, box=25.5, kgrid=27),
+             dict(nw=260, nchains=1, chain_len=12, box=22.0, kgrid=24),
+             dict(nw=500, nchains=3, chain_len=8, box=27.0, kgrid=32)]
+    tmp = tempfile.mkdtemp(prefix="fzbk_")
+    runs = {}
+    for mode in ("1", "0"):
+        old = os.environ.get("FZ_BATCH_KERNELS")
+        os.environ["FZ_BATCH_KERNELS"] = mode
+        try:
+            sys_ = [_load(gen_system.build(name="custom", rc=9.0, ron=7.5, seed=40 + i, **sp),
+                          os.path.join(tmp, f"{mode}_{i}")) for i, sp in enumerate(specs)]
+            b = fz.Batch(sys_)
+            b.step(30)
+            runs[mode] = [(s.positions(), s.velocities(), s.forces_fixed()) for s in sys_]
+            b.close()
+            for s in sys_:
+                s.close()
+        finally:
+            if old is None:
+                os.environ.pop("FZ_BATCH_KERNELS", None)
+            else:
+                os.environ["FZ_BATCH_KERNELS"] = old
+    for (p1, v1, f1), (p0, v0, f0) in zip(runs["1"], runs["0"]):
+        assert np.array_equal(p1, p0)
+        assert np.array_equal(v1, v0)
+        assert np.array_equal(f1, f0)
