@@ -56,6 +56,7 @@ __device__ __forceinline__ bool dihedral_geom(float4 ri, float4 rj, float4 rk, f
 
 template <bool ENERGY>
 __device__ __forceinline__ void bonded_body(const BondedArgs& a, int bid) {
+  griddep_wait();
   const int t = bid * blockDim.x + threadIdx.x;
   const int n = a.p.n;
   const SysParams& p = a.p;
@@ -244,9 +245,9 @@ __device__ __forceinline__ void bonded_body(const BondedArgs& a, int bid) {
 }
 
 template <bool ENERGY>
-__global__ void __launch_bounds__(256) k_bonded(BondedArgs a) { bonded_body<ENERGY>(a, blockIdx.x); }
+__global__ void __launch_bounds__(256) k_bonded(BondedArgs a) { griddep_wait(); bonded_body<ENERGY>(a, blockIdx.x); }
 
-__global__ void __launch_bounds__(256) k_bonded_b(const BondedArgs* __restrict__ args, const int4* __restrict__ tab) {
+__global__ void __launch_bounds__(256) k_bonded_b(const BondedArgs* __restrict__ args, const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const BondedArgs a = args[t.x];
   bonded_body<false>(a, t.y);
@@ -257,9 +258,9 @@ void launch_bonded(const BondedArgs& a, bool energy, cudaStream_t st) {
   if (tot == 0) return;
   const int g = (tot + 255) / 256;
   if (energy)
-    k_bonded<true><<<g, 256, 0, st>>>(a);
+    launch_pdl(k_bonded<true>, dim3(g), dim3(256), 0, st, a);
   else
-    k_bonded<false><<<g, 256, 0, st>>>(a);
+    launch_pdl(k_bonded<false>, dim3(g), dim3(256), 0, st, a);
 }
 
 int bonded_blocks(const BondedArgs& a) {
@@ -267,7 +268,7 @@ int bonded_blocks(const BondedArgs& a) {
 }
 
 void launch_bonded_b(const BondedArgs* args, const BatchTables& t, cudaStream_t st) {
-  if (t.n[BT_BONDED] > 0) k_bonded_b<<<t.n[BT_BONDED], 256, 0, st>>>(args, t.tab[BT_BONDED]);
+  if (t.n[BT_BONDED] > 0) launch_pdl(k_bonded_b, dim3(t.n[BT_BONDED]), dim3(256), 0, st, args, t.tab[BT_BONDED]);
 }
 
 // ---------------------------------------------------------------- consharm restraint
@@ -277,7 +278,7 @@ constexpr double kFixCom = 16777216.0;  // mass-centre sums, 2^24 per amu A
 // per segment in fixed point (order independent)
 __global__ void __launch_bounds__(256) k_restraint_com(SysParams p, const float4* __restrict__ pos4,
                                                        const int* __restrict__ seg, const float* __restrict__ mass,
-                                                       long long* acc) {
+                                                       long long* acc) { griddep_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double w[6] = {0, 0, 0, 0, 0, 0};
   if (i < p.n) {
@@ -305,7 +306,7 @@ __global__ void __launch_bounds__(256) k_restraint_com(SysParams p, const float4
 __global__ void __launch_bounds__(256) k_restraint_force(int n, const int* __restrict__ seg,
                                                          const long long* __restrict__ acc, double inv_m0,
                                                          double inv_m1, double dx, double dy, double dz, double fc,
-                                                         long long* facc) {
+                                                         long long* facc) { griddep_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || seg[i] != 1) return;
   const double s = 1.0 / kFixCom;
@@ -320,8 +321,8 @@ __global__ void __launch_bounds__(256) k_restraint_force(int n, const int* __res
 void launch_restraint(const SysParams& p, const float4* pos4, const int* seg, const float* mass, long long* acc,
                       double inv_m0, double inv_m1, const double* dist, double fc, long long* facc, cudaStream_t st) {
   const int g = (p.n + 255) / 256;
-  k_restraint_com<<<g, 256, 0, st>>>(p, pos4, seg, mass, acc);
-  k_restraint_force<<<g, 256, 0, st>>>(p.n, seg, acc, inv_m0, inv_m1, dist[0], dist[1], dist[2], fc, facc);
+  launch_pdl(k_restraint_com, dim3(g), dim3(256), 0, st, p, pos4, seg, mass, acc);
+  launch_pdl(k_restraint_force, dim3(g), dim3(256), 0, st, p.n, seg, acc, inv_m0, inv_m1, dist[0], dist[1], dist[2], fc, facc);
 }
 
 }  // namespace fzk

@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <utility>
+
 namespace fzk {
 
 // AKMA constants (src/defs.in.h:156-158)
@@ -65,6 +67,28 @@ struct SysParams {
   int ncol[2];       // column grid (x, y)
   int K[3];          // PME grid
 };
+
+// Programmatic dependent launch (sm_90+): a kernel launched with launch_pdl may be set
+// up while its predecessor in the stream still runs; it waits here, before touching any
+// memory, until the predecessor has completed and its writes are visible, so the stream
+// order is kept and only the launch latency is hidden.  Every kernel that can be
+// launched with launch_pdl calls this first.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <class... P, class... A>
+inline void launch_pdl(void (*k)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, A&&... args) {
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
+}
 
 __device__ __forceinline__ long long to_fix(float f) { return __float2ll_rn(f * kFixF); }
 __device__ __forceinline__ long long to_fix_d(double f) { return __double2ll_rn(f * kFixFd); }

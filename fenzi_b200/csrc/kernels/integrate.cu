@@ -344,6 +344,7 @@ __device__ __forceinline__ void scale_com_velocity(const Unit& U, double v[4][3]
 // by a.lam), and its centre-of-mass velocity is scaled by a.vfric before the kick.
 template <bool NPT, int NA, int NC, bool SETTLE>
 __device__ __forceinline__ void kick_drift_body(const IntegrateArgs& a, int bid) {
+  griddep_wait();
   const int u = a.u_begin + bid * blockDim.x + threadIdx.x;
   if (u >= a.u_end) return;
   const Unit U = load_unit<NA, NC>(a, u);
@@ -449,10 +450,10 @@ __device__ __forceinline__ void kick_drift_body(const IntegrateArgs& a, int bid)
 }
 
 template <bool NPT, int NA, int NC, bool SETTLE = false>
-__global__ void __launch_bounds__(128) k_kick_drift(IntegrateArgs a) { kick_drift_body<NPT, NA, NC, SETTLE>(a, blockIdx.x); }
+__global__ void __launch_bounds__(128) k_kick_drift(IntegrateArgs a) { griddep_wait(); kick_drift_body<NPT, NA, NC, SETTLE>(a, blockIdx.x); }
 
 template <int NA, int NC, bool SETTLE>
-__global__ void __launch_bounds__(128) k_kick_drift_b(const IntegrateArgs* __restrict__ args, const int4* __restrict__ tab) {
+__global__ void __launch_bounds__(128) k_kick_drift_b(const IntegrateArgs* __restrict__ args, const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const IntegrateArgs a = args[t.x];
   kick_drift_body<false, NA, NC, SETTLE>(a, t.y);
@@ -464,7 +465,7 @@ __global__ void __launch_bounds__(128) k_kick_drift_b(const IntegrateArgs* __res
 // force virial into the virial of the unit centres (constraint forces are internal to
 // a unit and drop out).
 template <int NA, int NC>
-__global__ void __launch_bounds__(128) k_unit_virial(IntegrateArgs a) {
+__global__ void __launch_bounds__(128) k_unit_virial(IntegrateArgs a) { griddep_wait();
   const int u = a.u_begin + blockIdx.x * blockDim.x + threadIdx.x;
   double ke = 0.0, vir[3] = {0.0, 0.0, 0.0};
   if (u < a.u_end) {
@@ -512,6 +513,7 @@ __global__ void __launch_bounds__(128) k_unit_virial(IntegrateArgs a) {
 
 template <bool KIN, int NA, int NC>
 __device__ __forceinline__ void kick_rattle_body(const IntegrateArgs& a, int kick, int bid) {
+  griddep_wait();
   const int u = a.u_begin + bid * blockDim.x + threadIdx.x;
   double ke = 0.0;
   if (u < a.u_end) {
@@ -557,16 +559,16 @@ __device__ __forceinline__ void kick_rattle_body(const IntegrateArgs& a, int kic
 }
 
 template <bool KIN, int NA, int NC>
-__global__ void __launch_bounds__(128) k_kick_rattle(IntegrateArgs a, int kick) { kick_rattle_body<KIN, NA, NC>(a, kick, blockIdx.x); }
+__global__ void __launch_bounds__(128) k_kick_rattle(IntegrateArgs a, int kick) { griddep_wait(); kick_rattle_body<KIN, NA, NC>(a, kick, blockIdx.x); }
 
 template <int NA, int NC>
-__global__ void __launch_bounds__(128) k_kick_rattle_b(const IntegrateArgs* __restrict__ args, const int4* __restrict__ tab) {
+__global__ void __launch_bounds__(128) k_kick_rattle_b(const IntegrateArgs* __restrict__ args, const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const IntegrateArgs a = args[t.x];
   kick_rattle_body<false, NA, NC>(a, 1, t.y);
 }
 
-__global__ void __launch_bounds__(256) k_kinetic(IntegrateArgs a) {
+__global__ void __launch_bounds__(256) k_kinetic(IntegrateArgs a) { griddep_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double ke = 0.0;
   if (i < a.p.n) {
@@ -582,7 +584,7 @@ __global__ void __launch_bounds__(256) k_kinetic(IntegrateArgs a) {
 // give constraint forces G_a = sum_l sgn_la lambda_l r_l and the virial
 // sum_l lambda_l r_l (x) r_l (diagonal), added to the virial slots.
 template <int NA, int NC>
-__global__ void __launch_bounds__(128) k_constraint_virial(IntegrateArgs a) {
+__global__ void __launch_bounds__(128) k_constraint_virial(IntegrateArgs a) { griddep_wait();
   const int u = a.u_begin + blockIdx.x * blockDim.x + threadIdx.x;
   double vir[3] = {0.0, 0.0, 0.0};
   if (u < a.u_end) {
@@ -652,7 +654,7 @@ __global__ void __launch_bounds__(128) k_constraint_virial(IntegrateArgs a) {
 // puts the unit back on its constraints (the old positions as reference vectors), so
 // minimised rigid waters stay rigid.  Velocities are zeroed as in the reference.
 template <int NA, int NC>
-__global__ void __launch_bounds__(128) k_min_step(IntegrateArgs a) {
+__global__ void __launch_bounds__(128) k_min_step(IntegrateArgs a) { griddep_wait();
   const int u = a.u_begin + blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= a.u_end) return;
   const Unit U = load_unit<NA, NC>(a, u);
@@ -734,7 +736,7 @@ __device__ __forceinline__ double u01(uint64_t r) { return ((double)(r >> 11) + 
 constexpr double kFixP = 1099511627776.0;  // momentum sums, 2^40
 
 __global__ void __launch_bounds__(256) k_reassign_draw(IntegrateArgs a, double T, uint64_t seed, uint32_t counter,
-                                                       long long* psum) {
+                                                       long long* psum) { griddep_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double px = 0, py = 0, pz = 0;
   if (i < a.p.n) {
@@ -765,7 +767,7 @@ __global__ void __launch_bounds__(256) k_reassign_draw(IntegrateArgs a, double T
   }
 }
 
-__global__ void __launch_bounds__(256) k_reassign_shift(IntegrateArgs a, const long long* psum, double inv_mtot) {
+__global__ void __launch_bounds__(256) k_reassign_shift(IntegrateArgs a, const long long* psum, double inv_mtot) { griddep_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.p.n) return;
   const double s = inv_mtot / kFixP;
@@ -778,7 +780,7 @@ __global__ void __launch_bounds__(256) k_reassign_shift(IntegrateArgs a, const l
   a.vel4[i] = v;
 }
 
-__global__ void k_zero_ll(long long* p, int n) {
+__global__ void k_zero_ll(long long* p, int n) { griddep_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) p[i] = 0;
 }
@@ -822,11 +824,11 @@ static void kick_drift_classes(const IntegrateArgs& a, cudaStream_t st) {
     constexpr int NA = decltype(na)::value, NC = decltype(nc)::value;
     if constexpr (NA == 3 && NC == 3) {
       if (x.settle) {
-        k_kick_drift<NPT, 3, 3, true><<<unit_grid(x), 128, 0, st>>>(x);
+        launch_pdl(k_kick_drift<NPT, 3, 3, true>, dim3(unit_grid(x)), dim3(128), 0, st, x);
         return;
       }
     }
-    k_kick_drift<NPT, NA, NC><<<unit_grid(x), 128, 0, st>>>(x);
+    launch_pdl(k_kick_drift<NPT, NA, NC>, dim3(unit_grid(x)), dim3(128), 0, st, x);
   });
 }
 
@@ -849,11 +851,11 @@ void launch_kick_drift_b(const ClassBatch& c, cudaStream_t st) {
     constexpr int NA = decltype(na)::value, NC = decltype(nc)::value;
     if constexpr (NA == 3 && NC == 3) {
       if (c.settle) {
-        k_kick_drift_b<3, 3, true><<<c.nblocks, 128, 0, st>>>(c.args, c.tab);
+        launch_pdl(k_kick_drift_b<3, 3, true>, dim3(c.nblocks), dim3(128), 0, st, c.args, c.tab);
         return;
       }
     }
-    k_kick_drift_b<NA, NC, false><<<c.nblocks, 128, 0, st>>>(c.args, c.tab);
+    launch_pdl(k_kick_drift_b<NA, NC, false>, dim3(c.nblocks), dim3(128), 0, st, c.args, c.tab);
   });
 }
 
@@ -882,9 +884,9 @@ void launch_kick_rattle(const IntegrateArgs& a, bool kinetic, bool kick, cudaStr
   for_classes(a, [&](const IntegrateArgs& x, auto na, auto nc) {
     constexpr int NA = decltype(na)::value, NC = decltype(nc)::value;
     if (kinetic)
-      k_kick_rattle<true, NA, NC><<<unit_grid(x), 128, 0, st>>>(x, kick ? 1 : 0);
+      launch_pdl(k_kick_rattle<true, NA, NC>, dim3(unit_grid(x)), dim3(128), 0, st, x, kick ? 1 : 0);
     else
-      k_kick_rattle<false, NA, NC><<<unit_grid(x), 128, 0, st>>>(x, kick ? 1 : 0);
+      launch_pdl(k_kick_rattle<false, NA, NC>, dim3(unit_grid(x)), dim3(128), 0, st, x, kick ? 1 : 0);
   });
 }
 
@@ -895,14 +897,14 @@ void launch_min_step(const IntegrateArgs& a, cudaStream_t st) {
 }
 
 void launch_kinetic(const IntegrateArgs& a, cudaStream_t st) {
-  k_kinetic<<<(a.p.n + 255) / 256, 256, 0, st>>>(a);
+  launch_pdl(k_kinetic, dim3((a.p.n + 255) / 256), dim3(256), 0, st, a);
 }
 
 void launch_reassign(const IntegrateArgs& a, double T, uint64_t seed, uint32_t counter, double inv_mtot,
                      long long* psum, cudaStream_t st) {
-  k_zero_ll<<<1, 32, 0, st>>>(psum, 3);
-  k_reassign_draw<<<(a.p.n + 255) / 256, 256, 0, st>>>(a, T, seed, counter, psum);
-  k_reassign_shift<<<(a.p.n + 255) / 256, 256, 0, st>>>(a, psum, inv_mtot);
+  launch_pdl(k_zero_ll, dim3(1), dim3(32), 0, st, psum, 3);
+  launch_pdl(k_reassign_draw, dim3((a.p.n + 255) / 256), dim3(256), 0, st, a, T, seed, counter, psum);
+  launch_pdl(k_reassign_shift, dim3((a.p.n + 255) / 256), dim3(256), 0, st, a, psum, inv_mtot);
   launch_kick_rattle(a, false, false, st);
 }
 

@@ -17,6 +17,7 @@ namespace fzk {
 
 // wrap positions into [-L/2, L/2), record build positions, bin into columns
 __device__ __forceinline__ void rb_bin_body(const RebuildArgs& A, int bid, int nbid) {
+  griddep_wait();
   const SysParams p = A.p;
   const int* __restrict__ flag = A.flag;
   float4* pos4 = A.pos4;
@@ -52,8 +53,8 @@ __device__ __forceinline__ void rb_bin_body(const RebuildArgs& A, int bid, int n
   if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&col_count[c], __popc(peers));
 }
 
-__global__ void k_rb_bin(RebuildArgs a) { rb_bin_body(a, blockIdx.x, gridDim.x); }
-__global__ void k_rb_bin_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) {
+__global__ void k_rb_bin(RebuildArgs a) { griddep_wait(); rb_bin_body(a, blockIdx.x, gridDim.x); }
+__global__ void k_rb_bin_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const RebuildArgs a = args[t.x];
   rb_bin_body(a, t.y, t.z);
@@ -62,6 +63,7 @@ __global__ void k_rb_bin_b(const RebuildArgs* __restrict__ args, const int4* __r
 
 // exclusive scan of the 32-padded column sizes (one block)
 __device__ __forceinline__ void rb_scan_body(const RebuildArgs& A, int bid, int nbid) {
+  griddep_wait();
   const SysParams p = A.p;
   const int* __restrict__ flag = A.flag;
   const int* __restrict__ col_count = A.col_count;
@@ -99,8 +101,8 @@ __device__ __forceinline__ void rb_scan_body(const RebuildArgs& A, int bid, int 
   }
 }
 
-__global__ void k_rb_scan(RebuildArgs a) { rb_scan_body(a, blockIdx.x, gridDim.x); }
-__global__ void k_rb_scan_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) {
+__global__ void k_rb_scan(RebuildArgs a) { griddep_wait(); rb_scan_body(a, blockIdx.x, gridDim.x); }
+__global__ void k_rb_scan_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const RebuildArgs a = args[t.x];
   rb_scan_body(a, t.y, t.z);
@@ -108,6 +110,7 @@ __global__ void k_rb_scan_b(const RebuildArgs* __restrict__ args, const int4* __
 
 
 __device__ __forceinline__ void rb_scatter_body(const RebuildArgs& A, int bid, int nbid) {
+  griddep_wait();
   const SysParams p = A.p;
   const int* __restrict__ flag = A.flag;
   const int* __restrict__ col_of = A.col_of;
@@ -129,8 +132,8 @@ __device__ __forceinline__ void rb_scatter_body(const RebuildArgs& A, int bid, i
   if (s < p.nslots - 32) col_tmp[s] = a;
 }
 
-__global__ void k_rb_scatter(RebuildArgs a) { rb_scatter_body(a, blockIdx.x, gridDim.x); }
-__global__ void k_rb_scatter_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) {
+__global__ void k_rb_scatter(RebuildArgs a) { griddep_wait(); rb_scatter_body(a, blockIdx.x, gridDim.x); }
+__global__ void k_rb_scatter_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const RebuildArgs a = args[t.x];
   rb_scatter_body(a, t.y, t.z);
@@ -144,6 +147,7 @@ __device__ __forceinline__ uint32_t float_key(float f) {
 
 // one block per column: bitonic sort by (z, atom id), then fill the sorted arrays
 __device__ __forceinline__ void rb_colsort_body(const RebuildArgs& A, int bid, int nbid) {
+  griddep_wait();
   const SysParams p = A.p;
   const int* __restrict__ flag = A.flag;
   int* col_count = A.col_count;
@@ -221,8 +225,8 @@ __device__ __forceinline__ void rb_colsort_body(const RebuildArgs& A, int bid, i
   }
 }
 
-__global__ void __launch_bounds__(256) k_rb_colsort(RebuildArgs a) { rb_colsort_body(a, blockIdx.x, gridDim.x); }
-__global__ void __launch_bounds__(256) k_rb_colsort_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) {
+__global__ void __launch_bounds__(256) k_rb_colsort(RebuildArgs a) { griddep_wait(); rb_colsort_body(a, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(256) k_rb_colsort_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const RebuildArgs a = args[t.x];
   rb_colsort_body(a, t.y, t.z);
@@ -242,6 +246,7 @@ __device__ __forceinline__ float box_gap2(float3 d, float3 h) {
 // The diagonal block (J == I, no image) is implicit and not stored.  Entries append to
 // the block's own region outer[I * ocap ...] in a fixed order (deterministic).
 __device__ __forceinline__ void rb_outer_body(const RebuildArgs& A, int bid, int nbid) {
+  griddep_wait();
   const SysParams p = A.p;
   const int* __restrict__ flag = A.flag;
   const int* __restrict__ counters = A.counters;
@@ -344,8 +349,8 @@ __device__ __forceinline__ void rb_outer_body(const RebuildArgs& A, int bid, int
   }
 }
 
-__global__ void __launch_bounds__(256) k_rb_outer(RebuildArgs a) { rb_outer_body(a, blockIdx.x, gridDim.x); }
-__global__ void __launch_bounds__(256) k_rb_outer_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) {
+__global__ void __launch_bounds__(256) k_rb_outer(RebuildArgs a) { griddep_wait(); rb_outer_body(a, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(256) k_rb_outer_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const RebuildArgs a = args[t.x];
   rb_outer_body(a, t.y, t.z);
@@ -355,6 +360,7 @@ __global__ void __launch_bounds__(256) k_rb_outer_b(const RebuildArgs* __restric
 // Per slot: the partner slots of its excluded atoms (1-2, 1-3, 1-4), for the prune's
 // masks; per 32-slot block (one warp): the bounding box of its atoms
 __device__ __forceinline__ void rb_slots_body(const RebuildArgs& A, int bid, int nbid) {
+  griddep_wait();
   const SysParams p = A.p;
   const int* __restrict__ flag = A.flag;
   const int* __restrict__ counters = A.counters;
@@ -401,8 +407,8 @@ __device__ __forceinline__ void rb_slots_body(const RebuildArgs& A, int bid, int
   }
 }
 
-__global__ void k_rb_slots(RebuildArgs a) { rb_slots_body(a, blockIdx.x, gridDim.x); }
-__global__ void k_rb_slots_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) {
+__global__ void k_rb_slots(RebuildArgs a) { griddep_wait(); rb_slots_body(a, blockIdx.x, gridDim.x); }
+__global__ void k_rb_slots_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const RebuildArgs a = args[t.x];
   rb_slots_body(a, t.y, t.z);
@@ -412,6 +418,7 @@ __global__ void k_rb_slots_b(const RebuildArgs* __restrict__ args, const int4* _
 // Closes a rebuild (counts it, lowers its flag, raises the prune flag: a new outer list
 // always gets a fresh inner list) and opens a prune (zeroes the list counters).
 __device__ __forceinline__ void prune_begin_body(const RebuildArgs& A, int bid, int nbid) {
+  griddep_wait();
   int* flag = A.flag;
   int* flag_prune = A.flag_prune;
   int* counters = A.counters;
@@ -427,8 +434,8 @@ __device__ __forceinline__ void prune_begin_body(const RebuildArgs& A, int bid, 
   counters[CNT_ITEMS] = 0;
 }
 
-__global__ void k_prune_begin(RebuildArgs a) { prune_begin_body(a, blockIdx.x, gridDim.x); }
-__global__ void k_prune_begin_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) {
+__global__ void k_prune_begin(RebuildArgs a) { griddep_wait(); prune_begin_body(a, blockIdx.x, gridDim.x); }
+__global__ void k_prune_begin_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const RebuildArgs a = args[t.x];
   prune_begin_body(a, t.y, t.z);
@@ -464,6 +471,7 @@ __device__ __forceinline__ uint32_t excl_mask(int I, uint32_t je, int lane, uint
 // list was made at.  Run after every rebuild and whenever an atom has moved more than
 // delta/2 since the last prune, so no pair within rc is ever missed.
 __device__ __forceinline__ void prune_body(const RebuildArgs& A, int bid, int nbid) {
+  griddep_wait();
   const SysParams p = A.p;
   const int* __restrict__ flag_prune = A.flag_prune;
   int* counters = A.counters;
@@ -622,8 +630,8 @@ __device__ __forceinline__ void prune_body(const RebuildArgs& A, int bid, int nb
   }
 }
 
-__global__ void __launch_bounds__(256, 6) k_prune(RebuildArgs a) { prune_body(a, blockIdx.x, gridDim.x); }
-__global__ void __launch_bounds__(256, 6) k_prune_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) {
+__global__ void __launch_bounds__(256, 6) k_prune(RebuildArgs a) { griddep_wait(); prune_body(a, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(256, 6) k_prune_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const RebuildArgs a = args[t.x];
   prune_body(a, t.y, t.z);
@@ -631,6 +639,7 @@ __global__ void __launch_bounds__(256, 6) k_prune_b(const RebuildArgs* __restric
 
 
 __device__ __forceinline__ void prune_end_body(const RebuildArgs& A, int bid, int nbid) {
+  griddep_wait();
   int* flag_prune = A.flag_prune;
   int* counters = A.counters;
 
@@ -640,8 +649,8 @@ __device__ __forceinline__ void prune_end_body(const RebuildArgs& A, int bid, in
   *flag_prune = 0;
 }
 
-__global__ void k_prune_end(RebuildArgs a) { prune_end_body(a, blockIdx.x, gridDim.x); }
-__global__ void k_prune_end_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) {
+__global__ void k_prune_end(RebuildArgs a) { griddep_wait(); prune_end_body(a, blockIdx.x, gridDim.x); }
+__global__ void k_prune_end_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const RebuildArgs a = args[t.x];
   prune_end_body(a, t.y, t.z);
@@ -651,7 +660,7 @@ __global__ void k_prune_end_b(const RebuildArgs* __restrict__ args, const int4* 
 // sets a graph conditional node's value from a device flag (the neighbour kernels run
 // inside an IF node only when their flag is raised)
 __global__ void k_set_condition(cudaGraphConditionalHandle h, const int* __restrict__ flag,
-                                const int* __restrict__ flag2) {
+                                const int* __restrict__ flag2) { griddep_wait();
   cudaGraphSetConditional(h, (*flag != 0 || (flag2 && *flag2 != 0)) ? 1u : 0u);
 }
 
@@ -669,20 +678,20 @@ void launch_rebuild_build(const RebuildArgs& a, cudaStream_t st) {
   const SysParams& p = a.p;
   const int ncol = p.ncol[0] * p.ncol[1];
   const int maxblk = (p.nslots) / 32;
-  k_rb_bin<<<(p.n + 255) / 256, 256, 0, st>>>(a);
-  k_rb_scan<<<1, 1024, 0, st>>>(a);
-  k_rb_scatter<<<(p.n + 255) / 256, 256, 0, st>>>(a);
-  k_rb_colsort<<<ncol, 256, kColCap * sizeof(unsigned long long), st>>>(a);
-  k_rb_slots<<<(p.nslots + 255) / 256, 256, 0, st>>>(a);
-  k_rb_outer<<<(maxblk + 7) / 8, 256, 0, st>>>(a);
+  launch_pdl(k_rb_bin, dim3((p.n + 255) / 256), dim3(256), 0, st, a);
+  launch_pdl(k_rb_scan, dim3(1), dim3(1024), 0, st, a);
+  launch_pdl(k_rb_scatter, dim3((p.n + 255) / 256), dim3(256), 0, st, a);
+  launch_pdl(k_rb_colsort, dim3(ncol), dim3(256), kColCap * sizeof(unsigned long long), st, a);
+  launch_pdl(k_rb_slots, dim3((p.nslots + 255) / 256), dim3(256), 0, st, a);
+  launch_pdl(k_rb_outer, dim3((maxblk + 7) / 8), dim3(256), 0, st, a);
 }
 
 void launch_rebuild_prune(const RebuildArgs& a, cudaStream_t st) {
   const SysParams& p = a.p;
   const int maxblk = (p.nslots) / 32;
-  k_prune_begin<<<1, 1, 0, st>>>(a);
-  k_prune<<<(maxblk + 7) / 8, 256, 0, st>>>(a);
-  k_prune_end<<<1, 1, 0, st>>>(a);
+  launch_pdl(k_prune_begin, dim3(1), dim3(1), 0, st, a);
+  launch_pdl(k_prune, dim3((maxblk + 7) / 8), dim3(256), 0, st, a);
+  launch_pdl(k_prune_end, dim3(1), dim3(1), 0, st, a);
 }
 
 // ------------------------------------------------------------------ batched launchers
@@ -698,18 +707,18 @@ void rebuild_grids(const RebuildArgs& a, int* g6) {
 }
 
 void launch_rebuild_build_b(const RebuildArgs* args, const BatchTables& t, cudaStream_t st) {
-  k_rb_bin_b<<<t.n[BT_ATOMS256], 256, 0, st>>>(args, t.tab[BT_ATOMS256]);
-  k_rb_scan_b<<<t.n[BT_ONE], 1024, 0, st>>>(args, t.tab[BT_ONE]);
-  k_rb_scatter_b<<<t.n[BT_ATOMS256], 256, 0, st>>>(args, t.tab[BT_ATOMS256]);
-  k_rb_colsort_b<<<t.n[BT_COLUMNS], 256, kColCap * sizeof(unsigned long long), st>>>(args, t.tab[BT_COLUMNS]);
-  k_rb_slots_b<<<t.n[BT_SLOTS256], 256, 0, st>>>(args, t.tab[BT_SLOTS256]);
-  k_rb_outer_b<<<t.n[BT_BLOCKS8], 256, 0, st>>>(args, t.tab[BT_BLOCKS8]);
+  launch_pdl(k_rb_bin_b, dim3(t.n[BT_ATOMS256]), dim3(256), 0, st, args, t.tab[BT_ATOMS256]);
+  launch_pdl(k_rb_scan_b, dim3(t.n[BT_ONE]), dim3(1024), 0, st, args, t.tab[BT_ONE]);
+  launch_pdl(k_rb_scatter_b, dim3(t.n[BT_ATOMS256]), dim3(256), 0, st, args, t.tab[BT_ATOMS256]);
+  launch_pdl(k_rb_colsort_b, dim3(t.n[BT_COLUMNS]), dim3(256), kColCap * sizeof(unsigned long long), st, args, t.tab[BT_COLUMNS]);
+  launch_pdl(k_rb_slots_b, dim3(t.n[BT_SLOTS256]), dim3(256), 0, st, args, t.tab[BT_SLOTS256]);
+  launch_pdl(k_rb_outer_b, dim3(t.n[BT_BLOCKS8]), dim3(256), 0, st, args, t.tab[BT_BLOCKS8]);
 }
 
 void launch_rebuild_prune_b(const RebuildArgs* args, const BatchTables& t, cudaStream_t st) {
-  k_prune_begin_b<<<t.n[BT_ONE], 1, 0, st>>>(args, t.tab[BT_ONE]);
-  k_prune_b<<<t.n[BT_BLOCKS8], 256, 0, st>>>(args, t.tab[BT_BLOCKS8]);
-  k_prune_end_b<<<t.n[BT_ONE], 1, 0, st>>>(args, t.tab[BT_ONE]);
+  launch_pdl(k_prune_begin_b, dim3(t.n[BT_ONE]), dim3(1), 0, st, args, t.tab[BT_ONE]);
+  launch_pdl(k_prune_b, dim3(t.n[BT_BLOCKS8]), dim3(256), 0, st, args, t.tab[BT_BLOCKS8]);
+  launch_pdl(k_prune_end_b, dim3(t.n[BT_ONE]), dim3(1), 0, st, args, t.tab[BT_ONE]);
 }
 
 }  // namespace fzk

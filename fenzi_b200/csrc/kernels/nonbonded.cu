@@ -201,6 +201,7 @@ __device__ __forceinline__ void nonbonded_body(const SysParams& p, const PairCon
     const int* __restrict__ inner_m, const uint32_t* __restrict__ dmask, const uint32_t* __restrict__ masks,
     int* __restrict__ counters, const int2* __restrict__ items, int chunk, const float2* __restrict__ ljtab,
     long long* __restrict__ facc, long long* __restrict__ energy, int ocap) {
+  griddep_wait();
   extern __shared__ float2 lj[];
   __shared__ float4 jx_all[kWarps][64];
   __shared__ int jt_all[kWarps][64];
@@ -297,14 +298,14 @@ __global__ void __launch_bounds__(256, MINB)
                 const int* __restrict__ inner_m, const uint32_t* __restrict__ dmask,
                 const uint32_t* __restrict__ masks, int* __restrict__ counters, const int2* __restrict__ items,
                 int chunk, const float2* __restrict__ ljtab, long long* __restrict__ facc,
-                long long* __restrict__ energy, int ocap) {
+                long long* __restrict__ energy, int ocap) { griddep_wait();
   nonbonded_body<ENERGY>(p, c, xyzq, typ, perm, inner, inner_nt, inner_m, dmask, masks, counters, items, chunk, ljtab,
                          facc, energy, ocap);
 }
 
 // batched: every CTA serves one system's work queue (force variant only)
 __global__ void __launch_bounds__(256, 4) k_nonbonded_b(const NonbondedArgs* __restrict__ args,
-                                                        const int4* __restrict__ tab) {
+                                                        const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const NonbondedArgs a = args[t.x];
   const PairConst c = pair_const(a.p);
@@ -320,14 +321,14 @@ void launch_nonbonded(const NonbondedArgs& a, bool energy, cudaStream_t st) {
   // 3 CTAs per SM fit 80 registers a thread; the 4-CTA build is held to 64
   auto k = energy ? (a.minb >= 4 ? k_nonbonded<true, 4> : k_nonbonded<true, 3>)
                   : (a.minb >= 4 ? k_nonbonded<false, 4> : k_nonbonded<false, 3>);
-  k<<<a.grid, kWarps * 32, smem, st>>>(a.p, c, a.xyzq_s, a.typ_s, a.perm, a.inner, a.inner_nt, a.inner_m, a.dmask,
+  launch_pdl(k, dim3(a.grid), dim3(kWarps * 32), smem, st, a.p, c, a.xyzq_s, a.typ_s, a.perm, a.inner, a.inner_nt, a.inner_m, a.dmask,
                                        a.masks, a.counters, a.items, a.chunk, a.ljtab, a.facc, a.energy, a.ocap);
 }
 
 // the work counters are zeroed by the prune's last kernel every step in batched steps
 void launch_nonbonded_b(const NonbondedArgs* args, const BatchTables& t, int max_ntypes, cudaStream_t st) {
   const size_t smem = (size_t)(max_ntypes + 1) * (max_ntypes + 1) * sizeof(float2);
-  k_nonbonded_b<<<t.n[BT_NB], kWarps * 32, smem, st>>>(args, t.tab[BT_NB]);
+  launch_pdl(k_nonbonded_b, dim3(t.n[BT_NB]), dim3(kWarps * 32), smem, st, args, t.tab[BT_NB]);
 }
 
 }  // namespace fzk

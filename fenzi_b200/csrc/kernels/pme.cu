@@ -59,6 +59,7 @@ __device__ __forceinline__ void bsp4(float t, float* w, float* dw) {
 }
 
 __device__ __forceinline__ void pme_zero_body(const PmeArgs& a, int bid, int nbid) {
+  griddep_wait();
   int* cnt = a.brick_count;
   int* cur = a.brick_cursor;
   const int nb = a.nb[0] * a.nb[1] * a.nb[2];
@@ -68,8 +69,8 @@ __device__ __forceinline__ void pme_zero_body(const PmeArgs& a, int bid, int nbi
   }
 }
 
-__global__ void k_pme_zero(PmeArgs a) { pme_zero_body(a, blockIdx.x, gridDim.x); }
-__global__ void k_pme_zero_b(const PmeArgs* __restrict__ args, const int4* __restrict__ tab) {
+__global__ void k_pme_zero(PmeArgs a) { griddep_wait(); pme_zero_body(a, blockIdx.x, gridDim.x); }
+__global__ void k_pme_zero_b(const PmeArgs* __restrict__ args, const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const PmeArgs a = args[t.x];
   pme_zero_body(a, t.y, t.z);
@@ -77,6 +78,7 @@ __global__ void k_pme_zero_b(const PmeArgs* __restrict__ args, const int4* __res
 
 
 __device__ __forceinline__ void pme_bin_body(const PmeArgs& a, int bid, int nbid) {
+  griddep_wait();
   const int i = bid * blockDim.x + threadIdx.x;
   if (i >= a.n) return;
   const float4 r = a.pos4[i];
@@ -91,8 +93,8 @@ __device__ __forceinline__ void pme_bin_body(const PmeArgs& a, int bid, int nbid
   if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&a.brick_count[b], __popc(peers));
 }
 
-__global__ void k_pme_bin(PmeArgs a) { pme_bin_body(a, blockIdx.x, gridDim.x); }
-__global__ void k_pme_bin_b(const PmeArgs* __restrict__ args, const int4* __restrict__ tab) {
+__global__ void k_pme_bin(PmeArgs a) { griddep_wait(); pme_bin_body(a, blockIdx.x, gridDim.x); }
+__global__ void k_pme_bin_b(const PmeArgs* __restrict__ args, const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const PmeArgs a = args[t.x];
   pme_bin_body(a, t.y, t.z);
@@ -100,6 +102,7 @@ __global__ void k_pme_bin_b(const PmeArgs* __restrict__ args, const int4* __rest
 
 
 __device__ __forceinline__ void pme_scan_body(const PmeArgs& a, int bid, int nbid) {
+  griddep_wait();
   const int nbr = a.nb[0] * a.nb[1] * a.nb[2];
   __shared__ int part[1024];
   const int t = threadIdx.x, nt = blockDim.x;
@@ -123,8 +126,8 @@ __device__ __forceinline__ void pme_scan_body(const PmeArgs& a, int bid, int nbi
   if (t == nt - 1) a.brick_start[nbr] = part[t];
 }
 
-__global__ void k_pme_scan(PmeArgs a) { pme_scan_body(a, blockIdx.x, gridDim.x); }
-__global__ void k_pme_scan_b(const PmeArgs* __restrict__ args, const int4* __restrict__ tab) {
+__global__ void k_pme_scan(PmeArgs a) { griddep_wait(); pme_scan_body(a, blockIdx.x, gridDim.x); }
+__global__ void k_pme_scan_b(const PmeArgs* __restrict__ args, const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const PmeArgs a = args[t.x];
   pme_scan_body(a, t.y, t.z);
@@ -132,6 +135,7 @@ __global__ void k_pme_scan_b(const PmeArgs* __restrict__ args, const int4* __res
 
 
 __device__ __forceinline__ void pme_scatter_body(const PmeArgs& a, int bid, int nbid) {
+  griddep_wait();
   const int i = bid * blockDim.x + threadIdx.x;
   if (i >= a.n) return;
   const int b = a.brick_of[i];
@@ -144,8 +148,8 @@ __device__ __forceinline__ void pme_scatter_body(const PmeArgs& a, int bid, int 
   a.brick_atoms[a.brick_start[b] + k] = i;
 }
 
-__global__ void k_pme_scatter(PmeArgs a) { pme_scatter_body(a, blockIdx.x, gridDim.x); }
-__global__ void k_pme_scatter_b(const PmeArgs* __restrict__ args, const int4* __restrict__ tab) {
+__global__ void k_pme_scatter(PmeArgs a) { griddep_wait(); pme_scatter_body(a, blockIdx.x, gridDim.x); }
+__global__ void k_pme_scatter_b(const PmeArgs* __restrict__ args, const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const PmeArgs a = args[t.x];
   pme_scatter_body(a, t.y, t.z);
@@ -166,6 +170,7 @@ __device__ __forceinline__ float charge_at(const PmeArgs& a, size_t i) {
 // atomics (2^24 per e; values stay far below +-128 e).  The region is then added to
 // the int32 charge grid; integer sums are exact, so the grid is bit-reproducible.
 __device__ __forceinline__ void pme_spread_body(const PmeArgs& a, int bid, int nbid) {
+  griddep_wait();
   extern __shared__ int acc[];
   const int Bx = a.B[0], By = a.B[1], Bz = a.B[2];
   const int Ex = Bx + 3, Ey = By + 3, Ez = Bz + 3;
@@ -221,8 +226,8 @@ __device__ __forceinline__ void pme_spread_body(const PmeArgs& a, int bid, int n
   }
 }
 
-__global__ void __launch_bounds__(256) k_pme_spread(PmeArgs a) { pme_spread_body(a, blockIdx.x, gridDim.x); }
-__global__ void __launch_bounds__(256) k_pme_spread_b(const PmeArgs* __restrict__ args, const int4* __restrict__ tab) {
+__global__ void __launch_bounds__(256) k_pme_spread(PmeArgs a) { griddep_wait(); pme_spread_body(a, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(256) k_pme_spread_b(const PmeArgs* __restrict__ args, const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const PmeArgs a = args[t.x];
   pme_spread_body(a, t.y, t.z);
@@ -312,7 +317,7 @@ __device__ __forceinline__ void load_tw(float2* s, const float2* g, int n) {
 }
 
 // x pass forward: real rows -> half spectrum (mx = 0..Kx/2)
-__global__ void __launch_bounds__(256) k_fft_x_r2c(PmeArgs a, FftPlan pl, int nl) {
+__global__ void __launch_bounds__(256) k_fft_x_r2c(PmeArgs a, FftPlan pl, int nl) { griddep_wait();
   extern __shared__ float2 sm[];
   const int Kx = a.K[0], Kxh = Kx / 2 + 1;
   const int nrows = a.K[1] * a.K[2];
@@ -337,7 +342,7 @@ __global__ void __launch_bounds__(256) k_fft_x_r2c(PmeArgs a, FftPlan pl, int nl
 }
 
 // y pass (forward or inverse): lines along y for nl consecutive mx at fixed z
-__global__ void __launch_bounds__(256) k_fft_y(PmeArgs a, FftPlan pl, int nl, int inv) {
+__global__ void __launch_bounds__(256) k_fft_y(PmeArgs a, FftPlan pl, int nl, int inv) { griddep_wait();
   extern __shared__ float2 sm[];
   const int Kx = a.K[0], Ky = a.K[1], Kxh = Kx / 2 + 1;
   const int ng = (Kxh + nl - 1) / nl;
@@ -363,7 +368,7 @@ __global__ void __launch_bounds__(256) k_fft_y(PmeArgs a, FftPlan pl, int nl, in
 
 // z pass: forward, influence function (and reciprocal energy), inverse
 template <bool ENERGY>
-__global__ void __launch_bounds__(256) k_fft_z_conv(PmeArgs a, FftPlan pl, int nl) {
+__global__ void __launch_bounds__(256) k_fft_z_conv(PmeArgs a, FftPlan pl, int nl) { griddep_wait();
   extern __shared__ float2 sm[];
   const int Kx = a.K[0], Ky = a.K[1], Kz = a.K[2], Kxh = Kx / 2 + 1;
   const int ng = (Kxh + nl - 1) / nl;
@@ -424,7 +429,7 @@ __global__ void __launch_bounds__(256) k_fft_z_conv(PmeArgs a, FftPlan pl, int n
 }
 
 // x pass inverse: Hermitian half rows -> real potential rows
-__global__ void __launch_bounds__(256) k_fft_x_c2r(PmeArgs a, FftPlan pl, int nl) {
+__global__ void __launch_bounds__(256) k_fft_x_c2r(PmeArgs a, FftPlan pl, int nl) { griddep_wait();
   extern __shared__ float2 sm[];
   const int Kx = a.K[0], Kxh = Kx / 2 + 1;
   const int nrows = a.K[1] * a.K[2];
@@ -458,6 +463,7 @@ __global__ void __launch_bounds__(256) k_fft_x_c2r(PmeArgs a, FftPlan pl, int nl
 
 // one thread per atom, atoms taken in brick order so a warp reads neighbouring grid lines
 __device__ __forceinline__ void pme_gather_body(const PmeArgs& a, int bid, int nbid) {
+  griddep_wait();
   const int t = bid * blockDim.x + threadIdx.x;
   if (t >= a.n) return;
   const int i = a.brick_atoms[t];
@@ -501,8 +507,8 @@ __device__ __forceinline__ void pme_gather_body(const PmeArgs& a, int bid, int n
   red_add(a.facc + 2 * n + i, to_fix(-q * gz * (float)Kz * a.p.inv_box.z));
 }
 
-__global__ void __launch_bounds__(256) k_pme_gather(PmeArgs a) { pme_gather_body(a, blockIdx.x, gridDim.x); }
-__global__ void __launch_bounds__(256) k_pme_gather_b(const PmeArgs* __restrict__ args, const int4* __restrict__ tab) {
+__global__ void __launch_bounds__(256) k_pme_gather(PmeArgs a) { griddep_wait(); pme_gather_body(a, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(256) k_pme_gather_b(const PmeArgs* __restrict__ args, const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const PmeArgs a = args[t.x];
   pme_gather_body(a, t.y, t.z);
@@ -622,7 +628,7 @@ __device__ __forceinline__ float2* fft_run_t(float2* a, float2* b, const float2*
 // one complex line, so each complex FFT transforms two rows; with Z its transform,
 // X0(m) = (Z(m) + conj Z(N-m)) / 2 and X1(m) = (Z(m) - conj Z(N-m)) / 2i.
 template <int N>
-__global__ void __launch_bounds__(256) k_fft_x_r2c_t(PmeArgs a, int) {
+__global__ void __launch_bounds__(256) k_fft_x_r2c_t(PmeArgs a, int) { griddep_wait();
   constexpr int nl = fft_lines_per_block(N);  // complex lines = row pairs per block
   extern __shared__ float2 sm[];
   constexpr int LD = N + 1, NH = N / 2 + 1;
@@ -650,7 +656,7 @@ __global__ void __launch_bounds__(256) k_fft_x_r2c_t(PmeArgs a, int) {
 }
 
 template <int N, bool INV>
-__global__ void __launch_bounds__(256) k_fft_y_t(PmeArgs a, int) {
+__global__ void __launch_bounds__(256) k_fft_y_t(PmeArgs a, int) { griddep_wait();
   constexpr int nl = fft_lines_per_block(N);
   extern __shared__ float2 sm[];
   constexpr int LD = N + 1;
@@ -677,6 +683,7 @@ __global__ void __launch_bounds__(256) k_fft_y_t(PmeArgs a, int) {
 
 template <int N, bool ENERGY>
 __device__ __forceinline__ void fft_z_conv_body(const PmeArgs& a, int bid) {
+  griddep_wait();
   constexpr int nl = fft_lines_per_block(N);
   extern __shared__ float2 sm[];
   constexpr int LD = N + 1;
@@ -735,9 +742,9 @@ __device__ __forceinline__ void fft_z_conv_body(const PmeArgs& a, int bid) {
 }
 
 template <int N, bool ENERGY>
-__global__ void __launch_bounds__(256) k_fft_z_conv_t(PmeArgs a, int) { fft_z_conv_body<N, ENERGY>(a, blockIdx.x); }
+__global__ void __launch_bounds__(256) k_fft_z_conv_t(PmeArgs a, int) { griddep_wait(); fft_z_conv_body<N, ENERGY>(a, blockIdx.x); }
 template <int N>
-__global__ void __launch_bounds__(256) k_fft_z_conv_b(const PmeArgs* __restrict__ args, const int4* __restrict__ tab) {
+__global__ void __launch_bounds__(256) k_fft_z_conv_b(const PmeArgs* __restrict__ args, const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const PmeArgs a = args[t.x];
   fft_z_conv_body<N, false>(a, t.y);
@@ -747,7 +754,7 @@ __global__ void __launch_bounds__(256) k_fft_z_conv_b(const PmeArgs* __restrict_
 // Inverse of the pairing above: Z(m) = X0(m) + i X1(m) over the full line (Hermitian
 // extension for m > N/2) transforms back to row 2p + i row 2p+1.
 template <int N>
-__global__ void __launch_bounds__(256) k_fft_x_c2r_t(PmeArgs a, int) {
+__global__ void __launch_bounds__(256) k_fft_x_c2r_t(PmeArgs a, int) { griddep_wait();
   constexpr int nl = fft_lines_per_block(N);
   extern __shared__ float2 sm[];
   constexpr int LD = N + 1, NH = N / 2 + 1;
@@ -850,6 +857,7 @@ constexpr size_t plane_smem_bytes() {
 // forward: real plane z -> half spectrum along x, full spectrum along y, cgrid[z][y][mx]
 template <int N>
 __device__ __forceinline__ void fft_xy_plane_body(const PmeArgs& a, int z) {
+  griddep_wait();
   extern __shared__ float2 sm[];
   constexpr int LD = N + 1, NH = N / 2 + 1, NP = (N + 1) / 2, W = plane_words<N>();
   float2* tw = sm;
@@ -881,6 +889,7 @@ __device__ __forceinline__ void fft_xy_plane_body(const PmeArgs& a, int z) {
 // inverse x transform -> real potential plane z
 template <int N>
 __device__ __forceinline__ void fft_yx_plane_body(const PmeArgs& a, int z) {
+  griddep_wait();
   extern __shared__ float2 sm[];
   constexpr int LD = N + 1, NH = N / 2 + 1, NP = (N + 1) / 2, W = plane_words<N>();
   float2* tw = sm;
@@ -915,19 +924,19 @@ __device__ __forceinline__ void fft_yx_plane_body(const PmeArgs& a, int z) {
 }
 
 template <int N>
-__global__ void __launch_bounds__(kPlaneThreads) k_fft_xy_plane(PmeArgs a) { fft_xy_plane_body<N>(a, blockIdx.x); }
+__global__ void __launch_bounds__(kPlaneThreads) k_fft_xy_plane(PmeArgs a) { griddep_wait(); fft_xy_plane_body<N>(a, blockIdx.x); }
 template <int N>
-__global__ void __launch_bounds__(kPlaneThreads) k_fft_yx_plane(PmeArgs a) { fft_yx_plane_body<N>(a, blockIdx.x); }
+__global__ void __launch_bounds__(kPlaneThreads) k_fft_yx_plane(PmeArgs a) { griddep_wait(); fft_yx_plane_body<N>(a, blockIdx.x); }
 template <int N>
 __global__ void __launch_bounds__(kPlaneThreads) k_fft_xy_plane_b(const PmeArgs* __restrict__ args,
-                                                                  const int4* __restrict__ tab) {
+                                                                  const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const PmeArgs a = args[t.x];
   fft_xy_plane_body<N>(a, t.y);
 }
 template <int N>
 __global__ void __launch_bounds__(kPlaneThreads) k_fft_yx_plane_b(const PmeArgs* __restrict__ args,
-                                                                  const int4* __restrict__ tab) {
+                                                                  const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const PmeArgs a = args[t.x];
   fft_yx_plane_body<N>(a, t.y);
@@ -939,7 +948,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fft_yx_plane_b(const PmeArgs*
 
 static bool fft_x_r2c_t(const PmeArgs& a, int nl, dim3 g, size_t sm, cudaStream_t st) {
   switch (a.K[0]) {
-#define FZ_C(N) case N: k_fft_x_r2c_t<N><<<g, 256, sm, st>>>(a, nl); return true;
+#define FZ_C(N) case N: launch_pdl(k_fft_x_r2c_t<N>, dim3(g), dim3(256), sm, st, a, nl); return true;
     FZ_FFT_SIZES(FZ_C)
 #undef FZ_C
   }
@@ -949,8 +958,8 @@ static bool fft_y_t(const PmeArgs& a, int nl, bool inv, dim3 g, size_t sm, cudaS
   switch (a.K[1]) {
 #define FZ_C(N)                                                   \
   case N:                                                         \
-    if (inv) k_fft_y_t<N, true><<<g, 256, sm, st>>>(a, nl);        \
-    else k_fft_y_t<N, false><<<g, 256, sm, st>>>(a, nl);           \
+    if (inv) launch_pdl(k_fft_y_t<N, true>, dim3(g), dim3(256), sm, st, a, nl);        \
+    else launch_pdl(k_fft_y_t<N, false>, dim3(g), dim3(256), sm, st, a, nl);           \
     return true;
     FZ_FFT_SIZES(FZ_C)
 #undef FZ_C
@@ -961,8 +970,8 @@ static bool fft_z_t(const PmeArgs& a, int nl, bool energy, dim3 g, size_t sm, cu
   switch (a.K[2]) {
 #define FZ_C(N)                                                      \
   case N:                                                            \
-    if (energy) k_fft_z_conv_t<N, true><<<g, 256, sm, st>>>(a, nl);   \
-    else k_fft_z_conv_t<N, false><<<g, 256, sm, st>>>(a, nl);         \
+    if (energy) launch_pdl(k_fft_z_conv_t<N, true>, dim3(g), dim3(256), sm, st, a, nl);   \
+    else launch_pdl(k_fft_z_conv_t<N, false>, dim3(g), dim3(256), sm, st, a, nl);         \
     return true;
     FZ_FFT_SIZES(FZ_C)
 #undef FZ_C
@@ -992,8 +1001,8 @@ static void fft_plane(const PmeArgs& a, bool inverse, cudaStream_t st) {
       return true;                                                                                     \
     }();                                                                                               \
     (void)attr;                                                                                        \
-    if (inverse) k_fft_yx_plane<N><<<a.K[2], kPlaneThreads, sm, st>>>(a);                              \
-    else k_fft_xy_plane<N><<<a.K[2], kPlaneThreads, sm, st>>>(a);                                      \
+    if (inverse) launch_pdl(k_fft_yx_plane<N>, dim3(a.K[2]), dim3(kPlaneThreads), sm, st, a);                              \
+    else launch_pdl(k_fft_xy_plane<N>, dim3(a.K[2]), dim3(kPlaneThreads), sm, st, a);                                      \
     return;                                                                                            \
   }
     FZ_PLANE_SIZES(FZ_C)
@@ -1012,7 +1021,7 @@ static bool fft_size_compiled(int n) {
 
 static bool fft_x_c2r_t(const PmeArgs& a, int nl, dim3 g, size_t sm, cudaStream_t st) {
   switch (a.K[0]) {
-#define FZ_C(N) case N: k_fft_x_c2r_t<N><<<g, 256, sm, st>>>(a, nl); return true;
+#define FZ_C(N) case N: launch_pdl(k_fft_x_c2r_t<N>, dim3(g), dim3(256), sm, st, a, nl); return true;
     FZ_FFT_SIZES(FZ_C)
 #undef FZ_C
   }
@@ -1037,13 +1046,13 @@ int pme_launches(const PmeArgs& a) { return 5 + (use_plane_fft(a) ? 3 : 5) + 1; 
 
 void launch_pme(const PmeArgs& a, bool energy, cudaStream_t st) {
   const int nbr = a.nb[0] * a.nb[1] * a.nb[2];
-  k_pme_zero<<<(nbr + 255) / 256, 256, 0, st>>>(a);
-  k_pme_bin<<<(a.n + 255) / 256, 256, 0, st>>>(a);
-  k_pme_scan<<<1, 1024, 0, st>>>(a);
-  k_pme_scatter<<<(a.n + 255) / 256, 256, 0, st>>>(a);
+  launch_pdl(k_pme_zero, dim3((nbr + 255) / 256), dim3(256), 0, st, a);
+  launch_pdl(k_pme_bin, dim3((a.n + 255) / 256), dim3(256), 0, st, a);
+  launch_pdl(k_pme_scan, dim3(1), dim3(1024), 0, st, a);
+  launch_pdl(k_pme_scatter, dim3((a.n + 255) / 256), dim3(256), 0, st, a);
   const size_t sp = (size_t)(a.B[0] + 3) * (a.B[1] + 3) * (a.B[2] + 3) * sizeof(int);
   cudaMemsetAsync(a.grid, 0, (size_t)a.K[0] * a.K[1] * a.K[2] * sizeof(float), st);
-  k_pme_spread<<<nbr, 256, sp, st>>>(a);
+  launch_pdl(k_pme_spread, dim3(nbr), dim3(256), sp, st, a);
   const int Kx = a.K[0], Ky = a.K[1], Kz = a.K[2], Kxh = Kx / 2 + 1;
   const FftPlan px = make_plan(Kx), py = make_plan(Ky), pz = make_plan(Kz);
   const int lx = lines_for(Kx), ly = lines_for(Ky), lz = lines_for(Kz);
@@ -1058,27 +1067,27 @@ void launch_pme(const PmeArgs& a, bool energy, cudaStream_t st) {
   if (plane) {
     fft_plane(a, false, st);
   } else {
-    if (!fft_x_r2c_t(a, lx, gx2, smx, st)) k_fft_x_r2c<<<gx, 256, smx, st>>>(a, px, lx);
-    if (!fft_y_t(a, ly, false, gy, smy, st)) k_fft_y<<<gy, 256, smy, st>>>(a, py, ly, 0);
+    if (!fft_x_r2c_t(a, lx, gx2, smx, st)) launch_pdl(k_fft_x_r2c, dim3(gx), dim3(256), smx, st, a, px, lx);
+    if (!fft_y_t(a, ly, false, gy, smy, st)) launch_pdl(k_fft_y, dim3(gy), dim3(256), smy, st, a, py, ly, 0);
   }
   if (!fft_z_t(a, lz, energy, gz, smz, st)) {
     if (energy)
-      k_fft_z_conv<true><<<gz, 256, smz, st>>>(a, pz, lz);
+      launch_pdl(k_fft_z_conv<true>, dim3(gz), dim3(256), smz, st, a, pz, lz);
     else
-      k_fft_z_conv<false><<<gz, 256, smz, st>>>(a, pz, lz);
+      launch_pdl(k_fft_z_conv<false>, dim3(gz), dim3(256), smz, st, a, pz, lz);
   }
   if (plane) {
     fft_plane(a, true, st);
   } else {
-    if (!fft_y_t(a, ly, true, gy, smy, st)) k_fft_y<<<gy, 256, smy, st>>>(a, py, ly, 1);
-    if (!fft_x_c2r_t(a, lx, gx2, smx, st)) k_fft_x_c2r<<<gx, 256, smx, st>>>(a, px, lx);
+    if (!fft_y_t(a, ly, true, gy, smy, st)) launch_pdl(k_fft_y, dim3(gy), dim3(256), smy, st, a, py, ly, 1);
+    if (!fft_x_c2r_t(a, lx, gx2, smx, st)) launch_pdl(k_fft_x_c2r, dim3(gx), dim3(256), smx, st, a, px, lx);
   }
-  k_pme_gather<<<(a.n + 255) / 256, 256, 0, st>>>(a);
+  launch_pdl(k_pme_gather, dim3((a.n + 255) / 256), dim3(256), 0, st, a);
 }
 
 // ------------------------------------------------------------------ batched PME
 // zeroes the int32 charge grid of each system (the memset of the single-system path)
-__global__ void k_grid_zero_b(const PmeArgs* __restrict__ args, const int4* __restrict__ tab) {
+__global__ void k_grid_zero_b(const PmeArgs* __restrict__ args, const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const PmeArgs a = args[t.x];
   const size_t kt = (size_t)a.K[0] * a.K[1] * a.K[2];
@@ -1097,12 +1106,12 @@ bool pme_batchable(const PmeArgs& a) { return use_plane_fft(a) && a.K[2] == a.K[
 
 void launch_pme_b(const PmeArgs* args, const BatchTables& t, const PmeSizeBatch* sizes, int nsizes,
                   size_t spread_smem, cudaStream_t st) {
-  k_pme_zero_b<<<t.n[BT_BRICKS256], 256, 0, st>>>(args, t.tab[BT_BRICKS256]);
-  k_pme_bin_b<<<t.n[BT_ATOMS256], 256, 0, st>>>(args, t.tab[BT_ATOMS256]);
-  k_pme_scan_b<<<t.n[BT_ONE], 1024, 0, st>>>(args, t.tab[BT_ONE]);
-  k_pme_scatter_b<<<t.n[BT_ATOMS256], 256, 0, st>>>(args, t.tab[BT_ATOMS256]);
-  k_grid_zero_b<<<t.n[BT_GRID256], 256, 0, st>>>(args, t.tab[BT_GRID256]);
-  k_pme_spread_b<<<t.n[BT_BRICKS], 256, spread_smem, st>>>(args, t.tab[BT_BRICKS]);
+  launch_pdl(k_pme_zero_b, dim3(t.n[BT_BRICKS256]), dim3(256), 0, st, args, t.tab[BT_BRICKS256]);
+  launch_pdl(k_pme_bin_b, dim3(t.n[BT_ATOMS256]), dim3(256), 0, st, args, t.tab[BT_ATOMS256]);
+  launch_pdl(k_pme_scan_b, dim3(t.n[BT_ONE]), dim3(1024), 0, st, args, t.tab[BT_ONE]);
+  launch_pdl(k_pme_scatter_b, dim3(t.n[BT_ATOMS256]), dim3(256), 0, st, args, t.tab[BT_ATOMS256]);
+  launch_pdl(k_grid_zero_b, dim3(t.n[BT_GRID256]), dim3(256), 0, st, args, t.tab[BT_GRID256]);
+  launch_pdl(k_pme_spread_b, dim3(t.n[BT_BRICKS]), dim3(256), spread_smem, st, args, t.tab[BT_BRICKS]);
   for (int pass = 0; pass < 3; ++pass)
     for (int k = 0; k < nsizes; ++k) {
       const PmeSizeBatch& b = sizes[k];
@@ -1118,16 +1127,16 @@ void launch_pme_b(const PmeArgs* args, const BatchTables& t, const PmeSizeBatch*
     (void)attr;                                                                                        \
     constexpr int nl = fft_lines_per_block(N);                                                         \
     constexpr size_t smz = (size_t)(N + 2 * nl * (N + 1)) * sizeof(float2);                           \
-    if (pass == 0) k_fft_xy_plane_b<N><<<b.nplane, kPlaneThreads, sm, st>>>(args, b.plane_tab);       \
-    if (pass == 1) k_fft_z_conv_b<N><<<b.nz, 256, smz, st>>>(args, b.z_tab);                           \
-    if (pass == 2) k_fft_yx_plane_b<N><<<b.nplane, kPlaneThreads, sm, st>>>(args, b.plane_tab);       \
+    if (pass == 0) launch_pdl(k_fft_xy_plane_b<N>, dim3(b.nplane), dim3(kPlaneThreads), sm, st, args, b.plane_tab);       \
+    if (pass == 1) launch_pdl(k_fft_z_conv_b<N>, dim3(b.nz), dim3(256), smz, st, args, b.z_tab);                           \
+    if (pass == 2) launch_pdl(k_fft_yx_plane_b<N>, dim3(b.nplane), dim3(kPlaneThreads), sm, st, args, b.plane_tab);       \
     break;                                                                                             \
   }
         FZ_PLANE_SIZES(FZ_C)
 #undef FZ_C
       }
     }
-  k_pme_gather_b<<<t.n[BT_ATOMS256], 256, 0, st>>>(args, t.tab[BT_ATOMS256]);
+  launch_pdl(k_pme_gather_b, dim3(t.n[BT_ATOMS256]), dim3(256), 0, st, args, t.tab[BT_ATOMS256]);
 }
 
 }  // namespace fzk
