@@ -5,6 +5,7 @@
 namespace fzk {
 
 constexpr int kColCap = 4096;  // atoms per column sorted in shared memory
+constexpr int kWarpsPerCta = 8;  // warps of a pair-kernel CTA
 enum : int {
   CNT_TILES = 0, CNT_MASKS, CNT_SLOTS, CNT_REBUILDS, CNT_PRUNES, CNT_WORK, CNT_ITEMS, CNT_COUNT = 8
 };
