@@ -691,6 +691,7 @@ def main():
     nsd = 86.4 * dt_fs / ms_step
     value = nsd * world
 
+    shapes = sysm.launch_shapes()
     # per-stage breakdown (separate, untimed run with events between stages)
     sysm.stage_timing(True)
     sysm.SingleStep(50)
@@ -766,7 +767,8 @@ def main():
                 "config": {"workload": WORKLOAD, "natom": natom, "parallelism": f"replicas x{world}",
                            "preparation": f"{a.equil} untimed MD steps with 300 K velocity reassignment every 100",
                            "l2": "flushed (256 MB write) before every timed step",
-                           "pairs_within_cutoff": pairs},
+                           "pairs_within_cutoff": pairs,
+                           "launch_shapes": shapes},
                 "atom_steps_per_s": natom * world / (ms_step * 1e-3),
                 "step_roofline": {"t_ideal_ms": t_ideal * 1e3, "frac": t_ideal * 1e3 / ms_step,
                                   "model": "60 FLOP/pair / FP32 peak + (56N + 24K^3 + 120N) B / HBM"},

@@ -88,7 +88,7 @@ class Info(C.Structure):
 EXPORTS = ["fz_last_error", "fz_version", "fz_read_input", "fz_load_system", "fz_get_info", "fz_get_array",
            "fz_free", "fz_upload", "fz_reassign_velocities", "fz_compute_forces", "fz_compute_forces_terms", "fz_step", "fz_eval_props",
            "fz_get_positions", "fz_set_positions", "fz_get_velocities", "fz_set_velocities", "fz_get_forces",
-           "fz_get_forces_fixed", "fz_set_state_f32", "fz_get_state_f32", "fz_get_counters", "fz_sync",
+           "fz_get_forces_fixed", "fz_set_state_f32", "fz_get_state_f32", "fz_get_counters", "fz_get_launch_shapes", "fz_sync",
            "fz_stream", "fz_set_stage_timing", "fz_get_stage_times", "fz_measure_fp32_peak",
            "fz_pme_reciprocal_static", "fz_batch_create", "fz_batch_add", "fz_batch_step", "fz_batch_free",
            "fz_set_barostat", "fz_get_virial", "fz_batch_remove", "fz_batch_size", "fz_server_create",
@@ -134,6 +134,7 @@ def lib():
             "fz_set_state_f32": ([vp, vp, vp], C.c_int),
             "fz_get_state_f32": ([vp, vp, vp], C.c_int),
             "fz_get_counters": ([vp, C.POINTER(C.c_longlong)], C.c_int),
+            "fz_get_launch_shapes": ([vp, C.POINTER(C.c_int)], C.c_int),
             "fz_sync": ([vp], C.c_int),
             "fz_set_stage_timing": ([vp, C.c_int], C.c_int),
             "fz_get_stage_times": ([vp, dp], C.c_int),
@@ -337,6 +338,14 @@ class FenZi:
         out = (C.c_longlong * 4)()
         _check(lib().fz_get_counters(self.h, out))
         return dict(launches=out[0], rebuilds=out[1], pair_slots=out[2], prunes=out[3])
+
+    def launch_shapes(self):
+        """Launch shapes in use: pair tiles per work item, pair-kernel CTAs per SM, PME
+        brick edge per dimension, gather kernel, and whether the autotuner picked them."""
+        out = (C.c_int * 7)()
+        _check(lib().fz_get_launch_shapes(self.h, out))
+        return dict(chunk_tiles=out[0], nb_ctas_per_sm=out[1], pme_brick=[out[2], out[3], out[4]],
+                    gather={0: "auto", 1: "brick", 2: "atom"}[out[5]], autotuned=bool(out[6]))
 
     def stage_timing(self, enable=True):
         _check(lib().fz_set_stage_timing(self.h, 1 if enable else 0))

@@ -15,6 +15,11 @@
 // device status word once per call.
 #include "engine.h"
 
+#include <algorithm>
+#include <array>
+#include <map>
+#include <mutex>
+
 namespace fz {
 
 void destroy_engine(Engine* e) { delete e; }
@@ -29,6 +34,24 @@ static int brick_edge(int K) {
   for (int d = 4; d <= K; ++d)
     if (K % d == 0) return d;
   return K;
+}
+
+// PME brick shapes the autotuner tries: the default edge, then for each target t the
+// largest divisor of K in [4, t] per dimension (cubic grids give cubic bricks)
+static std::vector<std::array<int, 3>> brick_candidates(const int K[3]) {
+  std::vector<std::array<int, 3>> out;
+  out.push_back({brick_edge(K[0]), brick_edge(K[1]), brick_edge(K[2])});
+  for (int t : {4, 6, 8, 12, 16}) {
+    std::array<int, 3> b;
+    for (int d = 0; d < 3; ++d) {
+      int best = 0;
+      for (int q = 4; q <= t; ++q)
+        if (K[d] % q == 0) best = q;
+      b[d] = best ? best : brick_edge(K[d]);
+    }
+    if (std::find(out.begin(), out.end(), b) == out.end()) out.push_back(b);
+  }
+  return out;
 }
 
 static bool fft_size_ok(int n) {
@@ -47,6 +70,136 @@ static double bmod2(int m, int K) {
     im += M4v[k] * std::sin(a);
   }
   return 1.0 / (re * re + im * im);
+}
+
+// ---------------------------------------------------------------- autotuner
+// Picks launch shapes that leave every result bit-identical, so a timing-dependent
+// choice never changes a force: pair-kernel CTAs per SM (the pair kernel's grid; each
+// work item's forces are summed and flushed alike whichever warp takes it), the PME
+// brick edge (the block shape of the charge spread and of the gather: grid charges
+// are integer sums) and the gather kernel (per brick or per atom, the same sums in
+// the same order).  The tiles per work item are not tuned: an item's i force is
+// summed in FP32 before its fixed-point flush, so that size is a fixed rule of the
+// tile count.  Each candidate is timed on the device with CUDA events (the best of 3
+// trials of 3 launches, after 2 warm-up launches), one knob at a time from the
+// defaults; a candidate replaces the current choice only when at least 1 % faster.
+// Choices are cached per shape (grid, atom count in eighth-octave buckets, pair tiles
+// in quarter-octave buckets), so batch members and served jobs of one shape tune once
+// per process.  FZ_AUTOTUNE=0 keeps the defaults; FZ_NB_CTAS_PER_SM, FZ_PME_BRICK and
+// FZ_PME_GATHER fix their knob.
+namespace {
+struct TunedShape {
+  int per_sm, B[3], gather;
+};
+std::mutex g_tune_mu;
+std::map<std::array<long long, 5>, TunedShape> g_tune_cache;
+
+template <class F>
+float time_launches(cudaStream_t st, F&& launch) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  launch();
+  launch();
+  float best = 3e38f;
+  for (int t = 0; t < 3; ++t) {
+    cudaEventRecord(a, st);
+    for (int k = 0; k < 3; ++k) launch();
+    cudaEventRecord(b, st);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    best = std::min(best, ms);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return best;
+}
+}  // namespace
+
+static void set_per_sm(Engine* e, int per) {
+  e->nb_per_sm = per;
+  e->nb_grid = e->n_sm * per;
+}
+
+static void set_bricks(Engine* e, const std::array<int, 3>& b) {
+  for (int d = 0; d < 3; ++d) {
+    e->B[d] = b[d];
+    e->nbk[d] = e->K[d] / b[d];
+  }
+}
+
+static fz_status autotune(Engine* e) {
+  if (const char* v = std::getenv("FZ_AUTOTUNE"))
+    if (std::atoi(v) == 0) return FZ_OK;
+  // a shape fixed by the environment is not tuned, and such runs bypass the cache
+  const bool fix_per_sm = std::getenv("FZ_NB_CTAS_PER_SM") != nullptr;
+  const bool fix_brick = std::getenv("FZ_PME_BRICK") != nullptr;
+  const bool fix_gather = std::getenv("FZ_PME_GATHER") != nullptr;
+  const bool cached = !(fix_per_sm || fix_brick || fix_gather);
+  const std::array<long long, 5> key = {e->K[0], e->K[1], e->K[2], (long long)std::floor(8.0 * std::log2((double)e->n)),
+                                        (long long)std::floor(4.0 * std::log2(1.0 + e->tiles))};
+  if (cached) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      const TunedShape& t = it->second;
+      set_per_sm(e, t.per_sm);
+      set_bricks(e, {t.B[0], t.B[1], t.B[2]});
+      e->gather_mode = t.gather;
+      e->tuned = true;
+      return FZ_OK;
+    }
+  }
+  // pair-kernel CTAs per SM
+  if (!fix_per_sm) {
+    const int p0 = e->nb_per_sm;
+    float best = time_launches(e->st, [&] { fzk::launch_nonbonded(e->nb_args(), false, e->st); });
+    int pick = p0;
+    for (int per : {4, 3, 2}) {
+      if (per == p0) continue;
+      set_per_sm(e, per);
+      const float t = time_launches(e->st, [&] { fzk::launch_nonbonded(e->nb_args(), false, e->st); });
+      if (t < 0.99f * best) {
+        best = t;
+        pick = per;
+      }
+    }
+    set_per_sm(e, pick);
+  }
+  // PME brick edge x gather kernel
+  if (!(fix_brick && fix_gather)) {
+    std::vector<std::array<int, 3>> cands = brick_candidates(e->K);
+    if (fix_brick) cands = {{e->B[0], e->B[1], e->B[2]}};
+    std::array<int, 3> bpick = cands[0];
+    int gpick = 0;
+    set_bricks(e, bpick);
+    e->gather_mode = 0;
+    float best = time_launches(e->st, [&] { fzk::launch_pme(e->pme_args(), false, e->st); });
+    for (const auto& b : cands)
+      for (int g : {1, 2}) {
+        set_bricks(e, b);
+        e->gather_mode = g;
+        const float t = time_launches(e->st, [&] { fzk::launch_pme(e->pme_args(), false, e->st); });
+        if (t < 0.99f * best) {
+          best = t;
+          bpick = b;
+          gpick = g;
+        }
+      }
+    set_bricks(e, bpick);
+    e->gather_mode = gpick;
+  }
+  // the timed launches added forces: the first step starts from a zeroed accumulator
+  FZ_CUDA(cudaMemsetAsync(e->facc, 0, 3 * sizeof(long long) * e->n, e->st));
+  FZ_CUDA(cudaStreamSynchronize(e->st));
+  FZ_CUDA(cudaGetLastError());
+  e->tuned = true;
+  if (cached) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = TunedShape{e->nb_per_sm, {e->B[0], e->B[1], e->B[2]}, e->gather_mode};
+  }
+  return e->check();
 }
 
 static fz_status build_engine(fz_system* s, int device, void* stream) {
@@ -130,9 +283,14 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
     e->K[d] = c.pme_grid[d];
     if (!fft_size_ok(e->K[d])) return fail(FZ_ERR_ARG, "PME grid sizes must be 2^a 3^b 5^c in [2, 1024]");
     e->B[d] = brick_edge(e->K[d]);
+    // FZ_PME_BRICK=t: the largest divisor of K in [4, t]
+    if (const char* v = std::getenv("FZ_PME_BRICK"))
+      for (int q = 4; q <= std::atoi(v); ++q)
+        if (e->K[d] % q == 0) e->B[d] = q;
     e->nbk[d] = e->K[d] / e->B[d];
     p.K[d] = e->K[d];
   }
+  if (const char* v = std::getenv("FZ_PME_GATHER")) e->gather_mode = std::max(0, std::min(2, std::atoi(v)));
   // per-block list capacity: atoms within rlist of a block box (Minkowski volume of a
   // box ~1.4 a), with room for blocks that see all their neighbours at higher index
   const double ab = 1.4 * a, R = plist;
@@ -182,6 +340,7 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
     const int per = v ? std::max(1, std::min(4, std::atoi(v))) : 4;
     e->nb_grid = dev_sms * per;
     e->nb_per_sm = per;
+    e->n_sm = dev_sms;
   }
   // ---- atom arrays
   std::vector<float4> pos4(n), vel4(n);
@@ -385,7 +544,9 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
   // ---- PME
   {
     const int Kx = e->K[0], Ky = e->K[1], Kz = e->K[2];
-    const int nbr = e->nbk[0] * e->nbk[1] * e->nbk[2];
+    // brick lists sized for the candidate brick shape with the most bricks
+    int nbr = e->nbk[0] * e->nbk[1] * e->nbk[2];
+    for (const auto& b : brick_candidates(e->K)) nbr = std::max(nbr, (Kx / b[0]) * (Ky / b[1]) * (Kz / b[2]));
     if ((r = e->alloc(&e->brick_of, n)) || (r = e->alloc(&e->brick_count, nbr)) ||
         (r = e->alloc(&e->brick_cursor, nbr)) || (r = e->alloc(&e->brick_start, nbr + 1)) ||
         (r = e->alloc(&e->brick_atoms, n)) || (r = e->alloc(&e->grid, (size_t)Kx * Ky * Kz)) ||
@@ -441,12 +602,14 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
   }
   // tiles per pair-kernel work item: ~16 items per pair-kernel warp, 2 to 4 tiles,
   // so the warps run out of work together (the last items are short); measured at
-  // 230,400 atoms (ms/step): 64 tiles 0.544, 16 0.532, 8 0.526, 4 0.526, 3 0.526, 2 0.539
+  // 230,400 atoms (ms/step): 64 tiles 0.544, 16 0.532, 8 0.526, 4 0.526, 3 0.526, 2 0.539.
+  // This is the default; the autotuner below times the alternatives on the device.
   {
     int cnt2[fzk::CNT_COUNT];
     FZ_CUDA(cudaMemcpyAsync(cnt2, e->counters, sizeof(cnt2), cudaMemcpyDeviceToHost, e->st));
     FZ_CUDA(cudaStreamSynchronize(e->st));
-    int want = std::max(2, std::min(4, cnt2[fzk::CNT_TILES] / (e->nb_grid * fzk::kWarpsPerCta * 16)));
+    e->tiles = cnt2[fzk::CNT_TILES];
+    int want = std::max(2, std::min(4, e->tiles / (e->n_sm * 4 * fzk::kWarpsPerCta * 16)));
     if (const char* v = std::getenv("FZ_CHUNK_TILES")) want = std::max(1, std::min(64, std::atoi(v)));
     if (want != e->chunk) {
       e->chunk = want;
@@ -454,6 +617,7 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
       fzk::launch_rebuild(e->rebuild_args(), e->st);
     }
   }
+  if ((r = autotune(e))) return r;
   FZ_CUDA(cudaStreamSynchronize(e->st));
   return e->check();
 }
@@ -958,6 +1122,19 @@ extern "C" fz_status fz_get_counters(fz_system* s, long long* out4) {
   out4[1] = cnt[fzk::CNT_REBUILDS];
   out4[2] = (long long)cnt[fzk::CNT_TILES] * fzk::kIG * 32;
   out4[3] = cnt[fzk::CNT_PRUNES];
+  return FZ_OK;
+}
+
+extern "C" fz_status fz_get_launch_shapes(fz_system* s, int* out7) {
+  fz_status r;
+  if ((r = need_engine(s))) return r;
+  if (!out7) return fail(FZ_ERR_ARG, "null output");
+  const Engine* e = s->eng;
+  out7[0] = e->chunk;
+  out7[1] = e->nb_per_sm;
+  for (int d = 0; d < 3; ++d) out7[2 + d] = e->B[d];
+  out7[5] = e->gather_mode;
+  out7[6] = e->tuned ? 1 : 0;
   return FZ_OK;
 }
 

@@ -28,7 +28,7 @@ struct Engine {
   int n = 0, nunits = 0, ncol = 0, nslots = 0, mask_cap = 0, all_images = 0;
   int ocap = 0;            // per-block pair-list capacity (multiple of 32)
   float rp2 = 0.f, prune_half2 = 0.f;
-  int nb_grid = 0, nb_per_sm = 3;
+  int nb_grid = 0, nb_per_sm = 3, n_sm = 148;
   int dcx = 1, dcy = 1;
   int* blk_col = nullptr;
   std::vector<void*> allocs;
@@ -45,6 +45,7 @@ struct Engine {
   float4* pos_prune = nullptr;
   int2* items = nullptr;
   int chunk = 16;
+  int tiles = 0;  // pair tiles of the first pruned list (sizes the work items)
   int *excl_off = nullptr, *excl_idx = nullptr;
   int *xn = nullptr, *xs = nullptr, xmax = 1;  // per-slot excluded-partner slots
   int *flag = nullptr, *counters = nullptr, *status = nullptr;
@@ -73,6 +74,8 @@ struct Engine {
   float4* unit_d = nullptr;
   // PME
   int K[3] = {0, 0, 0}, B[3] = {0, 0, 0}, nbk[3] = {0, 0, 0};
+  int gather_mode = 0;  // PME gather kernel (PmeArgs::gather)
+  bool tuned = false;   // launch shapes picked by the autotuner
   int *brick_of = nullptr, *brick_count = nullptr, *brick_cursor = nullptr, *brick_start = nullptr,
       *brick_atoms = nullptr;
   float* grid = nullptr;
@@ -275,6 +278,7 @@ struct Engine {
     a.facc = facc;
     a.energy = energy;
     a.status = status;
+    a.gather = gather_mode;
     return a;
   }
   fzk::BondedArgs bonded_args() const {

@@ -123,6 +123,7 @@ struct PmeArgs {
   long long* facc;
   long long* energy;
   int* status;
+  int gather;  // gather kernel: 1 one CTA per brick, 2 one thread per atom, 0 by atoms per brick
 };
 void launch_pme(const PmeArgs& a, bool energy, cudaStream_t st);
 // batched PME: the systems of one grid size share the FFT launches

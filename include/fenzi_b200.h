@@ -204,6 +204,14 @@ fz_status fz_get_state_f32(fz_system* sys, float* pos3n, float* vel3n);
  * [2] pair slots (i x j pairs the pair kernel evaluates per step, within or beyond the
  * cutoff) of the current pruned list, [3] list prunes. */
 fz_status fz_get_counters(fz_system* sys, long long* out4);
+/* Launch shapes in use: [0] pair tiles per pair-kernel work item (a fixed rule of the
+ * tile count), [1] pair-kernel CTAs per SM, [2..4] PME brick edge per dimension
+ * (charge-spread and gather block shape), [5] gather kernel (0 by atoms per brick, 1
+ * one CTA per brick, 2 one thread per atom), [6] 1 when the autotuner picked [1..5]
+ * at fz_upload (unless FZ_AUTOTUNE=0; every shape it can pick gives bit-identical
+ * results).  No reference counterpart: the reference fixes its block sizes at
+ * compile time (src/prmread.cu:109-115). */
+fz_status fz_get_launch_shapes(fz_system* sys, int* out7);
 /* Virial diagonal accumulated by the last fz_compute_forces_terms(..., energies = 1)
  * (force terms only: no constraint or kinetic part). */
 fz_status fz_get_virial(fz_system* sys, double* out3);
