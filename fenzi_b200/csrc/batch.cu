@@ -193,8 +193,10 @@ static fz_status build_batch_kernels(fz_batch* b) {
   std::vector<ClassAcc> cls;
   struct SizeAcc { int N; std::vector<int4> plane, z; };
   std::vector<SizeAcc> sizes;
-  // pair-kernel CTAs: the batch's total is that of one large system (nb_grid, ~4 per
-  // SM), shared out in proportion to the members' atoms, at least one each
+  // pair-kernel CTAs: the batch's total is one full wave of the batched pair kernel
+  // (kNbBatchCtasPerSm per SM), shared out in proportion to the members' atoms, at
+  // least one each.  Not the members' own nb_grid: the autotuner sizes that for a
+  // member running alone, where a small system often does best on 2 CTAs per SM.
   long long natoms = 0;
   for (const fz_system* s : b->systems) natoms += s->top.n;
   for (int i = 0; i < ns; ++i) {
@@ -213,7 +215,7 @@ static fz_status build_batch_kernels(fz_batch* b) {
     add_blocks(tabs[fzk::BT_SLOTS256], i, (p.nslots + 255) / 256);
     add_blocks(tabs[fzk::BT_BLOCKS8], i, (p.nslots / 32 + 7) / 8);
     add_blocks(tabs[fzk::BT_NB], i,
-               std::max(1, (int)std::lround((double)e->nb_grid * p.n / (double)std::max(1LL, natoms))));
+               std::max(1, (int)std::lround((double)e->n_sm * fzk::kNbBatchCtasPerSm * p.n / (double)std::max(1LL, natoms))));
     add_blocks(tabs[fzk::BT_BONDED], i, fzk::bonded_blocks(bd.back()));
     add_blocks(tabs[fzk::BT_BRICKS256], i, (nbr + 255) / 256);
     add_blocks(tabs[fzk::BT_BRICKS], i, nbr);

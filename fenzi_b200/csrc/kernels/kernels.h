@@ -6,6 +6,7 @@ namespace fzk {
 
 constexpr int kColCap = 4096;  // atoms per column sorted in shared memory
 constexpr int kWarpsPerCta = 8;  // warps of a pair-kernel CTA
+constexpr int kNbBatchCtasPerSm = 4;  // CTAs per SM the batched pair kernel is built and launched for
 enum : int {
   CNT_TILES = 0, CNT_MASKS, CNT_SLOTS, CNT_REBUILDS, CNT_PRUNES, CNT_WORK, CNT_ITEMS, CNT_COUNT = 8
 };

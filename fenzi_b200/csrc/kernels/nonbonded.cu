@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(256, MINB)
 }
 
 // batched: every CTA serves one system's work queue (force variant only)
-__global__ void __launch_bounds__(256, 4) k_nonbonded_b(const NonbondedArgs* __restrict__ args,
+__global__ void __launch_bounds__(256, kNbBatchCtasPerSm) k_nonbonded_b(const NonbondedArgs* __restrict__ args,
                                                         const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const NonbondedArgs a = args[t.x];
