@@ -15,7 +15,15 @@
 
 namespace fzk {
 
-__device__ __forceinline__ float3 sub3(float4 a, float4 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+// minimum-image difference a - b of two FP32 positions, formed in FP64 and rounded once:
+// two atoms of a term split by the periodic boundary are about L apart before the image
+// shift, and an FP32 difference would round at the ulp of L (up to 3.8e-6 A for
+// L = 130 A), a 1e-4 relative error in the force of a stiff bond
+__device__ __forceinline__ float3 image_diff(float4 a, float4 b, const SysParams& p) {
+  double d[3] = {(double)a.x - (double)b.x, (double)a.y - (double)b.y, (double)a.z - (double)b.z};
+  min_image_d(d, p);
+  return make_float3((float)d[0], (float)d[1], (float)d[2]);
+}
 __device__ __forceinline__ float dot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 __device__ __forceinline__ float3 cross(float3 a, float3 b) {
   return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
@@ -31,9 +39,9 @@ __device__ __forceinline__ void addf(long long* facc, int n, int i, float3 f) {
 __device__ __forceinline__ bool dihedral_geom(float4 ri, float4 rj, float4 rk, float4 rl, const SysParams& p,
                                               float* cphi, float* sphi, float3* gi, float3* gj, float3* gk,
                                               float3* gl, float3* rel) {
-  const float3 F = min_image(sub3(ri, rj), p);
-  const float3 G = min_image(sub3(rj, rk), p);
-  const float3 H = min_image(sub3(rl, rk), p);
+  const float3 F = image_diff(ri, rj, p);
+  const float3 G = image_diff(rj, rk, p);
+  const float3 H = image_diff(rl, rk, p);
   // positions relative to atom j: i - j = F, k - j = -G, l - j = H - G
   rel[0] = F;
   rel[1] = make_float3(-G.x, -G.y, -G.z);
@@ -67,7 +75,7 @@ __device__ __forceinline__ void bonded_body(const BondedArgs& a, int bid) {
   if (r < a.nbond) {
     const int2 b = a.bond[r];
     const float2 pr = a.bond_prm[r];
-    const float3 d = min_image(sub3(a.pos4[b.x], a.pos4[b.y]), p);
+    const float3 d = image_diff(a.pos4[b.x], a.pos4[b.y], p);
     const float rr = sqrtf(dot(d, d));
     const float dr = rr - pr.y;
     const float f = rr > 0.f ? -2.f * pr.x * dr / rr : 0.f;
@@ -83,8 +91,8 @@ __device__ __forceinline__ void bonded_body(const BondedArgs& a, int bid) {
     const int4 q = a.angle[r];
     const float2 pr = a.angle_prm[r];
     const float4 rj = a.pos4[q.y];
-    const float3 u = min_image(sub3(a.pos4[q.x], rj), p);
-    const float3 v = min_image(sub3(a.pos4[q.z], rj), p);
+    const float3 u = image_diff(a.pos4[q.x], rj, p);
+    const float3 v = image_diff(a.pos4[q.z], rj, p);
     const float uu = dot(u, u), vv = dot(v, v), uv = dot(u, v);
     const float3 uxv = cross(u, v);
     const float ruv = rsqrtf(uu * vv);
@@ -112,7 +120,7 @@ __device__ __forceinline__ void bonded_body(const BondedArgs& a, int bid) {
   } else if ((r -= a.nangle) < a.nub) {
     const int2 b = a.ub[r];
     const float2 pr = a.ub_prm[r];
-    const float3 d = min_image(sub3(a.pos4[b.x], a.pos4[b.y]), p);
+    const float3 d = image_diff(a.pos4[b.x], a.pos4[b.y], p);
     const float rr = sqrtf(dot(d, d));
     const float dr = rr - pr.y;
     const float f = rr > 0.f ? -2.f * pr.x * dr / rr : 0.f;
@@ -200,7 +208,7 @@ __device__ __forceinline__ void bonded_body(const BondedArgs& a, int bid) {
     // 1-4: 1-4 LJ (switched) + erfc Coulomb, no cutoff test (src/bonded_forces.cu:1155-1268)
     const int2 b = a.p14[r];
     const float4 ri = a.pos4[b.x], rj = a.pos4[b.y];
-    const float3 d = min_image(sub3(ri, rj), p);
+    const float3 d = image_diff(ri, rj, p);
     const float r2 = dot(d, d);
     const float rr = sqrtf(r2), r2inv = 1.f / r2;
     const float2 ls = a.lj14[a.type[b.x] * (p.ntypes + 1) + a.type[b.y]];

@@ -20,6 +20,7 @@ def system(key="small", **kw):
     presets = {
         "small": dict(name="custom", nw=400, nchains=2, chain_len=10, rc=8.0, ron=6.5, seed=7),
         "water3000": dict(name="water3000"),
+        "large230k": dict(name="large230k", seed=2345),
         "mid": dict(name="custom", nw=8760, nchains=6, chain_len=30, box=64.0, kgrid=64, rc=10.0, ron=8.0, seed=11),
         "tiny": dict(name="custom", nw=60, nchains=1, chain_len=8, box=14.0, kgrid=16, rc=6.0, ron=5.0, seed=3),
     }
