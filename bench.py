@@ -46,7 +46,7 @@ FLOP_PER_PAIR = 60  # algorithmic FP32 work per in-cutoff pair (FMA = 2)
 def args_():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=30)
     ap.add_argument("--impl", default="fenzi", choices=["fenzi", "reference"])
     ap.add_argument("--workload", default="large230k")
@@ -90,7 +90,7 @@ class Clocks:
     def start(self):
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                       "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                       "-lms", "100", "-i", str(self.device)], stdout=subprocess.PIPE,
                                       stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
