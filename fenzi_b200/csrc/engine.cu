@@ -283,9 +283,10 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
     e->K[d] = c.pme_grid[d];
     if (!fft_size_ok(e->K[d])) return fail(FZ_ERR_ARG, "PME grid sizes must be 2^a 3^b 5^c in [2, 1024]");
     e->B[d] = brick_edge(e->K[d]);
-    // FZ_PME_BRICK=t: the largest divisor of K in [4, t]
+    // FZ_PME_BRICK=t: the largest divisor of K in [4, min(t, 16)] (the spread and gather
+    // hold a (B+3)^3 region in shared memory sized for bricks of at most 16)
     if (const char* v = std::getenv("FZ_PME_BRICK"))
-      for (int q = 4; q <= std::atoi(v); ++q)
+      for (int q = 4; q <= std::min(std::atoi(v), 16); ++q)
         if (e->K[d] % q == 0) e->B[d] = q;
     e->nbk[d] = e->K[d] / e->B[d];
     p.K[d] = e->K[d];

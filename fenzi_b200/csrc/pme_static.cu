@@ -5,13 +5,16 @@
 // device memory after start-up.  fz_pme_reciprocal_static() serves them: it runs the
 // same spread / R2C-FFT + influence function / C2R / gather kernels as the system
 // path, but every scratch buffer lives in the fixed-size file-scope __device__ arrays
-// below (about 11 MB on every GPU that loads the library, held until the process
+// below (about 4.4 MB on every GPU that loads the library, held until the process
 // exits).  The caller passes its own device input (float4 x, y, z, q per atom) and
-// output (int64 fixed-point forces) buffers.
+// output (int64 fixed-point forces) buffers.  The per-call tables (twiddles, B-spline
+// moduli times the Gaussian, |m|^2) are computed on the device into the scratch, so a
+// call copies nothing from host memory; only energy_out reads a value back.
 //
 // Set-up: the first call on a device, with that device current, resolves the device
 // addresses of the scratch arrays with cudaGetSymbolAddress and caches them per
-// device; make that first call before any stream capture.  All calls share the same
+// device; make that first call before any stream capture.  The caller's current device
+// is restored before every return.  All calls share the same
 // scratch, which keeps the last call's contents: each call clears what must start at
 // zero, and calls that overlap on the GPU (different streams, or different host
 // threads on the same device) race on the scratch and must be serialised by the caller.
@@ -41,12 +44,11 @@ __device__ __align__(256) float2 s_tw[3][kSMaxK];
 __device__ __align__(256) float s_gfac[3][kSMaxK];
 __device__ __align__(256) float s_f2[3][kSMaxK];
 __device__ __align__(256) long long s_energy[fzk::EN_COUNT];
-__device__ __align__(256) int s_status[1];
 
 struct Scratch {
   float* grid;
   float2* cgrid;
-  int *brick_of, *brick_atoms, *brick_count, *brick_cursor, *brick_start, *status;
+  int *brick_of, *brick_atoms, *brick_count, *brick_cursor, *brick_start;
   float2* tw;
   float *gfac, *f2;
   long long* energy;
@@ -73,8 +75,7 @@ fz_status setup(int device, Scratch** out) {
         (e = cudaGetSymbolAddress((void**)&tw, s_tw)) != cudaSuccess ||
         (e = cudaGetSymbolAddress((void**)&gf, s_gfac)) != cudaSuccess ||
         (e = cudaGetSymbolAddress((void**)&f2, s_f2)) != cudaSuccess ||
-        (e = cudaGetSymbolAddress((void**)&s.energy, s_energy)) != cudaSuccess ||
-        (e = cudaGetSymbolAddress((void**)&s.status, s_status)) != cudaSuccess)
+        (e = cudaGetSymbolAddress((void**)&s.energy, s_energy)) != cudaSuccess)
       return fail(FZ_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
     s.tw = tw;
     s.gfac = gf;
@@ -104,6 +105,41 @@ static int brick_edge(int K) {
   return K;
 }
 
+// Per-call tables in FP64, rounded once to FP32, with the same expressions as the system
+// path's host tables: twiddles e^{-2 pi i m/K}, f^2 = (m'/L)^2 and
+// |b(m)|^2 exp(-pi^2 f^2 / beta^2) (order-4 Euler exponential-spline moduli); also clears
+// the energy slots.  One block per dimension, one thread per grid index.
+__global__ void k_static_tables(int K0, int K1, int K2, double L0, double L1, double L2, double beta) {
+  const int d = blockIdx.x;
+  const int Kd = d == 0 ? K0 : (d == 1 ? K1 : K2);
+  const double L = d == 0 ? L0 : (d == 1 ? L1 : L2);
+  if (d == 0)
+    for (int k = threadIdx.x; k < fzk::EN_COUNT; k += blockDim.x) s_energy[k] = 0;
+  const double b2 = beta * beta;
+  for (int m = threadIdx.x; m < Kd; m += blockDim.x) {
+    const double ang = -2.0 * M_PI * m / Kd;
+    s_tw[d][m] = make_float2((float)cos(ang), (float)sin(ang));
+    const double f = (m <= Kd / 2 ? m : m - Kd) / L;
+    s_f2[d][m] = (float)(f * f);
+    const double M4v[3] = {1.0 / 6.0, 4.0 / 6.0, 1.0 / 6.0};
+    double re = 0, im = 0;
+    for (int k = 0; k < 3; ++k) {
+      const double a = 2.0 * M_PI * (double)m * k / Kd;
+      re += M4v[k] * cos(a);
+      im += M4v[k] * sin(a);
+    }
+    s_gfac[d][m] = (float)((1.0 / (re * re + im * im)) * exp(-M_PI * M_PI * f * f / b2));
+  }
+}
+
+// restores the caller's current device when the entry point returns
+struct DeviceGuard {
+  int prev = -1;
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
 }  // namespace
 }  // namespace fz
 
@@ -122,34 +158,17 @@ extern "C" fz_status fz_pme_reciprocal_static(int device, void* stream, const fl
     if (!(box[d] > 0)) return fail(FZ_ERR_ARG, "fz_pme_reciprocal_static: box edges must be positive");
   }
   if (!(beta > 0)) return fail(FZ_ERR_ARG, "fz_pme_reciprocal_static: beta must be positive");
-  cudaError_t ce = cudaSetDevice(device);
-  if (ce != cudaSuccess) return fail(FZ_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(ce));
+  DeviceGuard guard;
+  cudaError_t ce = cudaGetDevice(&guard.prev);
+  if (ce != cudaSuccess) return fail(FZ_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(ce));
+  if ((ce = cudaSetDevice(device)) != cudaSuccess)
+    return fail(FZ_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(ce));
   Scratch* s = nullptr;
   fz_status r = setup(device, &s);
   if (r) return r;
   cudaStream_t st = (cudaStream_t)stream;
-  // per-call tables (twiddles, B-spline moduli x Gaussian, |m|^2), from host memory
-  float2 tw[3][kSMaxK];
-  float gfac[3][kSMaxK], f2[3][kSMaxK];
-  const double b2 = beta * beta;
-  for (int d = 0; d < 3; ++d)
-    for (int m = 0; m < K[d]; ++m) {
-      const double ang = -2.0 * M_PI * m / K[d];
-      tw[d][m] = make_float2((float)std::cos(ang), (float)std::sin(ang));
-      const double f = (m <= K[d] / 2 ? m : m - K[d]) / box[d];
-      f2[d][m] = (float)(f * f);
-      double re = 0, im = 0;
-      const double M4v[3] = {1.0 / 6.0, 4.0 / 6.0, 1.0 / 6.0};
-      for (int k = 0; k < 3; ++k) {
-        re += M4v[k] * std::cos(2.0 * M_PI * m * k / K[d]);
-        im += M4v[k] * std::sin(2.0 * M_PI * m * k / K[d]);
-      }
-      gfac[d][m] = (float)(std::exp(-M_PI * M_PI * f * f / b2) / (re * re + im * im));
-    }
-  if ((ce = cudaMemcpyAsync(s->tw, tw, sizeof(tw), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
-      (ce = cudaMemcpyAsync(s->gfac, gfac, sizeof(gfac), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
-      (ce = cudaMemcpyAsync(s->f2, f2, sizeof(f2), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
-      (ce = cudaMemsetAsync(s->energy, 0, sizeof(long long) * fzk::EN_COUNT, st)) != cudaSuccess ||
+  k_static_tables<<<3, 64, 0, st>>>(K[0], K[1], K[2], box[0], box[1], box[2], beta);
+  if ((ce = cudaGetLastError()) != cudaSuccess ||
       (ce = cudaMemsetAsync(facc, 0, sizeof(long long) * 3 * (size_t)n, st)) != cudaSuccess)
     return fail(FZ_ERR_CUDA, std::string("fz_pme_reciprocal_static: ") + cudaGetErrorString(ce));
   fzk::PmeArgs a{};
@@ -178,7 +197,7 @@ extern "C" fz_status fz_pme_reciprocal_static(int device, void* stream, const fl
   a.gscale = (float)(kCC / (M_PI * box[0] * box[1] * box[2]));
   a.facc = facc;
   a.energy = s->energy;
-  a.status = s->status;
+  a.status = nullptr;  // the PME kernels report no status
   fzk::launch_pme(a, energy_out != nullptr, st);
   if ((ce = cudaGetLastError()) != cudaSuccess)
     return fail(FZ_ERR_CUDA, std::string("fz_pme_reciprocal_static launch: ") + cudaGetErrorString(ce));

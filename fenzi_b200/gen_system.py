@@ -41,7 +41,7 @@ EXTRA_IMPR = (1.5, 0.0)
 EXTRA_NBFIX = (0.12, 3.7)          # CTU-OT emin, rmin
 EXTRA_14 = (0.05, 1.9)             # CTU 1-4 eps, rmin/2
 WATER_BOND = (450.0, ROH)
-WATER_HH = (0.0, RHH)
+WATER_HH = (0.0, round(RHH, 4))  # as written to the PRM (8.4f)
 WATER_ANGLE = (55.0, THOH)
 
 
@@ -347,7 +347,7 @@ def topology(s: System):
     cons = [(a, b) for a, b in s.bonds if s.mass[a] <= 1.5 or s.mass[b] <= 1.5]
     cd = []
     for a, b in cons:
-        cd.append(RHH if (s.types[a], s.types[b]) == ("HT", "HT") else ROH)
+        cd.append(WATER_HH[1] if (s.types[a], s.types[b]) == ("HT", "HT") else ROH)
     return dict(n=s.n, q=s.charge.astype(float), mass=s.mass.astype(float), type=typ, ntypes=nt,
                 eps4=eps4, sig2=sig2, eps4_14=eps4_14, sig2_14=sig2_14,
                 bond=s.bonds.astype(np.int32), bond_k=bk, bond_r0=br,

@@ -227,13 +227,15 @@ fz_status fz_measure_fp32_peak(int device, double* tflops);
 /* No counterpart in the reference.  PME reciprocal-space forces (and optionally the
  * reciprocal energy) of n atoms for callers that cannot call cudaMalloc (code living
  * inside another framework's memory pool or a pre-sized arena).  Allocates nothing:
- * scratch lives in fixed file-scope device arrays (about 11 MB on each GPU that loads
- * the library, held until exit).  pos4: device float4[n] (x, y, z, q); facc: device
- * int64[3n] fixed point (scale 2^32, x[n] y[n] z[n]), overwritten; energy_out: host
- * double or NULL (when given, the call synchronises `stream`).  Limits: n <= 262144,
- * grid sizes 2^a 3^b 5^c in 4..64.  The first call on a device resolves the scratch
- * addresses (make it before any stream capture); calls that overlap on the GPU race
- * on the shared scratch and must be serialised by the caller. */
+ * scratch lives in fixed file-scope device arrays (about 4.4 MB on each GPU that loads
+ * the library, held until exit), and the per-call tables are computed on the device, so
+ * nothing is copied from host memory.  pos4: device float4[n] (x, y, z, q); facc:
+ * device int64[3n] fixed point (scale 2^32, x[n] y[n] z[n]), overwritten; energy_out:
+ * host double or NULL (when given, the call synchronises `stream`).  Limits: n <=
+ * 262144, grid sizes 2^a 3^b 5^c in 4..64.  The caller's current device is restored
+ * on return.  The first call on a device resolves the scratch addresses (make it
+ * before any stream capture); calls that overlap on the GPU race on the shared scratch
+ * and must be serialised by the caller. */
 fz_status fz_pme_reciprocal_static(int device, void* stream, const float* pos4, int n, const double* box,
                                    const int* K, double beta, long long* facc, double* energy_out);
 /* ---- batched ensemble ------------------------------------------------- */

@@ -191,6 +191,19 @@ double bmod2(int m, int K) {
   return 1.0 / std::norm(den);
 }
 
+// C(m) = |b(m)|^2 exp(-pi^2 |m|^2 / beta^2) / |m|^2 with m the reciprocal vector of
+// grid index (mx, my, mz) (aliased to [-K/2, K/2]); 0 at m = 0.  The factor the
+// transformed charge grid is multiplied by, up to CC / (pi V) (src/cell_based_kernels.cu:1770-1826)
+double influence(int mx, int my, int mz, const int* K, const double* L, double beta, const double* bx,
+                 const double* by, const double* bz) {
+  if (mx == 0 && my == 0 && mz == 0) return 0.0;
+  const double fx = (mx <= K[0] / 2 ? mx : mx - K[0]) / L[0];
+  const double fy = (my <= K[1] / 2 ? my : my - K[1]) / L[1];
+  const double fz = (mz <= K[2] / 2 ? mz : mz - K[2]) / L[2];
+  const double m2 = fx * fx + fy * fy + fz * fz;
+  return bx[mx] * by[my] * bz[mz] * std::exp(-kPi * kPi * m2 / (beta * beta)) / m2;
+}
+
 void pme(const Orc& o, const double* pos, double* f, double* e) {
   const int Kx = o.s.K[0], Ky = o.s.K[1], Kz = o.s.K[2];
   const double* L = o.s.box;
@@ -230,25 +243,20 @@ void pme(const Orc& o, const double* pos, double* f, double* e) {
   const int nth = o.nthreads;
   fft3d(Q.data(), Kx, Ky, Kz, -1, nth);
   const double V = L[0] * L[1] * L[2];
-  const double b2 = o.s.beta * o.s.beta;
   std::vector<double> bx(Kx), by(Ky), bz(Kz);
   for (int m = 0; m < Kx; ++m) bx[m] = bmod2(m, Kx);
   for (int m = 0; m < Ky; ++m) by[m] = bmod2(m, Ky);
   for (int m = 0; m < Kz; ++m) bz[m] = bmod2(m, Kz);
   double E = 0;
   for (int mz = 0; mz < Kz; ++mz) {
-    const double fz = (mz <= Kz / 2 ? mz : mz - Kz) / L[2];
     for (int my = 0; my < Ky; ++my) {
-      const double fy = (my <= Ky / 2 ? my : my - Ky) / L[1];
       for (int mx = 0; mx < Kx; ++mx) {
-        const double fx = (mx <= Kx / 2 ? mx : mx - Kx) / L[0];
         const size_t idx = ((size_t)mz * Ky + my) * Kx + mx;
-        const double m2 = fx * fx + fy * fy + fz * fz;
         if (idx == 0) {
           Q[idx] = 0;
           continue;
         }
-        const double C = bx[mx] * by[my] * bz[mz] * std::exp(-kPi * kPi * m2 / b2) / m2;
+        const double C = influence(mx, my, mz, K, L, o.s.beta, bx.data(), by.data(), bz.data());
         E += C * std::norm(Q[idx]);
         Q[idx] *= ORC_CC / (kPi * V) * C;
       }
@@ -871,6 +879,20 @@ int orc_ewald_recip(void* h, const double* pos, int kmax, double* f, double* e) 
 
 int orc_fft3d(int nx, int ny, int nz, double* data, int sign) {
   fft3d(reinterpret_cast<cplx*>(data), nx, ny, nz, sign, 4);
+  return 0;
+}
+
+int orc_pme_influence(const int* K, const double* L, double beta, double* G) {
+  std::vector<double> b[3];
+  for (int d = 0; d < 3; ++d) {
+    b[d].resize(K[d]);
+    for (int m = 0; m < K[d]; ++m) b[d][m] = bmod2(m, K[d]);
+  }
+  for (int mz = 0; mz < K[2]; ++mz)
+    for (int my = 0; my < K[1]; ++my)
+      for (int mx = 0; mx < K[0]; ++mx)
+        G[((size_t)mz * K[1] + my) * K[0] + mx] =
+            influence(mx, my, mz, K, L, beta, b[0].data(), b[1].data(), b[2].data());
   return 0;
 }
 

@@ -26,10 +26,13 @@
  * plus a direct (non-mesh) Ewald reciprocal sum, which the reference does not have,
  * used as the truth for the PME error.
  *
- * Parity against reference OUTPUTS is unpinned: the reference ships no golden
- * energies/forces and its CUDA build does not compile with CUDA 12.9.  The
- * oracle is pinned instead by mathematical identities checked in tests/
- * (F = -dE/dr by finite differences, PME vs direct Ewald, FFT vs numpy).
+ * Pinned to the reference's own arithmetic: the reference ships no golden outputs and
+ * its CUDA build does not compile with CUDA 12.9, but its force kernels compile for the
+ * host from its sources (oracle/refbuild.py, oracle/ref_harness.cpp).  Their outputs
+ * (tests/golden/ref_terms.npz, made by tests/golden/make_ref_golden.py) agree with this
+ * oracle to 1e-12 wherever the formulas coincide, and differ exactly by the documented
+ * departures elsewhere (tests/test_ref_pin.py).  Mathematical identities are checked
+ * too (F = -dE/dr by finite differences, PME vs direct Ewald, FFT vs numpy).
  */
 #ifndef FENZI_ORACLE_H
 #define FENZI_ORACLE_H
@@ -86,6 +89,9 @@ void  orc_destroy(void* h);
 int orc_forces(void* h, const double* pos, double* f, double* e, int terms);
 /* direct reciprocal Ewald sum over |m_i| <= kmax (sphere |m~| <= kmax/min(L)) */
 int orc_ewald_recip(void* h, const double* pos, int kmax, double* f, double* e);
+/* PME influence function C(m) = |b(m)|^2 exp(-pi^2 |m|^2 / beta^2) / |m|^2 on the grid
+ * G[(mz K1 + my) K0 + mx] (0 at m = 0), the factor of the reciprocal sum up to CC/(pi V) */
+int orc_pme_influence(const int* K, const double* L, double beta, double* G);
 /* in-place 3-D complex DFT, x fastest; sign -1 forward, +1 inverse (unnormalised) */
 int orc_fft3d(int nx, int ny, int nz, double* data, int sign);
 

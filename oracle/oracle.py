@@ -36,6 +36,7 @@ def _lib():
     lib.orc_forces.argtypes = [C.c_void_p, dp, dp, dp, C.c_int]
     lib.orc_ewald_recip.argtypes = [C.c_void_p, dp, C.c_int, dp, dp]
     lib.orc_fft3d.argtypes = [C.c_int, C.c_int, C.c_int, dp, C.c_int]
+    lib.orc_pme_influence.argtypes = [C.POINTER(C.c_int), dp, C.c_double, dp]
     lib.orc_counts.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
     lib.orc_count_pairs.restype = C.c_longlong
     lib.orc_count_pairs.argtypes = [C.c_void_p, dp, C.c_double]
@@ -237,6 +238,15 @@ def fft3d(data, sign):
     nz, ny, nx = a.shape
     lib().orc_fft3d(nx, ny, nz, a.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)), int(sign))
     return a
+
+
+def pme_influence(K, box, beta):
+    """The oracle's PME influence function C(m) as a (Kz, Ky, Kx) array."""
+    Ka = (C.c_int * 3)(*[int(k) for k in K])
+    L = np.ascontiguousarray(box, np.float64)
+    G = np.zeros(int(K[0]) * int(K[1]) * int(K[2]))
+    lib().orc_pme_influence(Ka, _dp(L), float(beta), _dp(G))
+    return G.reshape(int(K[2]), int(K[1]), int(K[0]))
 
 
 def normals(n, seed, counter=0):

@@ -4,13 +4,15 @@ tests/examples_fenzi/dmpc_small (the only complete input set the reference ships
 Every number here is computed from the raw files by this script alone (no product
 code): the PSF section headers, and an independent restatement of the exclusion /
 1-4 / SHAKE-constraint rules (src/prmread.cu:1757-1761, 2928-3062) over the PSF lists.
-Run: python tests/golden/make_dmpc_small.py [reference_root]
+Run: python tests/golden/make_dmpc_small.py [reference_root]   (default $FENZI_REFERENCE)
 """
 import json
 import os
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("FENZI_REFERENCE", "")
+if not REF:
+    sys.exit("give the reference root as the argument or in $FENZI_REFERENCE")
 DECK = os.path.join(REF, "tests", "examples_fenzi", "dmpc_small")
 
 

@@ -1,5 +1,7 @@
 """Shared builders for the tests: seeded systems written through the drop-in file
-formats, loaded by the product readers, with the oracle built from the same topology."""
+formats and loaded by the product readers; the oracle is built from the generator's own
+topology (gen_system.topology: every parameter resolved without the readers), so a
+reader fault cannot hide in a force comparison."""
 import os
 import tempfile
 
@@ -8,6 +10,7 @@ import numpy as np
 from fenzi_b200 import gen_system
 
 _CACHE = {}
+_GEN_BY_DIR = {}  # input directory -> gen_system.System written there
 _TMP = tempfile.mkdtemp(prefix="fzb200_")
 
 ORACLE_BONDED = 16 | 32 | 64 | 128 | 256 | 2 | 4  # bonds angles ub dihe impr excl p14
@@ -29,6 +32,7 @@ def system(key="small", **kw):
     s = gen_system.build(**args)
     path = gen_system.write(s, os.path.join(_TMP, key))
     _CACHE[key] = (s, path)
+    _GEN_BY_DIR[os.path.realpath(os.path.dirname(path))] = s
     return s, path
 
 
@@ -39,5 +43,10 @@ def rel_rms(a, b):
 
 
 def oracle_for(fz_sys, nthreads=0):
+    """The oracle of a loaded system: from the generator's topology when the system
+    was written by system() (reader-free), else from the product readers' topology."""
     from oracle.oracle import Oracle
-    return Oracle(fz_sys.topology(), nthreads=nthreads)
+    crd = fz_sys.cfg.coordinates.decode()
+    gen = _GEN_BY_DIR.get(os.path.realpath(os.path.dirname(crd)))
+    topo = gen_system.topology(gen) if gen is not None else fz_sys.topology()
+    return Oracle(topo, nthreads=nthreads)

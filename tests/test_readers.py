@@ -10,10 +10,16 @@ from fenzi_b200 import gen_system
 from tests.helpers import system
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "dmpc_small.json")
-DMPC = "/root/reference/tests/examples_fenzi/dmpc_small/fenzi.in"
+# the reference's example deck: under $FENZI_REFERENCE, or the copy oracle/refbuild.py
+# keeps in oracle/_ref (built from the reference tree, not committed)
+_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DMPC = next((p for p in (os.path.join(os.environ.get("FENZI_REFERENCE", "-"), "tests", "examples_fenzi", "dmpc_small",
+                                      "fenzi.in"),
+                         os.path.join(_ROOT, "oracle", "_ref", "dmpc_small", "fenzi.in")) if os.path.exists(p)),
+            "")
 
 
-@pytest.mark.skipif(not os.path.exists(DMPC), reason="reference example deck not present")
+@pytest.mark.skipif(not DMPC, reason="reference example deck not present")
 def test_dmpc_small_matches_reference_headers():
     """The reference's own complete deck: counts equal the PSF headers and an
     independent restatement of the exclusion/constraint rules (golden fixture)."""
