@@ -19,7 +19,8 @@ e2e: the same metric through the C ABI with host buffers: per chunk of --chunk
 steps, host->device copy of positions+velocities from pinned memory, fz_step(chunk),
 device->host copy of positions+velocities, wall clock.
 --impl reference: the FP64 CPU oracle (the reference's own CUDA build does not
-compile with CUDA 12.9; it has no CPU path) on the same system, all host threads.
+compile with CUDA 12.9; it has no CPU path) on the same system, all host threads, W
+untimed and K timed full MD steps (about 0.6 s a step on 16 host cores), rank 0 only.
 """
 from __future__ import annotations
 
@@ -46,7 +47,7 @@ FLOP_PER_PAIR = 60  # algorithmic FP32 work per in-cutoff pair (FMA = 2)
 def args_():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=30)
     ap.add_argument("--impl", default="fenzi", choices=["fenzi", "reference"])
     ap.add_argument("--workload", default="large230k")
@@ -58,7 +59,7 @@ def args_():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ensemble", type=int, default=256,
                     help="batched-ensemble measurement (256 uneven TIP3P boxes of 648-6,000 atoms) with this many boxes; 0 skips it")
-    ap.add_argument("--served", type=int, default=32,
+    ap.add_argument("--served", type=int, default=256,
                     help="served-job measurement (Poisson arrivals of 1.5k-30k-atom jobs) with this many jobs; 0 skips it")
     ap.add_argument("--precision", type=int, default=100000,
                     help="precision study: NVE steps of the 17,280-atom system, then NPT; 0 skips it")
@@ -90,7 +91,7 @@ class Clocks:
     def start(self):
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                       "-lms", "100", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                       "-lms", "20", "-i", str(self.device)], stdout=subprocess.PIPE,
                                       stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -377,24 +378,29 @@ def served_jobs(njobs, seed):
     return jobs
 
 
-def bench_served(device, njobs=32, seed=4242, check=4):
-    """Served jobs through the serving loop (fz_server): each job is submitted at its
-    Poisson arrival time, admitted by the 150 GB HBM budget, advanced with the running
-    mix in the batch graph; latency = completion - submission on the server clock.
-    The one-at-a-time comparisons time 200 steps of each job alone (its own CUDA graph)
-    and 30 steps of it alone on the plain path, each scaled to the job's step count."""
+def bench_served(device, njobs=256, seed=4242, check=4, sample=32, max_running=64):
+    """Served jobs through the serving loop (fz_server): each job of the seeded stream
+    is submitted at its Poisson arrival time and admitted in FIFO order while fewer
+    than `max_running` jobs run and their device bytes fit the 150 GB HBM budget, so
+    later arrivals queue and are admitted as running jobs finish and free their slots
+    (continuous batching); running jobs advance together in the batch graph.
+    Per job: queue wait = start - submission, service = end - start, latency = end -
+    submission, all on the server's steady clock.  The one-at-a-time comparisons time
+    a seeded sample of `sample` jobs alone (200 steps on the product path, 30 on the
+    plain path, each scaled to the job's step count)."""
     import torch
     import fenzi_b200 as fz
     from fenzi_b200 import gen_system
     from oracle.oracle import Oracle
     jobs = served_jobs(njobs, seed)
     root = tempfile.mkdtemp(prefix="fzserve_")
-    paths = []
+    paths, gens = [], []
     for i, j in enumerate(jobs):
         box = (j["nw"] / 0.0334 + 15.0 * 30 * j["nchains"]) ** (1.0 / 3.0)  # ~15 A^3 per chain atom
-        g = gen_system.build(name=f"job{i:02d}", nw=j["nw"], nchains=j["nchains"], chain_len=30, box=box, rc=10.0,
+        g = gen_system.build(name=f"job{i:03d}", nw=j["nw"], nchains=j["nchains"], chain_len=30, box=box, rc=10.0,
                              ron=8.0, seed=j["seed"])
-        paths.append(gen_system.write(g, os.path.join(root, f"j{i:02d}")))
+        gens.append(g)
+        paths.append(gen_system.write(g, os.path.join(root, f"j{i:03d}")))
 
     def load(i):
         s = fz.FenZi.ReadInput(paths[i])
@@ -402,10 +408,12 @@ def bench_served(device, njobs=32, seed=4242, check=4):
             s.cfg.temp_reset_every = 1000
         return s.LoadSystem()
 
-    # one at a time: 200 steps of each job alone, scaled to its length
+    # one at a time, on a seeded sample of the stream
     from fenzi_b200.plain import Plain
-    seq_s, plain_s, natoms = 0.0, 0.0, []
-    for i, j in enumerate(jobs):
+    pick = sorted(np.random.default_rng(seed + 1).choice(len(jobs), min(sample, len(jobs)), replace=False))
+    seq_s, plain_s, sample_work = 0.0, 0.0, 0.0
+    for i in pick:
+        j = jobs[i]
         s = load(i)
         s.InitMem(device)
         s.InitVelocity(T=300.0, seed=j["seed"])
@@ -415,8 +423,7 @@ def bench_served(device, njobs=32, seed=4242, check=4):
         s.SingleStep(200)
         torch.cuda.synchronize()
         seq_s += (time.perf_counter() - t0) / 200 * j["steps"]
-        natoms.append(s.n)
-        # the same job alone on the plain path (its own engine, from the same state)
+        sample_work += s.n * j["steps"]
         pl = Plain(s, device)
         pl.set_positions(s.positions())
         pl.set_velocities(s.velocities())
@@ -427,8 +434,8 @@ def bench_served(device, njobs=32, seed=4242, check=4):
         pl.close()
         s.close()
     systems = [load(i) for i in range(len(jobs))]
-    total = sum(n * j["steps"] for n, j in zip(natoms, jobs))
-    server = fz.Server(device, hbm_budget_bytes=150e9, chunk_steps=100, max_running=64)
+    total = sum(sy.n * j["steps"] for sy, j in zip(systems, jobs))
+    server = fz.Server(device, hbm_budget_bytes=150e9, chunk_steps=100, max_running=max_running)
     ids = []
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -441,30 +448,38 @@ def bench_served(device, njobs=32, seed=4242, check=4):
     wall = time.perf_counter() - t0
     stats = server.stats()
     lat = np.array([x["latency_s"] for x in infos])
-    # final-frame force error against the FP64 oracle, on a sample of jobs
+    wait = np.array([x["start_s"] - x["submit_s"] for x in infos])
+    serv = np.array([x["end_s"] - x["start_s"] for x in infos])
+    # final-frame force error against the FP64 oracle (generator topology), smallest jobs
     errs = []
-    for i in sorted(range(len(jobs)), key=lambda k: natoms[k])[:check]:
+    for i in sorted(range(len(jobs)), key=lambda k: systems[k].n)[:check]:
         pos = server.positions(ids[i])
         s = load(i)
         s.InitMem(device)
         s.set_positions(pos)
         s.ComputeAccelGPU()
         f = s.forces()
-        f0, _ = Oracle(s.topology()).forces(s.positions())
+        f0, _ = Oracle(gen_system.topology(gens[i])).forces(s.positions())
         errs.append(float(np.sqrt(((f - f0) ** 2).sum() / (f0 ** 2).sum())))
         s.close()
     server.close()
-    return {"metric": "served p50/p99 job latency", "p50_s": float(np.percentile(lat, 50)),
-            "p99_s": float(np.percentile(lat, 99)), "unit": "s", "jobs": len(jobs),
+    pct = lambda a, q: float(np.percentile(a, q))
+    return {"metric": "served p50/p99 job latency", "p50_s": pct(lat, 50), "p99_s": pct(lat, 99), "unit": "s",
+            "jobs": len(jobs), "queue_wait_s": {"p50": pct(wait, 50), "p99": pct(wait, 99), "max": float(wait.max())},
+            "service_s": {"p50": pct(serv, 50), "p99": pct(serv, 99)},
             "aggregate_atom_steps_per_s": total / wall, "makespan_s": wall,
-            "one_at_a_time_atom_steps_per_s": total / seq_s, "speedup_vs_one_at_a_time": seq_s / wall,
-            "plain_one_at_a_time_atom_steps_per_s": total / plain_s, "speedup_vs_plain_one_at_a_time": plain_s / wall,
-            "peak_running_jobs": stats["peak_running"],
+            "max_running": max_running, "peak_running_jobs": stats["peak_running"],
+            "jobs_that_queued": int((wait > 0.05).sum()),
+            "one_at_a_time_atom_steps_per_s": sample_work / seq_s,
+            "speedup_vs_one_at_a_time": (total / wall) / (sample_work / seq_s),
+            "plain_one_at_a_time_atom_steps_per_s": sample_work / plain_s,
+            "speedup_vs_plain_one_at_a_time": (total / wall) / (sample_work / plain_s),
+            "one_at_a_time_sample": f"{len(pick)} seeded jobs of the stream",
             "final_frame_force_rel_rms_vs_oracle": {"max": max(errs), "jobs_checked": len(errs)},
             "workload": f"{len(jobs)} jobs of a Poisson(200/s) stream (seed {seed}): 1.5k-30k atoms, 0-40 30-atom "
                         f"chains + TIP3P, 1k-20k steps log-uniform, half NVT (reassignment every 1,000), rc 10, "
-                        f"beta 0.34, SHAKE, 1 fs; HBM budget 150 GB, 100-step chunks",
-            "timing": "wall clock from the first submission to the last completion; latency per job on the "
+                        f"beta 0.34, SHAKE, 1 fs; HBM budget 150 GB, at most {max_running} running, 100-step chunks",
+            "timing": "wall clock from the first submission to the last completion; per-job times on the "
                       "server's steady clock"}
 
 
@@ -579,48 +594,80 @@ def bench_precision(device, nve_steps=100000, npt_steps=2000, fp64_steps=20000):
     return out
 
 
-def cpu_baseline(path, nsteps):
-    """The FP64 oracle on the same system: nsteps MD steps on all host threads."""
-    import fenzi_b200 as fz
+def cpu_baseline(s_gen, nsteps, warmup=0):
+    """The FP64 oracle on the same system, on all host threads: `warmup` untimed MD
+    steps, then nsteps timed MD steps (forces + velocity Verlet + SHAKE/RATTLE).  The
+    oracle's topology comes from the generator (no product library is loaded)."""
+    from fenzi_b200 import gen_system
     from oracle.oracle import Oracle
-    s = fz.FenZi.ReadInput(path).LoadSystem()
-    top = s.topology()
-    orc = Oracle(top)
-    pos = top["pos"]
+    orc = Oracle(gen_system.topology(s_gen))
+    pos = np.asarray(s_gen.pos, np.float64)
     vel = orc.reassign_velocities(pos, 300.0, 2345, 0)
-    t0 = time.perf_counter()
-    orc.forces(pos)
-    tf = time.perf_counter() - t0
+    if warmup > 0:
+        st = orc.md(pos, vel, warmup, dt_ps=0.001, tol=1e-10, traces=False)
+        pos, vel = st["pos"], st["vel"]
+    else:
+        orc.forces(pos)  # first-touch of the oracle's buffers, untimed
     t0 = time.perf_counter()
     orc.md(pos, vel, nsteps, dt_ps=0.001, tol=1e-10, traces=False)
-    tmd = time.perf_counter() - t0
-    per_step = max(1e-9, (tmd - tf) / nsteps)
-    s.close()
+    per_step = max(1e-9, (time.perf_counter() - t0) / nsteps)
     return per_step, os.cpu_count()
 
 
+def pme_error(sysm, s_gen, nsample=2000):
+    """PME force error of the product against a converged direct Ewald sum (FP64, on a
+    seeded subsample of atoms), relative to the total nonbonded force, beside the error
+    of the FP64 order-4 mesh of the same grid (the method's own error)."""
+    import fenzi_b200 as fz
+    from fenzi_b200 import gen_system
+    from oracle import oracle as O
+    from oracle.ewald_direct import kmax_for, recip_forces
+    pos = sysm.positions()
+    sysm.ComputeAccelGPU(terms=fz.TERM_PME)
+    f_pme = sysm.forces()
+    sysm.ComputeAccelGPU(terms=fz.TERM_NONBONDED | fz.TERM_PAIRS14 | fz.TERM_EXCLUSIONS)
+    f_real = sysm.forces()
+    atoms = np.random.default_rng(7).choice(len(pos), min(nsample, len(pos)), replace=False)
+    fe, _ = recip_forces(pos, s_gen.charge, s_gen.box, s_gen.beta, atoms, kmax_for(s_gen.box, s_gen.beta))
+    f64, _ = O.Oracle(gen_system.topology(s_gen)).forces(pos, O.T_PME)
+    den = ((f_real[atoms] + fe) ** 2).sum()
+    return {"vs_direct_ewald": float(np.sqrt(((f_pme[atoms] - fe) ** 2).sum() / den)),
+            "fp64_mesh_vs_direct_ewald": float(np.sqrt(((f64[atoms] - fe) ** 2).sum() / den)),
+            "vs_fp64_mesh": float(np.sqrt(((f_pme - f64) ** 2).sum() / (f64 ** 2).sum())),
+            "relative_to": "total nonbonded force (real-space pairs + 1-4 + exclusion + reciprocal)",
+            "sample": f"{len(atoms)} seeded atoms; direct sum over |m| with exp(-pi^2 m^2/beta^2) > 1e-12"}
+
+
+def config_block(natom):
+    """The `config` object of both arms (the workload only; run details are elsewhere)."""
+    return {"workload": WORKLOAD, "natom": natom, "timestep_fs": 1.0,
+            "l2": "GPU arm: flushed (256 MB write) before every timed step"}
+
+
 def run_reference(a):
+    """The reference arm: the FP64 CPU restatement of the reference's algorithm (its own
+    CUDA build does not compile with CUDA 12.9 and it has no CPU path), W untimed and K
+    timed full MD steps of the same 230,400-atom system on all host threads, rank 0 only."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    _, path = build_inputs(a.workload, 2345)
-    nsteps = max(1, min(a.steps, 4))
-    per_step, cores = cpu_baseline(path, nsteps)
+    s_gen, _ = build_inputs(a.workload, 2345)
+    per_step, cores = cpu_baseline(s_gen, a.steps, a.warmup)
     nsd = 86.4 / (per_step * 1e3)
-    natom = 230400 if a.workload == "large230k" else None
+    natom = s_gen.n
     line = {"metric": "ns/day @230K atoms (MD step, 1 fs)", "value": nsd, "unit": "ns/day", "impl": "reference",
-            "n_gpus": a.gpus, "steps": nsteps, "warmup": 1, "ms_per_step": per_step * 1e3,
+            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": per_step * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
             "data": "synthetic (seeded generator, CHARMM file formats)",
-            "config": {"workload": WORKLOAD, "parallelism": "host threads"},
+            "config": config_block(natom),
+            "parallelism": f"host threads x{cores} (rank 0)",
             "cpu_baseline": {"value": nsd, "unit": "ns/day", "cores": cores, "kind": "port",
-                             "sample": f"{nsteps} full MD steps (forces + velocity Verlet + SHAKE/RATTLE) of the "
-                                       f"230,400-atom system after one untimed force evaluation (the warm-up); FP64 oracle, OpenMP"},
+                             "sample": f"{a.steps} full MD steps (forces + velocity Verlet + SHAKE/RATTLE) of the "
+                                       f"230,400-atom system after {a.warmup} untimed steps; FP64 oracle, OpenMP"},
             "e2e": {"value": nsd, "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "atom_steps_per_s": natom / per_step,
             "note": "reference CUDA build does not compile with CUDA 12.9 (legacy texture references); "
                     "timed arm is the FP64 CPU restatement of its algorithm"}
-    if natom:
-        line["atom_steps_per_s"] = natom / per_step
     print(json.dumps(line))
     return 0
 
@@ -746,10 +793,11 @@ def main():
         t_ideal = FLOP_PER_PAIR * pairs / (peak * 1e12) + bytes_ / (hbm * 1e9)
         cpu = None
         if not a.no_cpu_baseline and world == 1:
-            per, cores = cpu_baseline(path, 4)
+            per, cores = cpu_baseline(s_gen, 4)
             cpu = {"value": 86.4 * dt_fs / (per * 1e3), "unit": "ns/day", "cores": cores, "kind": "port",
                    "sample": "4 full MD steps of the 230,400-atom system (FP64 oracle, OpenMP, all host threads)"}
         plain = bench_plain_single(sysm, local, t_ideal, ms_step) if world == 1 else None
+        pme_err = pme_error(sysm, s_gen) if world == 1 else None
         small = bench_small(local, peak, a.small) if a.small > 0 and world == 1 else None
         batched = batched_multi
         if a.ensemble > 0 and world == 1:
@@ -764,11 +812,10 @@ def main():
                 "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_step,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
                 "data": "synthetic (seeded generator written as CHARMM crd/psf/prm/rtf + .in)",
-                "config": {"workload": WORKLOAD, "natom": natom, "parallelism": f"replicas x{world}",
-                           "preparation": f"{a.equil} untimed MD steps with 300 K velocity reassignment every 100",
-                           "l2": "flushed (256 MB write) before every timed step",
-                           "pairs_within_cutoff": pairs,
-                           "launch_shapes": shapes},
+                "config": config_block(natom),
+                "parallelism": f"replicas x{world}",
+                "run": {"preparation": f"{a.equil} untimed MD steps with 300 K velocity reassignment every 100",
+                        "pairs_within_cutoff": pairs, "launch_shapes": shapes},
                 "atom_steps_per_s": natom * world / (ms_step * 1e-3),
                 "step_roofline": {"t_ideal_ms": t_ideal * 1e3, "frac": t_ideal * 1e3 / ms_step,
                                   "model": "60 FLOP/pair / FP32 peak + (56N + 24K^3 + 120N) B / HBM"},
@@ -783,7 +830,8 @@ def main():
                         "step": f"one C-ABI call chain per {a.chunk} MD steps: fz_set_state_f32 (positions + "
                                 f"velocities from pinned host memory) + fz_step({a.chunk}) + fz_get_state_f32 "
                                 f"(wall clock); bytes per MD step are the per-call copies / {a.chunk}"},
-                "gpu_launches": launches, "clocks": clocks, "batched": batched, "served": served,
+                "gpu_launches": launches, "clocks": clocks, "pme_error": pme_err, "batched": batched,
+                "served": served,
                 "precision": precision}
     if dist:
         dist.barrier()

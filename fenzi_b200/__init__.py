@@ -99,6 +99,9 @@ EXPORTS = ["fz_last_error", "fz_version", "fz_read_input", "fz_load_system", "fz
 STAGES = ["neighbour", "nonbonded", "bonded", "pme", "integrate"]
 
 TERM_NONBONDED, TERM_BONDED, TERM_PME, TERM_ALL = 1, 2, 4, 7
+# parts of TERM_BONDED, selectable one by one
+TERM_BONDS, TERM_ANGLES, TERM_UREYB, TERM_DIHEDRALS, TERM_IMPROPERS, TERM_PAIRS14, TERM_EXCLUSIONS = (
+    8, 16, 32, 64, 128, 256, 512)
 
 _lib = None
 

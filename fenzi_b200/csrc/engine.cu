@@ -620,7 +620,21 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
   }
   if ((r = autotune(e))) return r;
   FZ_CUDA(cudaStreamSynchronize(e->st));
-  return e->check();
+  if ((r = e->check())) return r;
+  // FZ_LIST_CAP=c (a test hook for the capacity path): from the next rebuild on, each
+  // block's pair list keeps at most c entries (a multiple of 32, within what is
+  // allocated; the lists are rebuilt at the new stride before any kernel reads them),
+  // so an overflow during dynamics is reported by fz_step as FZ_ERR_CAPACITY instead
+  // of being grown here
+  if (const char* v = std::getenv("FZ_LIST_CAP")) {
+    const int cap = std::max(32, std::min(e->ocap, (std::atoi(v) / 32) * 32));
+    e->ocap = cap;
+    e->mask_cap = ngrp * (cap / 32);
+    e->drop_graph();
+    FZ_CUDA(cudaMemcpyAsync(e->flag, &one, sizeof(int), cudaMemcpyHostToDevice, e->st));
+    FZ_CUDA(cudaStreamSynchronize(e->st));
+  }
+  return FZ_OK;
 }
 
 // ---------------------------------------------------------------- barostat
@@ -787,7 +801,7 @@ extern "C" fz_status fz_compute_forces_terms(fz_system* s, int terms, int energi
   Engine* e = s->eng;
   FZ_CUDA(cudaMemsetAsync(e->facc, 0, 3 * sizeof(long long) * e->n, e->st));
   if (energies) FZ_CUDA(cudaMemsetAsync(e->energy, 0, fzk::EN_COUNT * sizeof(long long), e->st));
-  e->forces(energies != 0, terms & FZ_TERM_ALL);
+  e->forces(energies != 0, terms & (FZ_TERM_ALL | FZ_TERM_BONDED_PARTS));
   // a partial evaluation is not the state's force: the next step recomputes
   e->forces_valid = (terms & FZ_TERM_ALL) == FZ_TERM_ALL;
   return e->check();

@@ -364,8 +364,19 @@ struct Engine {
       launches += 1;
     }
     mark(3);
-    if (terms & FZ_TERM_BONDED) {
-      fzk::launch_bonded(bonded_args(), energies, st);
+    if (terms & (FZ_TERM_BONDED | FZ_TERM_BONDED_PARTS)) {
+      fzk::BondedArgs a = bonded_args();
+      if (!(terms & FZ_TERM_BONDED)) {
+        // selected parts only: the kernel's flattened term range skips empty classes
+        if (!(terms & FZ_TERM_BONDS)) a.nbond = 0;
+        if (!(terms & FZ_TERM_ANGLES)) a.nangle = 0;
+        if (!(terms & FZ_TERM_UREYB)) a.nub = 0;
+        if (!(terms & FZ_TERM_DIHEDRALS)) a.ndihe = 0;
+        if (!(terms & FZ_TERM_IMPROPERS)) a.nimpr = 0;
+        if (!(terms & FZ_TERM_PAIRS14)) a.n14 = 0;
+        if (!(terms & FZ_TERM_EXCLUSIONS)) a.nexcl = 0;
+      }
+      fzk::launch_bonded(a, energies, st);
       launches += bonded_launches();
     }
     if ((terms & FZ_TERM_BONDED) && restraint) {

@@ -149,6 +149,18 @@ fz_status fz_compute_forces(fz_system* sys, int energies);
 #define FZ_TERM_BONDED 2
 #define FZ_TERM_PME 4
 #define FZ_TERM_ALL 7
+/* Parts of FZ_TERM_BONDED, selectable one by one (the reference keeps one energy
+ * array per part, src/bonded_forces.cu:597-640): bonds, angles, Urey-Bradley,
+ * dihedrals, impropers, 1-4 pairs, Ewald exclusion correction.  Restraints come only
+ * with FZ_TERM_BONDED. */
+#define FZ_TERM_BONDS 8
+#define FZ_TERM_ANGLES 16
+#define FZ_TERM_UREYB 32
+#define FZ_TERM_DIHEDRALS 64
+#define FZ_TERM_IMPROPERS 128
+#define FZ_TERM_PAIRS14 256
+#define FZ_TERM_EXCLUSIONS 512
+#define FZ_TERM_BONDED_PARTS 1016
 fz_status fz_compute_forces_terms(fz_system* sys, int terms, int energies);
 /* SingleStep (src/dynamics.cu:623-820) x nsteps: velocity Verlet with SHAKE/RATTLE,
  * device-side neighbour maintenance, velocity reassignment every temp_reset_every

@@ -46,7 +46,14 @@ def oracle_for(fz_sys, nthreads=0):
     """The oracle of a loaded system: from the generator's topology when the system
     was written by system() (reader-free), else from the product readers' topology."""
     from oracle.oracle import Oracle
-    crd = fz_sys.cfg.coordinates.decode()
-    gen = _GEN_BY_DIR.get(os.path.realpath(os.path.dirname(crd)))
-    topo = gen_system.topology(gen) if gen is not None else fz_sys.topology()
+    c = fz_sys.cfg
+    gen = _GEN_BY_DIR.get(os.path.realpath(os.path.dirname(c.coordinates.decode())))
+    if gen is None:
+        return Oracle(fz_sys.topology(), nthreads=nthreads)
+    topo = gen_system.topology(gen)
+    # run parameters come from the configuration the system was loaded with (a test may
+    # change them after reading the input file)
+    topo.update(box=np.array(list(c.box)), rc=c.cutoff, ron=c.cuton, beta=c.kappa, K=np.array(list(c.pme_grid)))
+    if not c.shake:
+        topo.update(cons=np.zeros((0, 2), np.int32), cons_d=np.zeros(0))
     return Oracle(topo, nthreads=nthreads)

@@ -53,7 +53,7 @@ def test_synthetic_round_trip():
     np.testing.assert_allclose(t["mass"], ref["mass"])
     assert np.array_equal(t["bond"], ref["bond"]) and np.array_equal(t["angle"], ref["angle"])
     np.testing.assert_allclose(t["bond_k"], ref["bond_k"])
-    np.testing.assert_allclose(t["bond_r0"], ref["bond_r0"], atol=1e-4)
+    np.testing.assert_allclose(t["bond_r0"], ref["bond_r0"], rtol=1e-14)
     np.testing.assert_allclose(t["angle_k"], ref["angle_k"])
     np.testing.assert_allclose(t["angle_t0"], ref["angle_t0"], atol=1e-6)
     np.testing.assert_allclose(t["dihe_k"], ref["dihe_k"])
@@ -63,10 +63,10 @@ def test_synthetic_round_trip():
     idx = np.arange(0, s.n, 37)
     e_prod = t["eps4"][ti[idx][:, None], ti[idx][None, :]]
     e_ref = ref["eps4"][tr[idx][:, None], tr[idx][None, :]]
-    np.testing.assert_allclose(e_prod, e_ref, rtol=1e-6)
+    np.testing.assert_allclose(e_prod, e_ref, rtol=1e-14)
     s_prod = t["sig2"][ti[idx][:, None], ti[idx][None, :]]
     s_ref = ref["sig2"][tr[idx][:, None], tr[idx][None, :]]
-    np.testing.assert_allclose(s_prod, s_ref, rtol=1e-3)
+    np.testing.assert_allclose(s_prod, s_ref, rtol=1e-14)
     i = sy.info()
     assert i.nconstraint == len(ref["cons"]) and i.ncluster == 400
     # exclusions: waters 3 pairs each, chains 1-2 + 1-3; 1-4 = chain dihedrals
