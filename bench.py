@@ -267,7 +267,7 @@ def bench_small(device, peak_tflops, steps=2000):
     import fenzi_b200 as fz
     from fenzi_b200.plain import Plain
     from oracle.oracle import Oracle
-    _, path = build_inputs("water3000", 2345)
+    s_gen, path = build_inputs("water3000", 2345)
     s = fz.FenZi.ReadInput(path).LoadSystem()
     s.InitMem(device)
     s.InitVelocity(T=300.0, seed=2345)
@@ -296,7 +296,7 @@ def bench_small(device, peak_tflops, steps=2000):
     hbm, hbm_src = measured_hbm_gbs()
     t_ideal = step_ideal_s(pairs, s.n, list(s.cfg.pme_grid), peak_tflops, hbm)
     err = oracle_force_error(s)
-    per, cores = cpu_baseline(path, 10)
+    per, cores = cpu_baseline(s_gen, 10)
     dt_fs = s.cfg.timestep_ps * 1000.0
     out = {"workload": "water3000: 3,000 TIP3P = 9,000 atoms, 44.8 A, 48^3 PME, beta 0.34, rc 10 / ron 8, "
                        "SHAKE, 1 fs (1,100 prepared steps with 300 K reassignment every 100)",
@@ -540,7 +540,7 @@ def bench_precision(device, nve_steps=100000, npt_steps=2000, fp64_steps=20000):
         s.InitVelocity(T=300.0, seed=2345, counter=k + 1)
     s.SingleStep(100)
     pos0, vel0 = s.positions(), s.velocities()
-    per, cores = cpu_baseline(path, 3)
+    per, cores = cpu_baseline(g, 3)
     cpu = {"value": 86.4 * s.cfg.timestep_ps * 1e3 / (per * 1e3), "unit": "ns/day", "cores": cores, "kind": "port",
            "sample": "3 MD steps of the same system, FP64 oracle, all host threads"}
     chunk = 1000

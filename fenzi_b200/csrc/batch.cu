@@ -99,6 +99,10 @@ struct fz_batch {
   std::vector<cudaEvent_t> ev_done;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  // batched kernels only: a graph of `chunk` consecutive steps (one launch per chunk)
+  cudaGraph_t chunk_graph = nullptr;
+  cudaGraphExec_t chunk_exec = nullptr;
+  int chunk = 100;
   int* pinned_status = nullptr;
   long long steps = 0;
   std::unique_ptr<BatchKernels> bk;
@@ -109,8 +113,12 @@ struct fz_batch {
     bk.reset();
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
+    if (chunk_exec) cudaGraphExecDestroy(chunk_exec);
+    if (chunk_graph) cudaGraphDestroy(chunk_graph);
     exec = nullptr;
     graph = nullptr;
+    chunk_exec = nullptr;
+    chunk_graph = nullptr;
     for (auto e : ev_done) cudaEventDestroy(e);
     ev_done.clear();
     if (pinned_status) cudaFreeHost(pinned_status);
@@ -329,6 +337,14 @@ static fz_status capture(fz_batch* b) {
     batched_step_body(b, b->master);
     FZ_CUDA(cudaStreamEndCapture(b->master, &b->graph));
     FZ_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
+    if (const char* c = std::getenv("FZ_GRAPH_CHUNK"))
+      if (b->chunk > 0) b->chunk = std::max(0, std::min(1000, std::atoi(c)));
+    if (b->chunk > 1) {
+      FZ_CUDA(cudaStreamBeginCapture(b->master, cudaStreamCaptureModeThreadLocal));
+      for (int k = 0; k < b->chunk; ++k) batched_step_body(b, b->master);
+      FZ_CUDA(cudaStreamEndCapture(b->master, &b->chunk_graph));
+      FZ_CUDA(cudaGraphInstantiate(&b->chunk_exec, b->chunk_graph, 0));
+    }
     return FZ_OK;
   }
   FZ_CUDA(cudaStreamBeginCapture(b->master, cudaStreamCaptureModeThreadLocal));
@@ -371,7 +387,10 @@ extern "C" fz_status fz_batch_step(fz_batch* b, int nsteps) {
       const Engine* e = s->eng;
       if (e->temp_reset_every > 0) k = std::min<long long>(k, e->temp_reset_every - e->step % e->temp_reset_every);
     }
-    for (int j = 0; j < k; ++j) FZ_CUDA(cudaGraphLaunch(b->exec, b->master));
+    int j = 0;
+    if (b->chunk_exec)
+      for (; j + b->chunk <= k; j += b->chunk) FZ_CUDA(cudaGraphLaunch(b->chunk_exec, b->master));
+    for (; j < k; ++j) FZ_CUDA(cudaGraphLaunch(b->exec, b->master));
     for (int i = 0; i < ns; ++i) {
       Engine* e = b->systems[i]->eng;
       e->step += k;
@@ -474,6 +493,9 @@ void fz_server::run() {
   cudaSetDevice(dev);
   fz_batch* batch = nullptr;
   fz_batch_create(&batch);
+  // the membership changes about every chunk (a job ends): a multi-step graph would be
+  // captured for one replay, so the served batch replays its one-step graph
+  batch->chunk = 0;
   std::vector<Job*> running;
   auto finish = [&](Job* j, fz_status st, const std::string& msg) {
     if (j->sys->eng) {

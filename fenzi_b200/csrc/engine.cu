@@ -223,6 +223,7 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
     // they replace, so they are off unless FZ_GRAPH_COND=1
     const char* v = std::getenv("FZ_GRAPH_COND");
     e->cond_graph = v && std::atoi(v) == 1;
+    if (const char* c = std::getenv("FZ_GRAPH_CHUNK")) e->chunk_steps = std::max(0, std::min(1000, std::atoi(c)));
   }
   FZ_CUDA(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
   FZ_CUDA(cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming));
@@ -823,6 +824,20 @@ extern "C" fz_status fz_step(fz_system* s, int nsteps) {
   }
   const fzk::IntegrateArgs ia = e->int_args();
   for (int k = 0; k < nsteps; ++k) {
+    // a whole chunk in one graph launch when no velocity reassignment falls inside it
+    if (!e->npt && e->use_graph && !e->timing && e->chunk_steps > 1 && nsteps - k >= e->chunk_steps &&
+        (e->temp_reset_every <= 0 ||
+         e->temp_reset_every - e->step % e->temp_reset_every >= e->chunk_steps)) {
+      if ((r = e->graph_chunk())) return r;
+      e->step += e->chunk_steps;
+      k += e->chunk_steps - 1;
+      if (e->temp_reset_every > 0 && e->step % e->temp_reset_every == 0) {
+        fzk::launch_reassign(ia, e->temperature, e->seed, (uint32_t)(e->step / e->temp_reset_every), e->inv_mtot,
+                             e->psum, e->st);
+        e->launches += 3 + e->ncls;
+      }
+      continue;
+    }
     if (e->npt) {
       if ((r = npt_step(e))) return r;
     } else if (e->use_graph && !e->timing) {
@@ -933,6 +948,10 @@ extern "C" fz_status fz_minimize(fz_system* s, int max_steps, int* steps_done, d
   const double rate[3] = {0.0, c.conjgradrate, c.steepdesrate};
   double prev = 0.0, cur = 0.0;
   if ((r = energy(&cur))) return r;
+  // the reference's MinimizeStep keeps its previous energy in a static that starts at 0
+  // and never undoes a move while it is 0, so the first move is always kept; an undone
+  // move is not counted (stepCount - 1, src/dynamics.cu:598-618)
+  bool first = true;
   int step = 0;
   for (; step < max_steps && method != 0; ++step) {
     FZ_CUDA(cudaMemcpyAsync(e->min_pos, e->pos4, sizeof(float4) * e->n, cudaMemcpyDeviceToDevice, e->st));
@@ -944,13 +963,15 @@ extern "C" fz_status fz_minimize(fz_system* s, int max_steps, int* steps_done, d
     fzk::launch_min_step(ia, e->st);
     prev = cur;
     if ((r = energy(&cur))) return r;
-    if (cur > prev) {  // undo the move, switch method
+    if (cur > prev && !first) {  // undo the move, switch method
       FZ_CUDA(cudaMemcpyAsync(e->pos4, e->min_pos, sizeof(float4) * e->n, cudaMemcpyDeviceToDevice, e->st));
       const int one = 1;
       FZ_CUDA(cudaMemcpyAsync(e->flag, &one, sizeof(int), cudaMemcpyHostToDevice, e->st));
       if ((r = energy(&cur))) return r;
       method = method == 1 ? 2 : 0;
+      --step;
     }
+    first = false;
     if (step > 0 && step % 100 == 0 && method != 0) fac[method] *= rate[method] * 100.0;
   }
   FZ_CUDA(cudaMemsetAsync(e->facc, 0, 3 * sizeof(long long) * e->n, e->st));

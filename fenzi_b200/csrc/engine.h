@@ -103,6 +103,11 @@ struct Engine {
   // kick/RATTLE); captured on first use, replayed with one launch per step
   cudaGraph_t step_graph = nullptr;
   cudaGraphExec_t step_exec = nullptr;
+  // graph of `chunk_steps` consecutive steps (one launch per chunk): replayed for the
+  // runs of steps with no velocity reassignment inside; 0 or 1 disables (FZ_GRAPH_CHUNK)
+  cudaGraph_t chunk_graph = nullptr;
+  cudaGraphExec_t chunk_exec = nullptr;
+  int chunk_steps = 100;
   bool use_graph = true;
   // With cond_graph (env FZ_GRAPH_COND=1) the rebuild and prune kernels of captured
   // steps are the bodies of two conditional IF nodes set from the device flags, else
@@ -175,6 +180,8 @@ struct Engine {
     if (st) cudaStreamSynchronize(st);
     if (step_exec) cudaGraphExecDestroy(step_exec);
     if (step_graph) cudaGraphDestroy(step_graph);
+    if (chunk_exec) cudaGraphExecDestroy(chunk_exec);
+    if (chunk_graph) cudaGraphDestroy(chunk_graph);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
     if (st2) cudaStreamDestroy(st2);
@@ -556,11 +563,35 @@ struct Engine {
     graph_since_check = true;
     return FZ_OK;
   }
+  // chunk_steps steps in one graph launch (captured on first use)
+  fz_status graph_chunk() {
+    if (!chunk_exec) {
+      capture_error = cudaSuccess;
+      FZ_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      const long long l0 = launches;
+      for (int k = 0; k < chunk_steps; ++k) step_body();
+      launches = l0;
+      cudaGraph_t g = nullptr;
+      FZ_CUDA(cudaStreamEndCapture(st, &g));
+      chunk_graph = g;
+      if (capture_error != cudaSuccess)
+        return fail(FZ_ERR_CUDA, std::string("chunk capture: ") + cudaGetErrorString(capture_error));
+      FZ_CUDA(cudaGraphInstantiate(&chunk_exec, chunk_graph, 0));
+    }
+    FZ_CUDA(cudaGraphLaunch(chunk_exec, st));
+    launches += (long long)chunk_steps * graph_step_launches();
+    graph_since_check = true;
+    return FZ_OK;
+  }
   void drop_graph() {
     if (step_exec) cudaGraphExecDestroy(step_exec);
     if (step_graph) cudaGraphDestroy(step_graph);
+    if (chunk_exec) cudaGraphExecDestroy(chunk_exec);
+    if (chunk_graph) cudaGraphDestroy(chunk_graph);
     step_exec = nullptr;
     step_graph = nullptr;
+    chunk_exec = nullptr;
+    chunk_graph = nullptr;
   }
   fz_status check() {
     int h = 0;

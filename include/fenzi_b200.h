@@ -188,9 +188,11 @@ fz_status fz_dcd_close(fz_dcd* traj);
 /* MinimizeStep x minimizesteps (src/dynamics.cu:491-620, src/fenzi.cu:397-418):
  * conjugate-gradient moves (conjgradfac, conjgradrate) until the potential energy
  * rises, then steepest descent (steepdesfac, steepdesrate) until it rises again, at
- * most max_steps moves; constraints are kept.  Velocities are zeroed: call
- * fz_reassign_velocities before dynamics.  Reports the moves made and the final
- * potential energy (kcal/mol). */
+ * most max_steps kept moves; a move that raised the energy is undone and not counted
+ * (the first move is always kept, as in the reference); every 100 moves the current
+ * factor is multiplied by its rate x 100; constraints are kept.  Velocities are
+ * zeroed: call fz_reassign_velocities before dynamics.  Reports the moves kept and
+ * the final potential energy (kcal/mol). */
 fz_status fz_minimize(fz_system* sys, int max_steps, int* steps_done, double* energy_out);
 /* Andersen constant-pressure dynamics for the following fz_step calls (the reference's
  * PCONSTANT build: src/cell_based_kernels.cu:566-579 piston acceleration,

@@ -1007,6 +1007,81 @@ int orc_md(void* h, double* pos, double* vel, int nsteps, double dt_ps, double t
   return bad;
 }
 
+// Energy minimisation, the reference's MinimizeStep loop (src/dynamics.cu:491-620) with
+// the moves of ConjugatedGradient / SteepestDescent (src/mdcuda.cu:126-351) and the
+// factor schedule of main() (src/fenzi.cu:397-418), in FP64:
+//   CG move per atom: gamma = |F|^2 / |F_prev|^2 (F_prev replaced by F when
+//     |F_prev|^2 < 1e-8), H = (F + gamma H_prev) cgfac, r += H; F_prev = F, H_prev = H;
+//   SD move per atom: r += F sdfac;
+//   after the move the energy is evaluated; if it rose (never on the first move, where
+//   the reference's previous energy is still its 0 sentinel) the move is undone, the
+//   step is not counted, and CG switches to SD, SD ends the minimisation;
+//   every 100 counted steps (step > 0) the current method's factor is multiplied by
+//   rate x 100.
+// Constrained units are kept rigid by SHAKE against the positions before the move
+// (the reference moves those atoms freely).  pos in/out; energies[k] (may be NULL) is
+// the potential energy after counted step k; methods[k] (may be NULL) the method of
+// that step's move.  Returns the number of counted steps.
+int orc_minimize(void* h, double* pos, int max_steps, double cgfac, double sdfac, double cgrate, double sdrate,
+                 double* energies, int* methods) {
+  Orc* o = (Orc*)h;
+  const int n = o->s.n;
+  std::vector<double> f(3 * (size_t)n), fprev(3 * (size_t)n, 0.0), dir(3 * (size_t)n, 0.0),
+      pos0(3 * (size_t)n), vel(3 * (size_t)n, 0.0);
+  double e[ORC_NE];
+  auto evaluate = [&]() {
+    std::fill(f.begin(), f.end(), 0.0);
+    orc_forces(h, pos, f.data(), e, ORC_T_ALL);
+    double u = 0;
+    for (int k = 0; k < ORC_NE; ++k) u += e[k];
+    return u;
+  };
+  int method = 1;
+  double fac[3] = {0.0, cgfac, sdfac};
+  const double rate[3] = {0.0, cgrate, sdrate};
+  double cur = evaluate(), prev = 0.0;
+  bool first = true;
+  int step = 0;
+  for (; step < max_steps && method != 0; ++step) {
+    std::memcpy(pos0.data(), pos, sizeof(double) * 3 * n);
+    const int used = method;
+    for (int i = 0; i < n; ++i) {
+      double* F = &f[3 * (size_t)i];
+      double H[3];
+      if (method == 1) {
+        double* F1 = &fprev[3 * (size_t)i];
+        const double ff = F[0] * F[0] + F[1] * F[1] + F[2] * F[2];
+        double f11 = F1[0] * F1[0] + F1[1] * F1[1] + F1[2] * F1[2];
+        if (f11 < 1e-8) f11 = ff;
+        const double gamma = f11 > 0.0 ? ff / f11 : 0.0;
+        for (int c = 0; c < 3; ++c) {
+          H[c] = (F[c] + dir[3 * (size_t)i + c] * gamma) * fac[1];
+          dir[3 * (size_t)i + c] = H[c];
+          F1[c] = F[c];
+        }
+      } else {
+        for (int c = 0; c < 3; ++c) H[c] = F[c] * fac[2];
+      }
+      for (int c = 0; c < 3; ++c) pos[3 * (size_t)i + c] += H[c];
+    }
+    if (o->s.ncons > 0) orc_shake(h, pos0.data(), pos, vel.data(), 1.0, 1e-12, 1000);
+    prev = cur;
+    cur = evaluate();
+    if (cur > prev && !first) {
+      std::memcpy(pos, pos0.data(), sizeof(double) * 3 * n);
+      cur = evaluate();
+      method = method == 1 ? 2 : 0;
+      --step;
+    } else {
+      if (energies) energies[step] = cur;
+      if (methods) methods[step] = used;
+    }
+    first = false;
+    if (step > 0 && step % 100 == 0 && method != 0) fac[method] *= rate[method] * 100.0;
+  }
+  return step;
+}
+
 void orc_normals(int n, uint64_t seed, uint32_t counter, double* out) {
   const uint64_t z = splitmix64(seed ^ (0xD1B54A32D192ED03ULL * ((uint64_t)counter + 1)));
   for (int a = 0; a < n; ++a) {

@@ -111,6 +111,13 @@ double orc_kinetic(void* h, const double* vel);
 int orc_md(void* h, double* pos, double* vel, int nsteps, double dt_ps, double tol,
            double* f, double* epot, double* ekin);
 
+/* energy minimisation (the reference's MinimizeStep loop: conjugate gradient, then
+ * steepest descent, undoing moves that raise the energy; src/dynamics.cu:491-620,
+ * src/mdcuda.cu:126-351, src/fenzi.cu:397-418); pos in/out, per counted step the
+ * potential energy and the method (1 CG, 2 SD) of its move (may be NULL); returns the
+ * number of counted steps */
+int orc_minimize(void* h, double* pos, int max_steps, double cgfac, double sdfac, double cgrate, double sdrate,
+                 double* energies, int* methods);
 /* Maxwell-Boltzmann velocity reassignment (counter-based RNG shared with the GPU),
  * COM momentum removal, RATTLE projection.  src/init.cu:19-211 */
 void orc_reassign_velocities(void* h, const double* pos, double T, uint64_t seed, uint32_t counter, double* vel);

@@ -45,6 +45,8 @@ def _lib():
     lib.orc_kinetic.restype = C.c_double
     lib.orc_kinetic.argtypes = [C.c_void_p, dp]
     lib.orc_md.argtypes = [C.c_void_p, dp, dp, C.c_int, C.c_double, C.c_double, dp, dp, dp]
+    lib.orc_minimize.argtypes = [C.c_void_p, dp, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, dp,
+                                 C.POINTER(C.c_int)]
     lib.orc_reassign_velocities.argtypes = [C.c_void_p, dp, C.c_double, C.c_uint64, C.c_uint32, dp]
     lib.orc_normals.argtypes = [C.c_int, C.c_uint64, C.c_uint32, dp]
     lib.orc_virial_fd.argtypes = [C.c_void_p, dp, C.c_double, C.c_int, C.c_int, dp]
@@ -183,6 +185,16 @@ class Oracle:
         bad = lib().orc_md(self.h, _dp(p), _dp(v), int(nsteps), float(dt_ps), float(tol), _dp(f),
                            _dp(ep) if traces else None, _dp(ek) if traces else None)
         return dict(pos=p, vel=v, f=f, epot=ep[:nsteps], ekin=ek[:nsteps], bad=bad)
+
+    def minimize(self, pos, max_steps, cgfac=1e-10, sdfac=1e-4, cgrate=0.1, sdrate=0.01):
+        """The reference's minimiser (CG then SD, moves that raise the energy undone);
+        returns final positions, per-step energies and methods of the counted steps."""
+        p = np.ascontiguousarray(pos, np.float64).copy()
+        e = np.zeros(max(1, max_steps))
+        m = np.zeros(max(1, max_steps), np.int32)
+        k = lib().orc_minimize(self.h, _dp(p), int(max_steps), float(cgfac), float(sdfac), float(cgrate),
+                               float(sdrate), _dp(e), m.ctypes.data_as(C.POINTER(C.c_int)))
+        return dict(pos=p, steps=k, energy=e[:k], method=m[:k])
 
     def virial_fd(self, pos, hrel=1e-6, terms=T_ALL, group=False):
         """Diagonal virial -L_a dU/dL_a by central differences: atomic scaling, or the

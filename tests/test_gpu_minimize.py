@@ -33,3 +33,31 @@ def test_minimize_lowers_energy_and_keeps_constraints():
     s.SingleStep(50)
     assert np.isfinite(s.EvalProps()["potential"])
     s.close()
+
+
+@pytest.mark.parametrize("nsteps", [1, 2, 5, 10, 20, 40])
+def test_minimize_moves_match_oracle(nsteps):
+    """The first moves of fz_minimize against the oracle's FP64 restatement of the
+    reference's MinimizeStep loop (CG moves with the per-atom gamma, the undo-and-switch
+    rule, SD moves) on a system without constraints, from the same positions: energy
+    and positions after each number of moves."""
+    g, path = system("min_free", name="custom", nw=200, nchains=2, chain_len=10, rc=7.0, ron=6.0, seed=13)
+    s = fz.FenZi.ReadInput(path)
+    s.cfg.shake = 0
+    # factors at which the third CG move raises the energy: undone, then SD moves
+    s.cfg.conjgradfac = 1e-3
+    s.cfg.steepdesfac = 2e-4
+    s.LoadSystem()
+    s.InitMem(0)
+    pos0 = s.positions()
+    k, e = s.Minimize(nsteps)
+    orc = oracle_for(s)
+    ref = orc.minimize(pos0, nsteps, cgfac=1e-3, sdfac=2e-4, cgrate=s.cfg.conjgradrate, sdrate=s.cfg.steepdesrate)
+    if nsteps >= 5:
+        assert list(ref["method"][:3]) == [1, 1, 2]  # the switch is exercised
+    assert k == ref["steps"], (k, ref["steps"], ref["method"])
+    assert abs(e - ref["energy"][-1]) <= 2e-5 * abs(ref["energy"][-1]), (e, ref["energy"][-1])
+    d = s.positions() - ref["pos"]
+    d -= np.round(d / s.cfg.box[0]) * s.cfg.box[0]
+    assert np.abs(d).max() <= 2e-4, np.abs(d).max()
+    s.close()
