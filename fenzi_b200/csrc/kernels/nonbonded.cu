@@ -55,7 +55,7 @@ struct PairConst {
   float p_b;              // p * beta
   float c2b;              // 2 beta / sqrt(pi)
   float sw_a, sw_b;       // t = sat(r2 * sw_a + sw_b)
-  float dsw_k;            // 12 / (rc^2 - ron^2)
+  float dsw_k;            // 12 / (rc^2 - ron^2) / 6 (the LJ table in shared memory holds 6 eps4)
 };
 
 __host__ __device__ inline PairConst pair_const(const SysParams& p) {
@@ -68,11 +68,16 @@ __host__ __device__ inline PairConst pair_const(const SysParams& p) {
   const float d = p.rc2 - p.ron2;
   c.sw_a = d > 0.f ? 1.f / d : 0.f;
   c.sw_b = d > 0.f ? -p.ron2 / d : 0.f;
-  c.dsw_k = d > 0.f ? 12.f / d : 0.f;
+  c.dsw_k = d > 0.f ? 2.f / d : 0.f;
   return c;
 }
 
-// force/r for one pair (FP32); returns 0 outside the cutoff or when masked
+// force/r for one pair (FP32); returns 0 outside the cutoff or when masked.  ls.x is
+// 6 eps4 (the shared-memory table is scaled by 6 when loaded), so with a6 = 6 eps4 s^6 and
+// b6 = a6 s^6 the unswitched LJ force/r is (2 b6 - a6) / r^2 and the LJ energy
+// (b6 - a6) / 6; both force parts share the 1 / r^2:
+//   F/r = [(2 b6 - a6) sw + qq e^{-b^2 r^2} (erfc(br)/(r e^{-b^2 r^2}) + 2b/sqrt(pi))] / r^2
+//         + (b6 - a6)/6 dsw
 template <bool ENERGY>
 __device__ __forceinline__ float pair_force(const PairConst& c, float r2, float qq, float2 ls, bool ok, float& ev,
                                             float& ee) {
@@ -81,23 +86,20 @@ __device__ __forceinline__ float pair_force(const PairConst& c, float r2, float 
   const float ex = ex2_a(r2 * c.eb2);                    // exp(-beta^2 r^2)
   const float tt = rcp_a(fmaf(c.p_b, r2 * rinv, 1.f));   // 1 / (1 + p beta r)
   const float poly = tt * fmaf(tt, fmaf(tt, fmaf(tt, fmaf(tt, kAS_a5, kAS_a4), kAS_a3), kAS_a2), kAS_a1);
-  // erfc(beta r) = poly exp(-beta^2 r^2), so F_C r / r^2 = qq (erfc(beta r)/r + 2 beta/sqrt(pi)
-  // exp(-beta^2 r^2)) / r^2 = qq exp(-beta^2 r^2) (poly / r + 2 beta/sqrt(pi)) / r^2
+  // erfc(beta r) = poly exp(-beta^2 r^2): F_C r / r^2 = qq exp(-beta^2 r^2) (poly / r + 2 beta/sqrt(pi)) / r^2
   const float qex = qq * ex;
-  const float fc = qex * fmaf(poly, rinv, c.c2b) * r2inv;
   const float s2 = ls.y * r2inv;
   const float s6 = s2 * s2 * s2;
-  const float a = ls.x * s6;
-  const float b = a * s6;
-  const float elj = b - a;
-  const float flj = fmaf(2.f, b, -a) * (6.f * r2inv);
+  const float a6 = ls.x * s6;
+  const float b6 = a6 * s6;
   const float t = __saturatef(fmaf(r2, c.sw_a, c.sw_b));
   const float t2 = t * t;
   const float sw = fmaf(-t2, fmaf(-2.f, t, 3.f), 1.f);
-  const float dsw = (t - t2) * c.dsw_k;
-  float fr = fmaf(flj, sw, fmaf(elj, dsw, fc));
+  const float e6 = b6 - a6;
+  const float h = fmaf(fmaf(2.f, b6, -a6), sw, qex * fmaf(poly, rinv, c.c2b));
+  const float fr = fmaf(h, r2inv, e6 * ((t - t2) * c.dsw_k));
   if (ENERGY) {
-    ev += ok ? elj * sw : 0.f;
+    ev += ok ? e6 * sw * (1.f / 6.f) : 0.f;
     ee += ok ? qex * poly * rinv : 0.f;
   }
   return ok ? fr : 0.f;
@@ -206,7 +208,7 @@ __device__ __forceinline__ void nonbonded_body(const SysParams& p, const PairCon
   __shared__ float4 jx_all[kWarps][64];
   __shared__ int jt_all[kWarps][64];
   const int nt1 = p.ntypes + 1;
-  for (int k = threadIdx.x; k < nt1 * nt1; k += blockDim.x) lj[k] = ljtab[k];
+  for (int k = threadIdx.x; k < nt1 * nt1; k += blockDim.x) lj[k] = make_float2(6.f * ljtab[k].x, ljtab[k].y);
   __syncthreads();
   const int nitems = counters[CNT_ITEMS];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
