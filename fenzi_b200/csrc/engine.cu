@@ -602,6 +602,13 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
     FZ_CUDA(cudaMemcpyAsync(&st_h, e->status, sizeof(int), cudaMemcpyDeviceToHost, e->st));
     FZ_CUDA(cudaStreamSynchronize(e->st));
   }
+  // the prune: a warp per i-block fills the GPU above ~16 blocks per SM; below, one CTA
+  // of 8 warps per block (the same lists, so the same forces); FZ_PRUNE_SPLIT=0/1 forces it
+  {
+    e->prune_split = (nblk < 16 * e->n_sm && fzk::prune_split_fits(e->ocap)) ? 1 : 0;
+    if (const char* v = std::getenv("FZ_PRUNE_SPLIT"))
+      e->prune_split = (std::atoi(v) != 0 && fzk::prune_split_fits(e->ocap)) ? 1 : 0;
+  }
   // tiles per pair-kernel work item: ~16 items per pair-kernel warp, 2 to 4 tiles,
   // so the warps run out of work together (the last items are short); measured at
   // 230,400 atoms (ms/step): 64 tiles 0.544, 16 0.532, 8 0.526, 4 0.526, 3 0.526, 2 0.539.

@@ -108,6 +108,8 @@ struct Engine {
   cudaGraph_t chunk_graph = nullptr;
   cudaGraphExec_t chunk_exec = nullptr;
   int chunk_steps = 100;
+  // prune with one CTA per i-block (systems with few blocks; identical lists)
+  int prune_split = 0;
   bool use_graph = true;
   // With cond_graph (env FZ_GRAPH_COND=1) the rebuild and prune kernels of captured
   // steps are the bodies of two conditional IF nodes set from the device flags, else
@@ -234,6 +236,7 @@ struct Engine {
     a.pos_prune = pos_prune;
     a.items = items;
     a.chunk = chunk;
+    a.prune_split = prune_split;
     a.blk_col = blk_col;
     a.dcx = dcx;
     a.dcy = dcy;

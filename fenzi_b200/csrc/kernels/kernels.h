@@ -69,7 +69,10 @@ struct RebuildArgs {
   float4* pos_prune;
   int2* items;   // pair-kernel work items (i-block, first tile)
   int chunk;     // tiles per work item
+  int prune_split;  // 1: prune with a CTA per i-block (small systems), same lists
 };
+// whether the CTA-per-block prune's shared memory (kNG x ocap entries) fits
+bool prune_split_fits(int ocap);
 void launch_rebuild(const RebuildArgs& a, cudaStream_t st);
 // the two halves of launch_rebuild: the outer-list build (flag) and the prune (flag_prune)
 void launch_rebuild_build(const RebuildArgs& a, cudaStream_t st);

@@ -638,6 +638,148 @@ __global__ void __launch_bounds__(256, 6) k_prune_b(const RebuildArgs* __restric
 }
 
 
+// The same prune with one CTA of kPruneWarps warps per i-block, for systems with too
+// few blocks to fill the GPU with a warp per block (a 9,000-atom box has ~290 blocks:
+// ~36 CTAs of the kernel above).  The block's outer entries are cut into contiguous
+// runs of whole 32-entry chunks, one run per warp; each warp keeps its entries for
+// each i-group (the same distance test) and stores them compacted at its run's start
+// in shared memory; the kept lists are then read in warp order, which is the outer
+// list's order, so the inner tiles, their exclusion masks and the work items are
+// identical to the warp-per-block prune's: the forces are bit-identical either way.
+constexpr int kPruneWarps = 8;
+
+__device__ __forceinline__ void prune_split_body(const RebuildArgs& A, int I) {
+  griddep_wait();
+  const SysParams p = A.p;
+  if (!*A.flag_prune) return;
+  const int nblk = A.counters[CNT_SLOTS] >> 5;
+  if (I >= nblk) return;
+  extern __shared__ uint32_t kept[];  // [kNG][ocap]
+  __shared__ float4 ipos[32];
+  __shared__ uint32_t msk_all[kPruneWarps][32];
+  __shared__ int cnt[kPruneWarps][kNG];
+  __shared__ int off[kPruneWarps + 1][kNG];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t* msk = msk_all[warp];
+  const int ocap = A.ocap;
+  const int islot = I * 32 + lane;
+  const float4 o = A.xyzq_s[I * 32];
+  if (warp == 0) {
+    const float4 pi = A.xyzq_s[islot];
+    const int ia = A.perm[islot];
+    if (ia >= 0) A.pos_prune[ia] = pi;
+    const float qx = pi.x - o.x, qy = pi.y - o.y, qz = pi.z - o.z;
+    ipos[lane] = make_float4(-2.f * qx, -2.f * qy, -2.f * qz, fmaf(qx, qx, fmaf(qy, qy, qz * qz)));
+    A.dmask[islot] = excl_mask(I, (uint32_t)islot, lane, msk, A.xn, A.xs, A.xmax);
+  }
+  __syncthreads();
+  const uint32_t dummy = (uint32_t)(p.nslots - 1) | ((uint32_t)kNoShift << kSlotBits);
+  const int n = A.outer_n[I];
+  const uint32_t* src = A.outer + (size_t)I * ocap;
+  const int nch = (n + 31) >> 5;
+  const int c_begin = (warp * nch) / kPruneWarps, c_end = ((warp + 1) * nch) / kPruneWarps;
+  const float rp2_keep = A.rp2 + 1e-3f;
+  int count[kNG];
+#pragma unroll
+  for (int s = 0; s < kNG; ++s) count[s] = 0;
+  for (int c = c_begin; c < c_end; ++c) {
+    const int e_i = c * 32 + lane;
+    const bool valid = e_i < n;
+    const uint32_t e = valid ? src[e_i] : dummy;
+    float4 r = A.xyzq_s[e & kSlotMask];
+    const int code = (int)(e >> kSlotBits);
+    if (code != kNoShift) {
+      const float3 sh = shift_of(code, p);
+      r.x += sh.x;
+      r.y += sh.y;
+      r.z += sh.z;
+    }
+    r.x -= o.x;
+    r.y -= o.y;
+    r.z -= o.z;
+    const float rr = fmaf(r.x, r.x, fmaf(r.y, r.y, r.z * r.z));
+    float m2[kNG];
+#pragma unroll
+    for (int s = 0; s < kNG; ++s) m2[s] = 3e38f;
+#pragma unroll
+    for (int k = 0; k < 32; ++k) {
+      const float4 q = ipos[k];
+      m2[k / kIG] = fminf(m2[k / kIG], fmaf(q.x, r.x, fmaf(q.y, r.y, fmaf(q.z, r.z, q.w))));
+    }
+#pragma unroll
+    for (int s = 0; s < kNG; ++s) {
+      const bool keep = valid && m2[s] + rr < rp2_keep;
+      const unsigned b = __ballot_sync(0xffffffffu, keep);
+      if (keep) kept[s * ocap + c_begin * 32 + count[s] + __popc(b & ((1u << lane) - 1u))] = e;
+      count[s] += __popc(b);
+    }
+  }
+  if (lane == 0)
+    for (int s = 0; s < kNG; ++s) cnt[warp][s] = count[s];
+  __syncthreads();
+  if (threadIdx.x < kNG) {
+    const int s = threadIdx.x;
+    int run = 0;
+    for (int w = 0; w < kPruneWarps; ++w) {
+      off[w][s] = run;
+      run += cnt[w][s];
+    }
+    off[kPruneWarps][s] = run;
+  }
+  __syncthreads();
+  // tiles: dense entry d of group s is entry d - off[w][s] of warp w's kept run
+  for (int s = 0; s < kNG; ++s) {
+    const int g = I * kNG + s;
+    const int total = off[kPruneWarps][s];
+    const int ntile = (total + 31) >> 5;
+    for (int t = warp; t < ntile; t += kPruneWarps) {
+      const int d = t * 32 + lane;
+      uint32_t je = dummy;
+      if (d < total) {
+        int w = 0;
+        while (w + 1 < kPruneWarps && off[w + 1][s] <= d) ++w;
+        const int cb = (w * nch) / kPruneWarps;
+        je = kept[s * ocap + cb * 32 + (d - off[w][s])];
+      }
+      A.inner[(size_t)g * ocap + t * 32 + lane] = je;
+      uint32_t wd = 0u;
+      if (__ballot_sync(0xffffffffu, (je & kExclBit) != 0u)) {
+        excl_mask(I, (je & kExclBit) ? je : dummy, lane, msk, A.xn, A.xs, A.xmax);
+        wd = lane < kIG ? msk[s * kIG + lane] : 0u;
+      }
+      int m = -1;
+      if (__ballot_sync(0xffffffffu, wd != 0)) {
+        if (lane == 0) m = atomicAdd(&A.counters[CNT_MASKS], 1);
+        m = __shfl_sync(0xffffffffu, m, 0);
+        if (m >= A.mask_cap) {
+          if (lane == 0) atomicOr(A.status, ST_MASK_OVERFLOW);
+          m = -1;
+        } else if (lane < kIG) {
+          A.masks[(size_t)m * kIG + lane] = wd;
+        }
+      }
+      if (lane == 0) A.inner_m[(size_t)g * (ocap >> 5) + t] = m;
+      __syncwarp();
+    }
+    if (warp == 0) {
+      const int nitems = (ntile + 1 + A.chunk - 1) / A.chunk;
+      int base = 0;
+      if (lane == 0) {
+        A.inner_nt[g] = ntile;
+        atomicAdd(&A.counters[CNT_TILES], ntile + 1);
+        base = atomicAdd(&A.counters[CNT_ITEMS], nitems);
+      }
+      base = __shfl_sync(0xffffffffu, base, 0);
+      for (int k = lane; k < nitems; k += 32) A.items[base + k] = make_int2(g, k * A.chunk);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kPruneWarps * 32) k_prune_split(RebuildArgs a) {
+  griddep_wait();
+  prune_split_body(a, blockIdx.x);
+}
+
 __device__ __forceinline__ void prune_end_body(const RebuildArgs& A, int bid, int nbid) {
   griddep_wait();
   int* flag_prune = A.flag_prune;
@@ -690,8 +832,23 @@ void launch_rebuild_prune(const RebuildArgs& a, cudaStream_t st) {
   const SysParams& p = a.p;
   const int maxblk = (p.nslots) / 32;
   launch_pdl(k_prune_begin, dim3(1), dim3(1), 0, st, a);
-  launch_pdl(k_prune, dim3((maxblk + 7) / 8), dim3(256), 0, st, a);
+  if (a.prune_split) {
+    const size_t smem = (size_t)kNG * a.ocap * sizeof(uint32_t);
+    launch_pdl(k_prune_split, dim3(maxblk), dim3(kPruneWarps * 32), smem, st, a);
+  } else {
+    launch_pdl(k_prune, dim3((maxblk + 7) / 8), dim3(256), 0, st, a);
+  }
   launch_pdl(k_prune_end, dim3(1), dim3(1), 0, st, a);
+}
+
+// (sets the kernel's dynamic shared-memory limit on the current device)
+bool prune_split_fits(int ocap) {
+  const size_t smem = (size_t)kNG * ocap * sizeof(uint32_t);
+  if (cudaFuncSetAttribute(k_prune_split, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return smem <= 160 * 1024;
 }
 
 // ------------------------------------------------------------------ batched launchers

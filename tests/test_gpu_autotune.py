@@ -2,7 +2,8 @@
 SM, PME brick edge, gather kernel) and keeps the fastest.  Every shape it can
 pick gives bit-identical forces, energies and trajectories, because forces, charge
 grids and energies are integer sums; this checks the defaults, the tuned shapes and
-two forced extremes against one another.
+two forced extremes against one another, with the prune as a warp per i-block and as
+a CTA per i-block (the same inner lists).
 """
 import os
 
@@ -14,12 +15,12 @@ from tests.helpers import system
 
 pytestmark = pytest.mark.gpu
 
-KNOBS = ("FZ_AUTOTUNE", "FZ_NB_CTAS_PER_SM", "FZ_PME_BRICK", "FZ_PME_GATHER")
+KNOBS = ("FZ_AUTOTUNE", "FZ_NB_CTAS_PER_SM", "FZ_PME_BRICK", "FZ_PME_GATHER", "FZ_PRUNE_SPLIT")
 SHAPES = [
     {"FZ_AUTOTUNE": "0"},
     {},
-    {"FZ_NB_CTAS_PER_SM": "2", "FZ_PME_BRICK": "4", "FZ_PME_GATHER": "1"},
-    {"FZ_NB_CTAS_PER_SM": "3", "FZ_PME_BRICK": "16", "FZ_PME_GATHER": "2"},
+    {"FZ_NB_CTAS_PER_SM": "2", "FZ_PME_BRICK": "4", "FZ_PME_GATHER": "1", "FZ_PRUNE_SPLIT": "1"},
+    {"FZ_NB_CTAS_PER_SM": "3", "FZ_PME_BRICK": "16", "FZ_PME_GATHER": "2", "FZ_PRUNE_SPLIT": "0"},
 ]
 
 

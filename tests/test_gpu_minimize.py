@@ -56,7 +56,10 @@ def test_minimize_moves_match_oracle(nsteps):
     if nsteps >= 5:
         assert list(ref["method"][:3]) == [1, 1, 2]  # the switch is exercised
     assert k == ref["steps"], (k, ref["steps"], ref["method"])
-    assert abs(e - ref["energy"][-1]) <= 2e-5 * abs(ref["energy"][-1]), (e, ref["energy"][-1])
+    # the potential is a small difference of large terms: tolerance on their scale
+    _, terms = orc.forces(ref["pos"])
+    scale = sum(abs(v) for v in terms.values())
+    assert abs(e - ref["energy"][-1]) <= 2e-6 * scale, (e, ref["energy"][-1], scale)
     d = s.positions() - ref["pos"]
     d -= np.round(d / s.cfg.box[0]) * s.cfg.box[0]
     assert np.abs(d).max() <= 2e-4, np.abs(d).max()
