@@ -67,6 +67,8 @@ def args_():
                     help="9,000-atom water box: timed product-path steps (plus plain path and CPU oracle); 0 skips it")
     ap.add_argument("--profile", action="store_true",
                     help="only run warm-up + steps (no timing/report): a clean target for ncu")
+    ap.add_argument("--profile-ensemble", action="store_true",
+                    help="only prepare the batched ensemble (--ensemble boxes) and run --steps batched steps")
     return ap.parse_args()
 
 
@@ -160,7 +162,7 @@ def traffic_from_profiles(kernel_file):
         return None
 
 
-def bench_ensemble(nsys, device, steps=30, dist=None, peak_tflops=None):
+def bench_ensemble(nsys, device, steps=200, dist=None, peak_tflops=None, profile_steps=0):
     """Aggregate atom-steps/s of nsys independent water boxes advanced together (one
     graph launch per step) versus the same boxes stepped one at a time; wall clock with
     a device synchronisation on both sides of each timed region.  Under a process group
@@ -191,6 +193,13 @@ def bench_ensemble(nsys, device, steps=30, dist=None, peak_tflops=None):
             sy.InitVelocity(T=300.0, seed=100 + i, counter=k + 1)
     batch.step(10)
     torch.cuda.synchronize()
+    if profile_steps:
+        batch.step(profile_steps)
+        torch.cuda.synchronize()
+        batch.close()
+        for sy in systems:
+            sy.close()
+        return None
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
@@ -204,7 +213,7 @@ def bench_ensemble(nsys, device, steps=30, dist=None, peak_tflops=None):
         return {"metric": "batched aggregate atom-steps/s", "value": natoms_all / tb, "unit": "atom-steps/s",
                 "systems": nsys, "atoms": natoms_all, "ms_per_batched_step": tb * 1e3, "n_gpus": world,
                 "scaling": "strong", "sharding": "longest-processing-time-first on atoms, one batch per rank",
-                "timing": "wall clock over 30 batched steps, max over ranks"}
+                "timing": f"wall clock over {steps} batched steps (100-step graphs), max over ranks"}
     seq_steps = max(3, steps // 3)
     for sy in systems:  # warm each system's own graph
         sy.SingleStep(1)
@@ -254,8 +263,8 @@ def bench_ensemble(nsys, device, steps=30, dist=None, peak_tflops=None):
                             f"its own plain-path engine from its current state, 3 warm-up + 10 timed steps",
             "workload": f"{nsys} TIP3P boxes, 216-2000 waters each at 0.0334/A^3, grids 16^3-36^3 (smallest "
                         f"2^a3^b5^c >= L/1.2), rc 9 / ron 7.5, beta 0.34, SHAKE, NVE, 1 fs; seeded",
-            "timing": "wall clock over 30 batched steps vs 10-step sweeps of the boxes one at a time, device "
-                      "synchronised around each; working set > L2"}
+            "timing": f"wall clock over {steps} batched steps (100-step graphs) vs a sweep of {seq_steps}-step runs "
+                      "of each box alone, device synchronised around each; working set > L2"}
 
 
 def bench_small(device, peak_tflops, steps=2000):
@@ -676,6 +685,9 @@ def main():
     a = args_()
     if a.impl == "reference":
         return run_reference(a)
+    if a.profile_ensemble:
+        bench_ensemble(a.ensemble, 0, profile_steps=a.steps)
+        return 0
     import torch
     import fenzi_b200 as fz
     rank = int(os.environ.get("RANK", "0"))
