@@ -207,12 +207,31 @@ static fz_status build_batch_kernels(fz_batch* b) {
   // member running alone, where a small system often does best on 2 CTAs per SM.
   long long natoms = 0;
   for (const fz_system* s : b->systems) natoms += s->top.n;
+  bool big_bricks = true;
+  if (const char* v = std::getenv("FZ_BATCH_BRICK")) big_bricks = std::atoi(v) != 0;
   for (int i = 0; i < ns; ++i) {
     Engine* e = b->systems[i]->eng;
     rb.push_back(e->rebuild_args());
     nb.push_back(e->nb_args());
     bd.push_back(e->bonded_args());
     pme.push_back(e->pme_args());
+    if (big_bricks) {
+      // a batch has CTAs to spare: bricks as large as the spread's shared region allows
+      // (largest divisor of K in [4, 16]) give each spread / gather CTA hundreds of
+      // atoms instead of the ~15 a member's solo shape (>= 256 bricks) leaves it; grid
+      // charges are integer sums and the gather's sums run in the same order, so the
+      // results do not change
+      fzk::PmeArgs& q = pme.back();
+      for (int d = 0; d < 3; ++d) {
+        int best = 0;
+        for (int c = 4; c <= 16; ++c)
+          if (q.K[d] % c == 0) best = c;
+        if (best) {
+          q.B[d] = best;
+          q.nb[d] = q.K[d] / best;
+        }
+      }
+    }
     const fzk::SysParams& p = rb.back().p;
     const fzk::PmeArgs& pa = pme.back();
     const int nbr = pa.nb[0] * pa.nb[1] * pa.nb[2];
