@@ -201,14 +201,20 @@ static fz_status build_batch_kernels(fz_batch* b) {
   std::vector<ClassAcc> cls;
   struct SizeAcc { int N; std::vector<int4> plane, z; };
   std::vector<SizeAcc> sizes;
-  // pair-kernel CTAs: the batch's total is one full wave of the batched pair kernel
-  // (kNbBatchCtasPerSm per SM), shared out in proportion to the members' atoms, at
-  // least one each.  Not the members' own nb_grid: the autotuner sizes that for a
+  // pair-kernel CTAs: the batch's total is nb_waves full waves of the batched pair
+  // kernel (kNbBatchCtasPerSm per SM), shared out in proportion to the members' atoms,
+  // at least one each.  Not the members' own nb_grid: the autotuner sizes that for a
   // member running alone, where a small system often does best on 2 CTAs per SM.
   long long natoms = 0;
   for (const fz_system* s : b->systems) natoms += s->top.n;
   bool big_bricks = true;
   if (const char* v = std::getenv("FZ_BATCH_BRICK")) big_bricks = std::atoi(v) != 0;
+  // several waves of pair-kernel CTAs: each CTA drains its member's work queue and a
+  // finished CTA's slot takes the next CTA of the launch, so members whose rounded
+  // share of CTAs is short finish with the rest (one wave ends with the member of the
+  // largest work per CTA, up to 1.5x the mean)
+  int nb_waves = 2;
+  if (const char* v = std::getenv("FZ_BATCH_NB_WAVES")) nb_waves = std::max(1, std::min(16, std::atoi(v)));
   for (int i = 0; i < ns; ++i) {
     Engine* e = b->systems[i]->eng;
     rb.push_back(e->rebuild_args());
@@ -242,7 +248,8 @@ static fz_status build_batch_kernels(fz_batch* b) {
     add_blocks(tabs[fzk::BT_SLOTS256], i, (p.nslots + 255) / 256);
     add_blocks(tabs[fzk::BT_BLOCKS8], i, (p.nslots / 32 + 7) / 8);
     add_blocks(tabs[fzk::BT_NB], i,
-               std::max(1, (int)std::lround((double)e->n_sm * fzk::kNbBatchCtasPerSm * p.n / (double)std::max(1LL, natoms))));
+               std::max(1, (int)std::lround((double)e->n_sm * fzk::kNbBatchCtasPerSm * nb_waves * p.n /
+                                            (double)std::max(1LL, natoms))));
     add_blocks(tabs[fzk::BT_BONDED], i, fzk::bonded_blocks(bd.back()));
     add_blocks(tabs[fzk::BT_BRICKS256], i, (nbr + 255) / 256);
     add_blocks(tabs[fzk::BT_BRICKS], i, nbr);
