@@ -387,7 +387,7 @@ def served_jobs(njobs, seed):
     return jobs
 
 
-def bench_served(device, njobs=256, seed=4242, check=4, sample=32, max_running=64):
+def bench_served(device, njobs=256, seed=4242, check=4, sample=32, max_running=64, dist=None):
     """Served jobs through the serving loop (fz_server): each job of the seeded stream
     is submitted at its Poisson arrival time and admitted in FIFO order while fewer
     than `max_running` jobs run and their device bytes fit the 150 GB HBM budget, so
@@ -396,12 +396,22 @@ def bench_served(device, njobs=256, seed=4242, check=4, sample=32, max_running=6
     Per job: queue wait = start - submission, service = end - start, latency = end -
     submission, all on the server's steady clock.  The one-at-a-time comparisons time
     a seeded sample of `sample` jobs alone (200 steps on the product path, 30 on the
-    plain path, each scaled to the job's step count)."""
+    plain path, each scaled to the job's step count).
+    Under a process group the stream is routed online (each arrival to the rank with
+    the least atoms x steps routed so far, the same on every rank) and each rank serves
+    its jobs on its GPU; latencies are pooled over the ranks and the aggregate rate is
+    all atom-steps over the slowest rank's makespan (no one-at-a-time comparison)."""
     import torch
     import fenzi_b200 as fz
     from fenzi_b200 import gen_system
+    from fenzi_b200.shard import route_online
     from oracle.oracle import Oracle
-    jobs = served_jobs(njobs, seed)
+    world = dist.get_world_size() if dist else 1
+    rank = dist.get_rank() if dist else 0
+    stream = served_jobs(njobs, seed)
+    costs = [(3 * j["nw"] + 30 * j["nchains"]) * j["steps"] for j in stream]
+    mine = route_online(costs, world)[rank]
+    jobs = [stream[i] for i in mine]
     root = tempfile.mkdtemp(prefix="fzserve_")
     paths, gens = [], []
     for i, j in enumerate(jobs):
@@ -417,9 +427,10 @@ def bench_served(device, njobs=256, seed=4242, check=4, sample=32, max_running=6
             s.cfg.temp_reset_every = 1000
         return s.LoadSystem()
 
-    # one at a time, on a seeded sample of the stream
+    # one at a time, on a seeded sample of the stream (one GPU only)
     from fenzi_b200.plain import Plain
-    pick = sorted(np.random.default_rng(seed + 1).choice(len(jobs), min(sample, len(jobs)), replace=False))
+    pick = sorted(np.random.default_rng(seed + 1).choice(len(jobs), min(sample, len(jobs)), replace=False)) \
+        if world == 1 else []
     seq_s, plain_s, sample_work = 0.0, 0.0, 0.0
     for i in pick:
         j = jobs[i]
@@ -447,6 +458,8 @@ def bench_served(device, njobs=256, seed=4242, check=4, sample=32, max_running=6
     server = fz.Server(device, hbm_budget_bytes=150e9, chunk_steps=100, max_running=max_running)
     ids = []
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
     for i, j in enumerate(jobs):
         d = j["arrival"] - (time.perf_counter() - t0)
@@ -473,6 +486,26 @@ def bench_served(device, njobs=256, seed=4242, check=4, sample=32, max_running=6
         s.close()
     server.close()
     pct = lambda a, q: float(np.percentile(a, q))
+    if world > 1:
+        parts = [None] * world
+        dist.all_gather_object(parts, (lat.tolist(), wait.tolist(), serv.tolist(), total, wall, errs,
+                                       stats["peak_running"]))
+        lat = np.array([x for p in parts for x in p[0]])
+        wait = np.array([x for p in parts for x in p[1]])
+        serv = np.array([x for p in parts for x in p[2]])
+        total = sum(p[3] for p in parts)
+        wall = max(p[4] for p in parts)
+        errs = [e for p in parts for e in p[5]]
+        return {"metric": "served p50/p99 job latency", "p50_s": pct(lat, 50), "p99_s": pct(lat, 99), "unit": "s",
+                "jobs": len(stream), "n_gpus": world,
+                "queue_wait_s": {"p50": pct(wait, 50), "p99": pct(wait, 99), "max": float(wait.max())},
+                "service_s": {"p50": pct(serv, 50), "p99": pct(serv, 99)},
+                "aggregate_atom_steps_per_s": total / wall, "makespan_s": wall, "max_running_per_gpu": max_running,
+                "peak_running_jobs_per_gpu": [p[6] for p in parts],
+                "routing": "online: each arrival to the rank with the least atoms x steps routed so far",
+                "final_frame_force_rel_rms_vs_oracle": {"max": max(errs), "jobs_checked": len(errs)},
+                "timing": "wall clock from a barrier before the first submission to each rank's last "
+                          "completion; the aggregate uses the slowest rank"}
     return {"metric": "served p50/p99 job latency", "p50_s": pct(lat, 50), "p99_s": pct(lat, 99), "unit": "s",
             "jobs": len(jobs), "queue_wait_s": {"p50": pct(wait, 50), "p99": pct(wait, 99), "max": float(wait.max())},
             "service_s": {"p50": pct(serv, 50), "p99": pct(serv, 99)},
@@ -778,6 +811,8 @@ def main():
 
     # batched ensemble sharded over the ranks (every rank takes part)
     batched_multi = bench_ensemble(a.ensemble, local, dist=dist) if a.ensemble > 0 and world > 1 else None
+    # served stream routed over the ranks (every rank takes part)
+    served_multi = bench_served(local, a.served, dist=dist) if a.served > 0 and world > 1 else None
     line = None
     if rank == 0:
         # roofline of the dominant kernel (real-space pairs): algorithmic FLOPs / measured duration
@@ -814,7 +849,7 @@ def main():
         batched = batched_multi
         if a.ensemble > 0 and world == 1:
             batched = bench_ensemble(a.ensemble, local, peak_tflops=peak)
-        served = None
+        served = served_multi
         if a.served > 0 and world == 1:
             served = bench_served(local, a.served)
         precision = None

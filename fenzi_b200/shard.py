@@ -2,9 +2,10 @@
 
 A single system does not shard (one system per GPU, replicas only); a set of
 independent systems does, with no per-step exchange: each rank takes a subset and runs
-it as its own batch.  The subsets come from longest-processing-time-first greedy
-assignment on a per-system cost (atoms x steps), identical on every rank because it
-depends only on the costs.
+it as its own batch or serving loop.  A known set (the ensemble) is split by
+longest-processing-time-first greedy assignment on a per-system cost (atoms x steps);
+a stream of served jobs is routed online, each arrival to the least-loaded rank.  Both
+are identical on every rank because they depend only on the costs.
 """
 from __future__ import annotations
 
@@ -23,6 +24,22 @@ def lpt_assign(costs, nranks: int):
         out[r].append(i)
         load[r] += float(costs[i])
     return [sorted(x) for x in out]
+
+
+def route_online(costs, nranks: int):
+    """Routes a stream of jobs (in arrival order, cost costs[i] = atoms x steps) to
+    ranks as they arrive: each job to the rank with the least work routed to it so far
+    (lowest rank on ties).  The rule needs no knowledge of later jobs, and every rank
+    derives the same routing from the same stream.  Returns the job indices per rank."""
+    if nranks < 1:
+        raise ValueError("nranks must be >= 1")
+    load = [0.0] * nranks
+    out = [[] for _ in range(nranks)]
+    for i, c in enumerate(costs):
+        r = min(range(nranks), key=lambda k: (load[k], k))
+        out[r].append(i)
+        load[r] += float(c)
+    return out
 
 
 def max_over_ranks(value: float, dist=None, device=None) -> float:
