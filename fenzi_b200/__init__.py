@@ -348,7 +348,7 @@ class FenZi:
         out = (C.c_int * 7)()
         _check(lib().fz_get_launch_shapes(self.h, out))
         return dict(chunk_tiles=out[0], nb_ctas_per_sm=out[1], pme_brick=[out[2], out[3], out[4]],
-                    gather={0: "auto", 1: "brick", 2: "atom"}[out[5]], autotuned=bool(out[6]))
+                    gather={0: "auto", 1: "brick", 2: "atom", 3: "atom-spread"}[out[5]], autotuned=bool(out[6]))
 
     def stage_timing(self, enable=True):
         _check(lib().fz_set_stage_timing(self.h, 1 if enable else 0))

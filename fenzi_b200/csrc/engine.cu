@@ -187,6 +187,17 @@ static fz_status autotune(Engine* e) {
           gpick = g;
         }
       }
+    // no bricks at all: atom spread (RED into the grid) and atom gather
+    if (!fix_brick) {
+      set_bricks(e, cands[0]);
+      e->gather_mode = 3;
+      const float t = time_launches(e->st, [&] { fzk::launch_pme(e->pme_args(), false, e->st); });
+      if (t < 0.99f * best) {
+        best = t;
+        bpick = cands[0];
+        gpick = 3;
+      }
+    }
     set_bricks(e, bpick);
     e->gather_mode = gpick;
   }
@@ -292,7 +303,7 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
     e->nbk[d] = e->K[d] / e->B[d];
     p.K[d] = e->K[d];
   }
-  if (const char* v = std::getenv("FZ_PME_GATHER")) e->gather_mode = std::max(0, std::min(2, std::atoi(v)));
+  if (const char* v = std::getenv("FZ_PME_GATHER")) e->gather_mode = std::max(0, std::min(3, std::atoi(v)));
   // per-block list capacity: atoms within rlist of a block box (Minkowski volume of a
   // box ~1.4 a), with room for blocks that see all their neighbours at higher index
   const double ab = 1.4 * a, R = plist;

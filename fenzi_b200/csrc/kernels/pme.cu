@@ -228,6 +228,46 @@ __device__ __forceinline__ void pme_spread_body(const PmeArgs& a, int bid, int n
 }
 
 __global__ void __launch_bounds__(256) k_pme_spread(PmeArgs a) { griddep_wait(); pme_spread_body(a, blockIdx.x, gridDim.x); }
+
+// One thread per atom, each of its 64 weights added straight into the int32 charge grid
+// (RED atomics in L2; the grid of a small system stays there).  The values added are the
+// brick spread's own (same expressions), and integer sums do not depend on the order, so
+// the grid is bit-identical to the brick spread's; with no brick lists the bin, scan and
+// scatter launches disappear, which is what a small system's step is made of.
+__global__ void __launch_bounds__(256) k_pme_spread_atoms(PmeArgs a) {
+  griddep_wait();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  const int Kx = a.K[0], Ky = a.K[1], Kz = a.K[2];
+  const float4 r = a.pos4[i];
+  float tx, ty, tz, wx[4], wy[4], wz[4];
+  const int kx = grid_base(r.x, a.p.inv_box.x, Kx, &tx);
+  const int ky = grid_base(r.y, a.p.inv_box.y, Ky, &ty);
+  const int kz = grid_base(r.z, a.p.inv_box.z, Kz, &tz);
+  bsp4(tx, wx, nullptr);
+  bsp4(ty, wy, nullptr);
+  bsp4(tz, wz, nullptr);
+  const float q = r.w * kFixQ32;
+  int* g = reinterpret_cast<int*>(a.grid);
+#pragma unroll
+  for (int jz = 0; jz < 4; ++jz) {
+    int z = kz - jz;
+    z += z < 0 ? Kz : 0;
+#pragma unroll
+    for (int jy = 0; jy < 4; ++jy) {
+      int y = ky - jy;
+      y += y < 0 ? Ky : 0;
+      const float qzy = q * wz[jz] * wy[jy];
+      int* row = g + ((size_t)z * Ky + y) * Kx;
+#pragma unroll
+      for (int jx = 0; jx < 4; ++jx) {
+        int x = kx - jx;
+        x += x < 0 ? Kx : 0;
+        atomicAdd(row + x, __float2int_rn(qzy * wx[jx]));
+      }
+    }
+  }
+}
 __global__ void __launch_bounds__(256) k_pme_spread_b(const PmeArgs* __restrict__ args, const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const PmeArgs a = args[t.x];
@@ -469,7 +509,7 @@ __device__ __forceinline__ void pme_gather_atoms_body(const PmeArgs& a, int bid,
   griddep_wait();
   const int t = bid * blockDim.x + threadIdx.x;
   if (t >= a.n) return;
-  const int i = a.brick_atoms[t];
+  const int i = a.gather == 3 ? t : a.brick_atoms[t];  // mode 3: no brick lists, atom order
   const int Kx = a.K[0], Ky = a.K[1], Kz = a.K[2];
   const float4 r = a.pos4[i];
   float tx, ty, tz, wx[4], wy[4], wz[4], dx[4], dy[4], dz[4];
@@ -1115,17 +1155,33 @@ static int lines_for(int n) { return fft_lines_per_block(n); }
 constexpr int kGatherBrickAtoms = 128;
 
 // zero, bin, scan, scatter, spread, 3 or 5 FFT kernels, gather
-int pme_launches(const PmeArgs& a) { return 5 + (use_plane_fft(a) ? 3 : 5) + 1; }
+// gather / spread mode: FZ_PME_GATHER overrides the tuned one (0 by atoms per brick,
+// 1 brick gather, 2 per-atom gather in brick order, 3 atom spread and atom gather)
+static int pme_mode(const PmeArgs& a) {
+  const char* gv = std::getenv("FZ_PME_GATHER");
+  return gv ? std::max(0, std::min(3, std::atoi(gv))) : a.gather;
+}
 
-void launch_pme(const PmeArgs& a, bool energy, cudaStream_t st) {
+int pme_launches(const PmeArgs& a) {
+  return (pme_mode(a) == 3 ? 1 : 5) + (use_plane_fft(a) ? 3 : 5) + 1;
+}
+
+void launch_pme(const PmeArgs& a_in, bool energy, cudaStream_t st) {
+  PmeArgs a = a_in;
+  a.gather = pme_mode(a_in);
   const int nbr = a.nb[0] * a.nb[1] * a.nb[2];
-  launch_pdl(k_pme_zero, dim3((nbr + 255) / 256), dim3(256), 0, st, a);
-  launch_pdl(k_pme_bin, dim3((a.n + 255) / 256), dim3(256), 0, st, a);
-  launch_pdl(k_pme_scan, dim3(1), dim3(1024), 0, st, a);
-  launch_pdl(k_pme_scatter, dim3((a.n + 255) / 256), dim3(256), 0, st, a);
   const size_t sp = (size_t)(a.B[0] + 3) * (a.B[1] + 3) * (a.B[2] + 3) * sizeof(int);
-  cudaMemsetAsync(a.grid, 0, (size_t)a.K[0] * a.K[1] * a.K[2] * sizeof(float), st);
-  launch_pdl(k_pme_spread, dim3(nbr), dim3(256), sp, st, a);
+  if (a.gather == 3) {
+    cudaMemsetAsync(a.grid, 0, (size_t)a.K[0] * a.K[1] * a.K[2] * sizeof(float), st);
+    launch_pdl(k_pme_spread_atoms, dim3((a.n + 255) / 256), dim3(256), 0, st, a);
+  } else {
+    launch_pdl(k_pme_zero, dim3((nbr + 255) / 256), dim3(256), 0, st, a);
+    launch_pdl(k_pme_bin, dim3((a.n + 255) / 256), dim3(256), 0, st, a);
+    launch_pdl(k_pme_scan, dim3(1), dim3(1024), 0, st, a);
+    launch_pdl(k_pme_scatter, dim3((a.n + 255) / 256), dim3(256), 0, st, a);
+    cudaMemsetAsync(a.grid, 0, (size_t)a.K[0] * a.K[1] * a.K[2] * sizeof(float), st);
+    launch_pdl(k_pme_spread, dim3(nbr), dim3(256), sp, st, a);
+  }
   const int Kx = a.K[0], Ky = a.K[1], Kz = a.K[2], Kxh = Kx / 2 + 1;
   const FftPlan px = make_plan(Kx), py = make_plan(Ky), pz = make_plan(Kz);
   const int lx = lines_for(Kx), ly = lines_for(Ky), lz = lines_for(Kz);
@@ -1155,10 +1211,8 @@ void launch_pme(const PmeArgs& a, bool energy, cudaStream_t st) {
     if (!fft_y_t(a, ly, true, gy, smy, st)) launch_pdl(k_fft_y, dim3(gy), dim3(256), smy, st, a, py, ly, 1);
     if (!fft_x_c2r_t(a, lx, gx2, smx, st)) launch_pdl(k_fft_x_c2r, dim3(gx), dim3(256), smx, st, a, px, lx);
   }
-  // FZ_PME_GATHER=1 forces the brick gather, 2 the per-atom gather
-  const char* gv = std::getenv("FZ_PME_GATHER");
-  const int gmode = gv ? std::atoi(gv) : a.gather;
-  if (gmode == 1 || (gmode != 2 && (size_t)a.n <= (size_t)kGatherBrickAtoms * nbr))
+  const int gmode = a.gather;
+  if (gmode == 1 || (gmode == 0 && (size_t)a.n <= (size_t)kGatherBrickAtoms * nbr))
     launch_pdl(k_pme_gather, dim3(nbr), dim3(256), sp, st, a);
   else
     launch_pdl(k_pme_gather_atoms, dim3((a.n + 255) / 256), dim3(256), 0, st, a);

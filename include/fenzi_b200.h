@@ -221,7 +221,8 @@ fz_status fz_get_counters(fz_system* sys, long long* out4);
 /* Launch shapes in use: [0] pair tiles per pair-kernel work item (a fixed rule of the
  * tile count), [1] pair-kernel CTAs per SM, [2..4] PME brick edge per dimension
  * (charge-spread and gather block shape), [5] gather kernel (0 by atoms per brick, 1
- * one CTA per brick, 2 one thread per atom), [6] 1 when the autotuner picked [1..5]
+ * one CTA per brick, 2 one thread per atom, 3 one thread per atom for the spread too,
+ * without brick lists), [6] 1 when the autotuner picked [1..5]
  * at fz_upload (unless FZ_AUTOTUNE=0; every shape it can pick gives bit-identical
  * results).  No reference counterpart: the reference fixes its block sizes at
  * compile time (src/prmread.cu:109-115). */

@@ -2,8 +2,9 @@
 SM, PME brick edge, gather kernel) and keeps the fastest.  Every shape it can
 pick gives bit-identical forces, energies and trajectories, because forces, charge
 grids and energies are integer sums; this checks the defaults, the tuned shapes and
-two forced extremes against one another, with the prune as a warp per i-block and as
-a CTA per i-block (the same inner lists).
+forced shapes against one another: the prune as a warp per i-block and as a CTA per
+i-block (the same inner lists), and the PME spread through per-brick shared-memory
+regions and straight into the grid with no brick lists (the same integer grid).
 """
 import os
 
@@ -21,6 +22,7 @@ SHAPES = [
     {},
     {"FZ_NB_CTAS_PER_SM": "2", "FZ_PME_BRICK": "4", "FZ_PME_GATHER": "1", "FZ_PRUNE_SPLIT": "1"},
     {"FZ_NB_CTAS_PER_SM": "3", "FZ_PME_BRICK": "16", "FZ_PME_GATHER": "2", "FZ_PRUNE_SPLIT": "0"},
+    {"FZ_NB_CTAS_PER_SM": "4", "FZ_PME_GATHER": "3"},
 ]
 
 
@@ -57,6 +59,7 @@ def test_every_shape_bit_identical(key):
     assert runs[1][0]["autotuned"]
     assert runs[2][0]["nb_ctas_per_sm"] == 2 and runs[2][0]["pme_brick"] == [4, 4, 4]
     assert runs[3][0]["nb_ctas_per_sm"] == 3 and runs[3][0]["gather"] == "atom"
+    assert runs[4][0]["gather"] == "atom-spread"
     shapes0, f0, e0, p0 = runs[0]
     assert np.any(f0 != 0)
     for shapes, f, e, p in runs[1:]:
