@@ -171,33 +171,24 @@ static fz_status autotune(Engine* e) {
   if (!(fix_brick && fix_gather)) {
     std::vector<std::array<int, 3>> cands = brick_candidates(e->K);
     if (fix_brick) cands = {{e->B[0], e->B[1], e->B[2]}};
+    // gather modes tried per brick shape (the environment's alone when it fixes one);
+    // mode 3 (no brick lists) does not depend on the brick shape: tried once
+    const std::vector<int> gmodes = fix_gather ? std::vector<int>{e->gather_mode} : std::vector<int>{0, 1, 2, 3};
     std::array<int, 3> bpick = cands[0];
-    int gpick = 0;
-    set_bricks(e, bpick);
-    e->gather_mode = 0;
-    float best = time_launches(e->st, [&] { fzk::launch_pme(e->pme_args(), false, e->st); });
-    for (const auto& b : cands)
-      for (int g : {1, 2}) {
-        set_bricks(e, b);
+    int gpick = gmodes[0];
+    float best = 3e38f;
+    for (size_t ib = 0; ib < cands.size(); ++ib)
+      for (int g : gmodes) {
+        if (g == 3 && ib > 0) continue;
+        set_bricks(e, cands[ib]);
         e->gather_mode = g;
         const float t = time_launches(e->st, [&] { fzk::launch_pme(e->pme_args(), false, e->st); });
         if (t < 0.99f * best) {
           best = t;
-          bpick = b;
+          bpick = cands[ib];
           gpick = g;
         }
       }
-    // no bricks at all: atom spread (RED into the grid) and atom gather
-    if (!fix_brick) {
-      set_bricks(e, cands[0]);
-      e->gather_mode = 3;
-      const float t = time_launches(e->st, [&] { fzk::launch_pme(e->pme_args(), false, e->st); });
-      if (t < 0.99f * best) {
-        best = t;
-        bpick = cands[0];
-        gpick = 3;
-      }
-    }
     set_bricks(e, bpick);
     e->gather_mode = gpick;
   }
