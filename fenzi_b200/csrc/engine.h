@@ -261,6 +261,9 @@ struct Engine {
     a.items = items;
     a.chunk = chunk;
     a.grid = nb_grid;
+    // FZ_NB_GRID_PER_SM: fewer CTAs than the build's occupancy, leaving room on every SM
+    // for the PME kernels of the second stream (a measurement knob)
+    if (const char* v = std::getenv("FZ_NB_GRID_PER_SM")) a.grid = n_sm * std::max(1, std::min(8, std::atoi(v)));
     a.minb = nb_per_sm;
     return a;
   }
