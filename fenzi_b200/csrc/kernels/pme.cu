@@ -626,7 +626,18 @@ __global__ void __launch_bounds__(256) k_pme_gather_b(const PmeArgs* __restrict_
 // ------------------------------------------------------------------ compile-time FFT
 // The same Stockham autosort algorithm with the line length N a template parameter:
 // radices, strides and twiddle steps are constants, the small DFTs use constant roots.
-__host__ __device__ constexpr int radix_of(int m) { return m % 4 == 0 ? 4 : (m % 2 == 0 ? 2 : (m % 3 == 0 ? 3 : 5)); }
+// Radices 16 and 8 come first (128 = 16 x 8: two passes through shared memory per
+// line instead of four with radix 4), each DFT held in registers.
+__host__ __device__ constexpr int radix_of(int m) {
+  return m % 16 == 0 ? 16 : (m % 8 == 0 ? 8 : (m % 4 == 0 ? 4 : (m % 2 == 0 ? 2 : (m % 3 == 0 ? 3 : 5))));
+}
+
+// Shared-memory layout of a contiguous line: element i sits at sk(i) = i + i / 16 and
+// lines are fft_ld(N) apart.  A radix-R stage's first pass stores each thread's R
+// outputs at stride R; the pad slot every 16 elements spreads those stores over all
+// banks instead of a few (stride 16 float2 would put a half-warp on one bank).
+__host__ __device__ constexpr int fft_ld(int n) { return n + n / 16 + 1; }
+__device__ __forceinline__ int sk(int i) { return i + (i >> 4); }
 __host__ __device__ constexpr int radix_at(int n, int s) {
   int m = n, r = 1;
   for (int k = 0; k <= s; ++k) {
@@ -644,10 +655,66 @@ __host__ __device__ constexpr int nstages(int n) {
   return c;
 }
 
+// v e^{sg 2 pi i m / 16} for m known after unrolling (sg = -1 forward, +1 inverse);
+// the quarter turns are exact swaps and sign flips
+template <bool INV>
+__device__ __forceinline__ float2 rot16(float2 v, int m) {
+  const float sg = INV ? 1.f : -1.f;
+  constexpr float c1 = 0.92387953251128674f, s1 = 0.38268343236508977f, h = 0.70710678118654752f;
+  switch (m & 15) {
+    case 0: return v;
+    case 4: return make_float2(-sg * v.y, sg * v.x);
+    case 8: return make_float2(-v.x, -v.y);
+    case 12: return make_float2(sg * v.y, -sg * v.x);
+    case 1: return cmul(v, make_float2(c1, sg * s1));
+    case 2: return cmul(v, make_float2(h, sg * h));
+    case 3: return cmul(v, make_float2(s1, sg * c1));
+    case 5: return cmul(v, make_float2(-s1, sg * c1));
+    case 6: return cmul(v, make_float2(-h, sg * h));
+    case 7: return cmul(v, make_float2(-c1, sg * s1));
+    case 9: return cmul(v, make_float2(-c1, -sg * s1));
+    case 10: return cmul(v, make_float2(-h, -sg * h));
+    case 11: return cmul(v, make_float2(-s1, -sg * c1));
+    case 13: return cmul(v, make_float2(s1, -sg * c1));
+    case 14: return cmul(v, make_float2(h, -sg * h));
+    default: return cmul(v, make_float2(c1, -sg * s1));
+  }
+}
+
 template <int R, bool INV>
 __device__ __forceinline__ void small_dft(float2* v) {
   const float sg = INV ? 1.f : -1.f;  // exponent sign
-  if constexpr (R == 2) {
+  if constexpr (R == 16) {
+    // 16 = 4 x 4: with n = r + 4q and k = k1 + 4 k2, W16^{nk} = W4^{q k1} W16^{r k1} W4^{r k2}
+    float2 t[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) t[r][q] = v[r + 4 * q];
+      small_dft<4, INV>(t[r]);
+#pragma unroll
+      for (int k1 = 1; k1 < 4; ++k1) t[r][k1] = rot16<INV>(t[r][k1], r * k1);
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+      float2 u[4] = {t[0][k1], t[1][k1], t[2][k1], t[3][k1]};
+      small_dft<4, INV>(u);
+#pragma unroll
+      for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = u[k2];
+    }
+  } else if constexpr (R == 8) {
+    // 8 = 2 x 4: even and odd halves, the odd one turned by W8^k
+    float2 e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+    small_dft<4, INV>(e);
+    small_dft<4, INV>(o);
+#pragma unroll
+    for (int k = 1; k < 4; ++k) o[k] = rot16<INV>(o[k], 2 * k);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      v[k] = make_float2(e[k].x + o[k].x, e[k].y + o[k].y);
+      v[k + 4] = make_float2(e[k].x - o[k].x, e[k].y - o[k].y);
+    }
+  } else if constexpr (R == 2) {
     const float2 a = v[0], b = v[1];
     v[0] = make_float2(a.x + b.x, a.y + b.y);
     v[1] = make_float2(a.x - b.x, a.y - b.y);
@@ -696,14 +763,14 @@ __host__ __device__ constexpr int fft_lines_per_block(int n) { return n >= 128 ?
 
 template <int N, int R, int NS, bool INV>
 __device__ __forceinline__ void fft_stage_t(const float2* x, float2* y, const float2* tw, int nl) {
-  constexpr int NB = N / R, STEP = N / (NS * R), LD = N + 1;
+  constexpr int NB = N / R, STEP = N / (NS * R), LD = fft_ld(N);
   for (int idx = threadIdx.x; idx < nl * NB; idx += kFftThreads) {
     const int l = idx / NB, j = idx - l * NB;
     const int k = j % NS;
     const float2* xl = x + l * LD;
     float2 v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = xl[j + r * NB];
+    for (int r = 0; r < R; ++r) v[r] = xl[sk(j + r * NB)];
     if constexpr (NS > 1) {
 #pragma unroll
       for (int r = 1; r < R; ++r) {
@@ -716,7 +783,7 @@ __device__ __forceinline__ void fft_stage_t(const float2* x, float2* y, const fl
     float2* yl = y + l * LD;
     const int o = (j / NS) * NS * R + k;
 #pragma unroll
-    for (int r = 0; r < R; ++r) yl[o + r * NS] = v[r];
+    for (int r = 0; r < R; ++r) yl[sk(o + r * NS)] = v[r];
   }
 }
 
@@ -739,7 +806,7 @@ template <int N>
 __global__ void __launch_bounds__(256) k_fft_x_r2c_t(PmeArgs a, int) { griddep_wait();
   constexpr int nl = fft_lines_per_block(N);  // complex lines = row pairs per block
   extern __shared__ float2 sm[];
-  constexpr int LD = N + 1, NH = N / 2 + 1;
+  constexpr int LD = fft_ld(N), NH = N / 2 + 1;
   const int nrows = a.K[1] * a.K[2];
   float2* tw = sm;
   float2* A = sm + N;
@@ -749,7 +816,7 @@ __global__ void __launch_bounds__(256) k_fft_x_r2c_t(PmeArgs a, int) { griddep_w
   for (int idx = threadIdx.x; idx < nl * N; idx += kFftThreads) {
     const int l = idx / N, x = idx - l * N;
     const int row = r0 + 2 * l;
-    A[l * LD + x] = make_float2(row < nrows ? charge_at(a, (size_t)row * N + x) : 0.f,
+    A[l * LD + sk(x)] = make_float2(row < nrows ? charge_at(a, (size_t)row * N + x) : 0.f,
                                 row + 1 < nrows ? charge_at(a, (size_t)(row + 1) * N + x) : 0.f);
   }
   __syncthreads();
@@ -757,7 +824,7 @@ __global__ void __launch_bounds__(256) k_fft_x_r2c_t(PmeArgs a, int) { griddep_w
   for (int idx = threadIdx.x; idx < nl * NH; idx += kFftThreads) {
     const int l = idx / NH, m = idx - l * NH;
     const int row = r0 + 2 * l;
-    const float2 z = R[l * LD + m], w = R[l * LD + (m == 0 ? 0 : N - m)];  // w = Z(N-m)
+    const float2 z = R[l * LD + sk(m)], w = R[l * LD + sk(m == 0 ? 0 : N - m)];  // w = Z(N-m)
     if (row < nrows) a.cgrid[(size_t)row * NH + m] = make_float2(0.5f * (z.x + w.x), 0.5f * (z.y - w.y));
     if (row + 1 < nrows) a.cgrid[(size_t)(row + 1) * NH + m] = make_float2(0.5f * (z.y + w.y), 0.5f * (w.x - z.x));
   }
@@ -767,7 +834,7 @@ template <int N, bool INV>
 __global__ void __launch_bounds__(256) k_fft_y_t(PmeArgs a, int) { griddep_wait();
   constexpr int nl = fft_lines_per_block(N);
   extern __shared__ float2 sm[];
-  constexpr int LD = N + 1;
+  constexpr int LD = fft_ld(N);
   const int Kxh = a.K[0] / 2 + 1;
   const int ng = (Kxh + nl - 1) / nl;
   const int z = blockIdx.x / ng, mx0 = (blockIdx.x % ng) * nl;
@@ -778,14 +845,14 @@ __global__ void __launch_bounds__(256) k_fft_y_t(PmeArgs a, int) { griddep_wait(
   for (int idx = threadIdx.x; idx < nl * N; idx += kFftThreads) {
     const int y = idx / nl, l = idx - y * nl;
     const int mx = mx0 + l;
-    A[l * LD + y] = mx < Kxh ? a.cgrid[((size_t)z * N + y) * Kxh + mx] : make_float2(0.f, 0.f);
+    A[l * LD + sk(y)] = mx < Kxh ? a.cgrid[((size_t)z * N + y) * Kxh + mx] : make_float2(0.f, 0.f);
   }
   __syncthreads();
   const float2* R = fft_run_t<N, 0, 1, INV>(A, B, tw, nl);
   for (int idx = threadIdx.x; idx < nl * N; idx += kFftThreads) {
     const int y = idx / nl, l = idx - y * nl;
     const int mx = mx0 + l;
-    if (mx < Kxh) a.cgrid[((size_t)z * N + y) * Kxh + mx] = R[l * LD + y];
+    if (mx < Kxh) a.cgrid[((size_t)z * N + y) * Kxh + mx] = R[l * LD + sk(y)];
   }
 }
 
@@ -794,7 +861,7 @@ __device__ __forceinline__ void fft_z_conv_body(const PmeArgs& a, int bid) {
   griddep_wait();
   constexpr int nl = fft_lines_per_block(N);
   extern __shared__ float2 sm[];
-  constexpr int LD = N + 1;
+  constexpr int LD = fft_ld(N);
   const int Kx = a.K[0], Ky = a.K[1], Kxh = Kx / 2 + 1;
   const int ng = (Kxh + nl - 1) / nl;
   const int y = bid / ng, mx0 = (bid % ng) * nl;
@@ -805,7 +872,7 @@ __device__ __forceinline__ void fft_z_conv_body(const PmeArgs& a, int bid) {
   for (int idx = threadIdx.x; idx < nl * N; idx += kFftThreads) {
     const int z = idx / nl, l = idx - z * nl;
     const int mx = mx0 + l;
-    A[l * LD + z] = mx < Kxh ? a.cgrid[((size_t)z * Ky + y) * Kxh + mx] : make_float2(0.f, 0.f);
+    A[l * LD + sk(z)] = mx < Kxh ? a.cgrid[((size_t)z * Ky + y) * Kxh + mx] : make_float2(0.f, 0.f);
   }
   __syncthreads();
   float2* R = fft_run_t<N, 0, 1, false>(A, B, tw, nl);
@@ -815,7 +882,7 @@ __device__ __forceinline__ void fft_z_conv_body(const PmeArgs& a, int bid) {
   for (int idx = threadIdx.x; idx < nl * N; idx += kFftThreads) {
     const int l = idx / N, z = idx - l * N;
     const int mx = mx0 + l;
-    float2 v = R[l * LD + z];
+    float2 v = R[l * LD + sk(z)];
     float G = 0.f;
     if (mx < Kxh && (mx | y | z) != 0) G = a.gscale * a.gfac[0][mx] * gy * a.gfac[2][z] / (a.f2[0][mx] + fy2 + a.f2[2][z]);
     if (ENERGY && mx < Kxh && G != 0.f) {
@@ -832,14 +899,14 @@ __device__ __forceinline__ void fft_z_conv_body(const PmeArgs& a, int bid) {
     }
     v.x *= G;
     v.y *= G;
-    R[l * LD + z] = v;
+    R[l * LD + sk(z)] = v;
   }
   __syncthreads();
   const float2* Q = fft_run_t<N, 0, 1, true>(R, O, tw, nl);
   for (int idx = threadIdx.x; idx < nl * N; idx += kFftThreads) {
     const int z = idx / nl, l = idx - z * nl;
     const int mx = mx0 + l;
-    if (mx < Kxh) a.cgrid[((size_t)z * Ky + y) * Kxh + mx] = Q[l * LD + z];
+    if (mx < Kxh) a.cgrid[((size_t)z * Ky + y) * Kxh + mx] = Q[l * LD + sk(z)];
   }
   if (ENERGY) {
     energy_add(a.energy + EN_PME, e);
@@ -865,7 +932,7 @@ template <int N>
 __global__ void __launch_bounds__(256) k_fft_x_c2r_t(PmeArgs a, int) { griddep_wait();
   constexpr int nl = fft_lines_per_block(N);
   extern __shared__ float2 sm[];
-  constexpr int LD = N + 1, NH = N / 2 + 1;
+  constexpr int LD = fft_ld(N), NH = N / 2 + 1;
   const int nrows = a.K[1] * a.K[2];
   float2* tw = sm;
   float2* A = sm + N;
@@ -884,14 +951,14 @@ __global__ void __launch_bounds__(256) k_fft_x_c2r_t(PmeArgs a, int) { griddep_w
       x0.y = -x0.y;
       x1.y = -x1.y;
     }
-    A[l * LD + m] = make_float2(x0.x - x1.y, x0.y + x1.x);
+    A[l * LD + sk(m)] = make_float2(x0.x - x1.y, x0.y + x1.x);
   }
   __syncthreads();
   const float2* R = fft_run_t<N, 0, 1, true>(A, B, tw, nl);
   for (int idx = threadIdx.x; idx < nl * N; idx += kFftThreads) {
     const int l = idx / N, x = idx - l * N;
     const int row = r0 + 2 * l;
-    const float2 v = R[l * LD + x];
+    const float2 v = R[l * LD + sk(x)];
     if (row < nrows) a.grid[(size_t)row * N + x] = v.x;
     if (row + 1 < nrows) a.grid[(size_t)(row + 1) * N + x] = v.y;
   }
@@ -922,7 +989,7 @@ __device__ __forceinline__ void fft_stage_g(const float2* x, float2* y, const fl
     const float2* xl = x + l * LS;
     float2 v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = xl[(j + r * NB) * ES];
+    for (int r = 0; r < R; ++r) v[r] = xl[ES == 1 ? sk(j + r * NB) : (j + r * NB) * ES];
     if constexpr (NS > 1) {
 #pragma unroll
       for (int r = 1; r < R; ++r) {
@@ -935,7 +1002,7 @@ __device__ __forceinline__ void fft_stage_g(const float2* x, float2* y, const fl
     float2* yl = y + l * LS;
     const int o = (j / NS) * NS * R + k;
 #pragma unroll
-    for (int r = 0; r < R; ++r) yl[(o + r * NS) * ES] = v[r];
+    for (int r = 0; r < R; ++r) yl[ES == 1 ? sk(o + r * NS) : (o + r * NS) * ES] = v[r];
   }
 }
 
@@ -954,7 +1021,7 @@ __device__ __forceinline__ float2* fft_run_g(float2* a, float2* b, const float2*
 // rows pair up as (2l, 2l+1); an odd N leaves the last line with one row and a zero
 template <int N>
 __host__ __device__ constexpr int plane_words() {
-  constexpr int NH = N / 2 + 1, LD = N + 1, NP = (N + 1) / 2;
+  constexpr int NH = N / 2 + 1, LD = fft_ld(N), NP = (N + 1) / 2;
   return (N * NH > NP * LD) ? N * NH : NP * LD;
 }
 template <int N>
@@ -967,7 +1034,7 @@ template <int N>
 __device__ __forceinline__ void fft_xy_plane_body(const PmeArgs& a, int z) {
   griddep_wait();
   extern __shared__ float2 sm[];
-  constexpr int LD = N + 1, NH = N / 2 + 1, NP = (N + 1) / 2, W = plane_words<N>();
+  constexpr int LD = fft_ld(N), NH = N / 2 + 1, NP = (N + 1) / 2, W = plane_words<N>();
   float2* tw = sm;
   float2* A = sm + N;
   float2* B = A + W;
@@ -975,7 +1042,7 @@ __device__ __forceinline__ void fft_xy_plane_body(const PmeArgs& a, int z) {
   const size_t row0 = (size_t)z * N;
   for (int idx = threadIdx.x; idx < NP * N; idx += kPlaneThreads) {
     const int l = idx / N, x = idx - l * N;
-    A[l * LD + x] = make_float2(charge_at(a, (row0 + 2 * l) * N + x),
+    A[l * LD + sk(x)] = make_float2(charge_at(a, (row0 + 2 * l) * N + x),
                                 2 * l + 1 < N ? charge_at(a, (row0 + 2 * l + 1) * N + x) : 0.f);
   }
   __syncthreads();
@@ -983,7 +1050,7 @@ __device__ __forceinline__ void fft_xy_plane_body(const PmeArgs& a, int z) {
   float2* P = (R == A) ? B : A;  // plane [y][mx], row length NH
   for (int idx = threadIdx.x; idx < NP * NH; idx += kPlaneThreads) {
     const int l = idx / NH, m = idx - l * NH;
-    const float2 u = R[l * LD + m], w = R[l * LD + (m == 0 ? 0 : N - m)];
+    const float2 u = R[l * LD + sk(m)], w = R[l * LD + sk(m == 0 ? 0 : N - m)];
     P[(2 * l) * NH + m] = make_float2(0.5f * (u.x + w.x), 0.5f * (u.y - w.y));
     if (2 * l + 1 < N) P[(2 * l + 1) * NH + m] = make_float2(0.5f * (u.y + w.y), 0.5f * (w.x - u.x));
   }
@@ -999,7 +1066,7 @@ template <int N>
 __device__ __forceinline__ void fft_yx_plane_body(const PmeArgs& a, int z) {
   griddep_wait();
   extern __shared__ float2 sm[];
-  constexpr int LD = N + 1, NH = N / 2 + 1, NP = (N + 1) / 2, W = plane_words<N>();
+  constexpr int LD = fft_ld(N), NH = N / 2 + 1, NP = (N + 1) / 2, W = plane_words<N>();
   float2* tw = sm;
   float2* A = sm + N;
   float2* B = A + W;
@@ -1019,13 +1086,13 @@ __device__ __forceinline__ void fft_yx_plane_body(const PmeArgs& a, int z) {
       x0.y = -x0.y;
       x1.y = -x1.y;
     }
-    L[l * LD + m] = make_float2(x0.x - x1.y, x0.y + x1.x);
+    L[l * LD + sk(m)] = make_float2(x0.x - x1.y, x0.y + x1.x);
   }
   __syncthreads();
   const float2* R = fft_run_g<N, 0, 1, true, 1, LD, NP>(L, Q, tw);
   for (int idx = threadIdx.x; idx < NP * N; idx += kPlaneThreads) {
     const int l = idx / N, x = idx - l * N;
-    const float2 v = R[l * LD + x];
+    const float2 v = R[l * LD + sk(x)];
     a.grid[(row0 + 2 * l) * N + x] = v.x;
     if (2 * l + 1 < N) a.grid[(row0 + 2 * l + 1) * N + x] = v.y;
   }
@@ -1186,9 +1253,13 @@ void launch_pme(const PmeArgs& a_in, bool energy, cudaStream_t st) {
   const FftPlan px = make_plan(Kx), py = make_plan(Ky), pz = make_plan(Kz);
   const int lx = lines_for(Kx), ly = lines_for(Ky), lz = lines_for(Kz);
   const int rows = Ky * Kz;
+  // runtime-plan kernels: lines n + 1 apart; compile-time kernels: fft_ld(n) apart
   const size_t smx = (size_t)(Kx + 2 * lx * (Kx + 1)) * sizeof(float2);
   const size_t smy = (size_t)(Ky + 2 * ly * (Ky + 1)) * sizeof(float2);
   const size_t smz = (size_t)(Kz + 2 * lz * (Kz + 1)) * sizeof(float2);
+  const size_t smx_t = (size_t)(Kx + 2 * lx * fft_ld(Kx)) * sizeof(float2);
+  const size_t smy_t = (size_t)(Ky + 2 * ly * fft_ld(Ky)) * sizeof(float2);
+  const size_t smz_t = (size_t)(Kz + 2 * lz * fft_ld(Kz)) * sizeof(float2);
   const dim3 gx((rows + lx - 1) / lx), gy(Kz * ((Kxh + ly - 1) / ly)), gz(Ky * ((Kxh + lz - 1) / lz));
   // compile-time-sized kernels where available, runtime plans otherwise
   const dim3 gx2((rows + 2 * lx - 1) / (2 * lx));  // compile-time x kernels: row pairs
@@ -1196,10 +1267,10 @@ void launch_pme(const PmeArgs& a_in, bool energy, cudaStream_t st) {
   if (plane) {
     fft_plane(a, false, st);
   } else {
-    if (!fft_x_r2c_t(a, lx, gx2, smx, st)) launch_pdl(k_fft_x_r2c, dim3(gx), dim3(256), smx, st, a, px, lx);
-    if (!fft_y_t(a, ly, false, gy, smy, st)) launch_pdl(k_fft_y, dim3(gy), dim3(256), smy, st, a, py, ly, 0);
+    if (!fft_x_r2c_t(a, lx, gx2, smx_t, st)) launch_pdl(k_fft_x_r2c, dim3(gx), dim3(256), smx, st, a, px, lx);
+    if (!fft_y_t(a, ly, false, gy, smy_t, st)) launch_pdl(k_fft_y, dim3(gy), dim3(256), smy, st, a, py, ly, 0);
   }
-  if (!fft_z_t(a, lz, energy, gz, smz, st)) {
+  if (!fft_z_t(a, lz, energy, gz, smz_t, st)) {
     if (energy)
       launch_pdl(k_fft_z_conv<true>, dim3(gz), dim3(256), smz, st, a, pz, lz);
     else
@@ -1208,8 +1279,8 @@ void launch_pme(const PmeArgs& a_in, bool energy, cudaStream_t st) {
   if (plane) {
     fft_plane(a, true, st);
   } else {
-    if (!fft_y_t(a, ly, true, gy, smy, st)) launch_pdl(k_fft_y, dim3(gy), dim3(256), smy, st, a, py, ly, 1);
-    if (!fft_x_c2r_t(a, lx, gx2, smx, st)) launch_pdl(k_fft_x_c2r, dim3(gx), dim3(256), smx, st, a, px, lx);
+    if (!fft_y_t(a, ly, true, gy, smy_t, st)) launch_pdl(k_fft_y, dim3(gy), dim3(256), smy, st, a, py, ly, 1);
+    if (!fft_x_c2r_t(a, lx, gx2, smx_t, st)) launch_pdl(k_fft_x_c2r, dim3(gx), dim3(256), smx, st, a, px, lx);
   }
   const int gmode = a.gather;
   if (gmode == 1 || (gmode == 0 && (size_t)a.n <= (size_t)kGatherBrickAtoms * nbr))
@@ -1259,7 +1330,7 @@ void launch_pme_b(const PmeArgs* args, const BatchTables& t, const PmeSizeBatch*
     }();                                                                                               \
     (void)attr;                                                                                        \
     constexpr int nl = fft_lines_per_block(N);                                                         \
-    constexpr size_t smz = (size_t)(N + 2 * nl * (N + 1)) * sizeof(float2);                           \
+    constexpr size_t smz = (size_t)(N + 2 * nl * fft_ld(N)) * sizeof(float2);                         \
     if (pass == 0) launch_pdl(k_fft_xy_plane_b<N>, dim3(b.nplane), dim3(kPlaneThreads), sm, st, args, b.plane_tab);       \
     if (pass == 1) launch_pdl(k_fft_z_conv_b<N>, dim3(b.nz), dim3(256), smz, st, args, b.z_tab);                           \
     if (pass == 2) launch_pdl(k_fft_yx_plane_b<N>, dim3(b.nplane), dim3(kPlaneThreads), sm, st, args, b.plane_tab);       \
