@@ -226,6 +226,7 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
     const char* v = std::getenv("FZ_GRAPH_COND");
     e->cond_graph = v && std::atoi(v) == 1;
     if (const char* c = std::getenv("FZ_GRAPH_CHUNK")) e->chunk_steps = std::max(0, std::min(1000, std::atoi(c)));
+    if (const char* c = std::getenv("FZ_FUSE_CLOSE")) e->fuse_close = std::atoi(c) != 0;
   }
   FZ_CUDA(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
   FZ_CUDA(cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming));

@@ -108,6 +108,9 @@ struct Engine {
   cudaGraph_t chunk_graph = nullptr;
   cudaGraphExec_t chunk_exec = nullptr;
   int chunk_steps = 100;
+  // chunk graphs fuse each step's closing kick + RATTLE into the next step's opening
+  // kick + drift pass (FZ_FUSE_CLOSE=0 keeps the two passes apart)
+  bool fuse_close = true;
   // prune with one CTA per i-block (systems with few blocks; identical lists)
   int prune_split = 0;
   bool use_graph = true;
@@ -539,16 +542,23 @@ struct Engine {
     cudaEventRecord(ev_join, st2);
     cudaStreamWaitEvent(st, ev_join, 0);
   }
-  void step_body() {
+  // One MD step.  open: the step starts with its own kick + drift pass (else the
+  // previous step left its closing kick + RATTLE to this step's first pass); close: the
+  // step ends with the kick + RATTLE pass (else the next step's first pass does it).
+  void step_body(bool open = true, bool close = true) {
     const fzk::IntegrateArgs ia = int_args();
-    integrate_classes(ia, [](const fzk::IntegrateArgs& a, cudaStream_t s) { fzk::launch_kick_drift(a, s); });
+    if (open)
+      integrate_classes(ia, [](const fzk::IntegrateArgs& a, cudaStream_t s) { fzk::launch_kick_drift(a, s); });
+    else
+      integrate_classes(ia, [](const fzk::IntegrateArgs& a, cudaStream_t s) { fzk::launch_close_kick_drift(a, s); });
     if (st2)
       forces_overlapped();
     else
       forces(false);
-    integrate_classes(ia, [](const fzk::IntegrateArgs& a, cudaStream_t s) {
-      fzk::launch_kick_rattle(a, false, true, s);
-    });
+    if (close)
+      integrate_classes(ia, [](const fzk::IntegrateArgs& a, cudaStream_t s) {
+        fzk::launch_kick_rattle(a, false, true, s);
+      });
   }
   fz_status graph_step() {
     if (!step_exec) {
@@ -575,7 +585,8 @@ struct Engine {
       capture_error = cudaSuccess;
       FZ_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
       const long long l0 = launches;
-      for (int k = 0; k < chunk_steps; ++k) step_body();
+      // inside the chunk each step's closing pass joins the next step's opening one
+      for (int k = 0; k < chunk_steps; ++k) step_body(k == 0 || !fuse_close, k == chunk_steps - 1 || !fuse_close);
       launches = l0;
       cudaGraph_t g = nullptr;
       FZ_CUDA(cudaStreamEndCapture(st, &g));
@@ -585,7 +596,7 @@ struct Engine {
       FZ_CUDA(cudaGraphInstantiate(&chunk_exec, chunk_graph, 0));
     }
     FZ_CUDA(cudaGraphLaunch(chunk_exec, st));
-    launches += (long long)chunk_steps * graph_step_launches();
+    launches += (long long)chunk_steps * graph_step_launches() - (fuse_close ? (long long)(chunk_steps - 1) * ncls : 0);
     graph_since_check = true;
     return FZ_OK;
   }

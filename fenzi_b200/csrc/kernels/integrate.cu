@@ -339,26 +339,49 @@ __device__ __forceinline__ void scale_com_velocity(const Unit& U, double v[4][3]
       for (int c = 0; c < 3; ++c) v[k][c] += (f - 1.0) * p[c] / mt;
 }
 
+// v += (dt/2) F / m, one rounding per component (the same in every pass that kicks)
+__device__ __forceinline__ void half_kick(double* v, double3 F, double im, const IntegrateArgs& a) {
+  const double h = 0.5 * a.dtu * im;
+  v[0] = fma(h, F.x, v[0]);
+  v[1] = fma(h, F.y, v[1]);
+  v[2] = fma(h, F.z, v[2]);
+}
+
+// brings a line into L1 ahead of a load that comes after stores the compiler cannot
+// move it past (pointers that may alias), so that load does not wait on DRAM
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
 // NPT (Andersen barostat step with the integration units as scaling groups): the unit
 // moves rigidly with its mass centre scaled by a.lam about the origin (the box changed
 // by a.lam), and its centre-of-mass velocity is scaled by a.vfric before the kick.
-template <bool NPT, int NA, int NC, bool SETTLE>
+// CLOSE (not with NPT): the unit first finishes the previous step as the kick + RATTLE
+// pass does (half kick with the same forces, velocity constraints, velocities rounded
+// to the stored float), so one pass replaces the previous step's closing launch and
+// this step's opening one with bit-identical results.
+template <bool NPT, int NA, int NC, bool SETTLE, bool CLOSE = false>
 __device__ __forceinline__ void kick_drift_body(const IntegrateArgs& a, int bid) {
+  static_assert(!(NPT && CLOSE), "the closing pass is for constant-volume steps");
   griddep_wait();
   const int u = a.u_begin + bid * blockDim.x + threadIdx.x;
   if (u >= a.u_end) return;
   const Unit U = load_unit<NA, NC>(a, u);
   const int n = a.p.n;
   double r0[4][3], rn[4][3], v[4][3], im[4];
+  double3 F[4];
   float q[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     im[k] = 0.0;
     q[k] = 0.f;
+    F[k] = make_double3(0.0, 0.0, 0.0);
     for (int c = 0; c < 3; ++c) r0[k][c] = rn[k][c] = v[k][c] = 0.0;
     if (k < U.na) {
       const int i = U.atom[k];
       const float4 pr = a.pos4[i], vl = a.vel4[i];
+      F[k] = force_of(a.facc, n, i);
+      prefetch_l1(a.pos_build + i);
+      prefetch_l1(a.pos_prune + i);
+      prefetch_l1(a.inv_perm + i);
       im[k] = vl.w;
       q[k] = pr.w;
       v[k][0] = vl.x;
@@ -369,19 +392,25 @@ __device__ __forceinline__ void kick_drift_body(const IntegrateArgs& a, int bid)
       r0[k][2] = pr.z;
     }
   }
+  if (CLOSE) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (k < U.na) half_kick(v[k], F[k], im[k], a);
+    if (U.nc > 0) rattle_unit(U, r0, v, im, a);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) v[k][c] = (double)(float)v[k][c];
+  }
   if (NPT) scale_com_velocity(U, v, im, a.vfric);
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     if (k >= U.na) continue;
     const int i = U.atom[k];
-    const double3 Fk = force_of(a.facc, n, i);
     a.facc[i] = 0;
     a.facc[n + i] = 0;
     a.facc[2 * n + i] = 0;
-    const double h = 0.5 * a.dtu * im[k];
-    v[k][0] += h * Fk.x;
-    v[k][1] += h * Fk.y;
-    v[k][2] += h * Fk.z;
+    half_kick(v[k], F[k], im[k], a);
   }
   if (NPT) {
     // Each atom moves by (lam - 1) x the unit's mass centre taken in the atom's own
@@ -451,6 +480,12 @@ __device__ __forceinline__ void kick_drift_body(const IntegrateArgs& a, int bid)
 
 template <bool NPT, int NA, int NC, bool SETTLE = false>
 __global__ void __launch_bounds__(128) k_kick_drift(IntegrateArgs a) { griddep_wait(); kick_drift_body<NPT, NA, NC, SETTLE>(a, blockIdx.x); }
+
+template <int NA, int NC, bool SETTLE>
+__global__ void __launch_bounds__(128, SETTLE ? 4 : 1) k_close_kick_drift(IntegrateArgs a) {
+  griddep_wait();
+  kick_drift_body<false, NA, NC, SETTLE, true>(a, blockIdx.x);
+}
 
 template <int NA, int NC, bool SETTLE>
 __global__ void __launch_bounds__(128) k_kick_drift_b(const IntegrateArgs* __restrict__ args, const int4* __restrict__ tab) { griddep_wait();
@@ -531,13 +566,7 @@ __device__ __forceinline__ void kick_rattle_body(const IntegrateArgs& a, int kic
       v[k][0] = vl.x;
       v[k][1] = vl.y;
       v[k][2] = vl.z;
-      if (kick) {
-        const double3 F = force_of(a.facc, n, i);
-        const double h = 0.5 * a.dtu * im[k];
-        v[k][0] += h * F.x;
-        v[k][1] += h * F.y;
-        v[k][2] += h * F.z;
-      }
+      if (kick) half_kick(v[k], force_of(a.facc, n, i), im[k], a);
       r[k][0] = pr.x;
       r[k][1] = pr.y;
       r[k][2] = pr.z;
@@ -833,6 +862,19 @@ static void kick_drift_classes(const IntegrateArgs& a, cudaStream_t st) {
 }
 
 void launch_kick_drift(const IntegrateArgs& a, cudaStream_t st) { kick_drift_classes<false>(a, st); }
+
+void launch_close_kick_drift(const IntegrateArgs& a, cudaStream_t st) {
+  for_classes(a, [&](const IntegrateArgs& x, auto na, auto nc) {
+    constexpr int NA = decltype(na)::value, NC = decltype(nc)::value;
+    if constexpr (NA == 3 && NC == 3) {
+      if (x.settle) {
+        launch_pdl(k_close_kick_drift<3, 3, true>, dim3(unit_grid(x)), dim3(128), 0, st, x);
+        return;
+      }
+    }
+    launch_pdl(k_close_kick_drift<NA, NC, false>, dim3(unit_grid(x)), dim3(128), 0, st, x);
+  });
+}
 
 // batched: one launch per unit class over every system's units of that class
 template <class F>

@@ -211,6 +211,9 @@ struct ClassBatch {
 void launch_kick_drift_b(const ClassBatch& c, cudaStream_t st);
 void launch_kick_rattle_b(const ClassBatch& c, cudaStream_t st);
 void launch_kick_drift(const IntegrateArgs& a, cudaStream_t st);
+// the previous step's closing kick + RATTLE and this step's kick + drift + SHAKE in one
+// pass (constant volume; bit-identical to launch_kick_rattle then launch_kick_drift)
+void launch_close_kick_drift(const IntegrateArgs& a, cudaStream_t st);
 // the same for a barostat step (rigid unit scaling by lam, centre-of-mass velocity
 // scale vfric)
 void launch_kick_drift_npt(const IntegrateArgs& a, cudaStream_t st);
