@@ -211,19 +211,28 @@ __device__ __forceinline__ void pme_spread_body(const PmeArgs& a, int bid, int n
   // the brick more than 3 below its upper faces (region index 3 .. B-1 on every axis)
   // lies in no other brick's region, so it takes a plain store; the rest are shared
   // with the neighbouring bricks' halos and take atomic adds.
+  // Each thread keeps one (x, y) column of the region and walks it along z (the two
+  // halves of the block take alternate z), so the column's grid address and ownership
+  // are worked out once instead of dividing every region index by the extents.
   int* g = reinterpret_cast<int*>(a.grid);
-  for (int k = threadIdx.x; k < vol; k += blockDim.x) {
-    const int v = acc[k];
-    if (v == 0) continue;
-    const int rx = k % Ex, ry = (k / Ex) % Ey, rz = k / (Ex * Ey);
-    const bool own = rx >= 3 && rx < Bx && ry >= 3 && ry < By && rz >= 3 && rz < Bz;
-    int gx = ox + rx, gy = oy + ry, gz = oz + rz;
+  const int plane = Ex * Ey, half = blockDim.x >> 1;
+  const size_t zstride = (size_t)Ky * Kx;
+  for (int t = threadIdx.x % half; t < plane; t += half) {
+    const int ry = t / Ex, rx = t - ry * Ex;
+    int gx = ox + rx, gy = oy + ry;
     gx += gx < 0 ? Kx : 0;
     gy += gy < 0 ? Ky : 0;
-    gz += gz < 0 ? Kz : 0;
-    int* dst = g + ((size_t)gz * Ky + gy) * Kx + gx;
-    if (own) *dst = v;
-    else atomicAdd(dst, v);
+    const bool own_xy = rx >= 3 && rx < Bx && ry >= 3 && ry < By;
+    int* col = g + (size_t)gy * Kx + gx;
+    for (int rz = threadIdx.x / half; rz < Ez; rz += 2) {
+      const int v = acc[rz * plane + t];
+      if (v == 0) continue;
+      int gz = oz + rz;
+      gz += gz < 0 ? Kz : 0;
+      int* dst = col + (size_t)gz * zstride;
+      if (own_xy && rz >= 3 && rz < Bz) *dst = v;
+      else atomicAdd(dst, v);
+    }
   }
 }
 
@@ -569,14 +578,20 @@ __device__ __forceinline__ void pme_gather_body(const PmeArgs& a, int bid, int n
   const int bx = b % nbx, by = (b / nbx) % nby, bz = b / (nbx * nby);
   const int Kx = a.K[0], Ky = a.K[1], Kz = a.K[2];
   const int ox = bx * Bx - 3, oy = by * By - 3, oz = bz * Bz - 3;
-  const int vol = Ex * Ey * Ez;
-  for (int k = threadIdx.x; k < vol; k += blockDim.x) {
-    const int rx = k % Ex, ry = (k / Ex) % Ey, rz = k / (Ex * Ey);
-    int gx = ox + rx, gy = oy + ry, gz = oz + rz;
+  // region load by (x, y) columns walked along z, as the spread's flush
+  const int plane = Ex * Ey, half = blockDim.x >> 1;
+  const size_t zstride = (size_t)Ky * Kx;
+  for (int t = threadIdx.x % half; t < plane; t += half) {
+    const int ry = t / Ex, rx = t - ry * Ex;
+    int gx = ox + rx, gy = oy + ry;
     gx += gx < 0 ? Kx : 0;
     gy += gy < 0 ? Ky : 0;
-    gz += gz < 0 ? Kz : 0;
-    phi_reg[k] = __ldg(a.grid + ((size_t)gz * Ky + gy) * Kx + gx);
+    const float* col = a.grid + (size_t)gy * Kx + gx;
+    for (int rz = threadIdx.x / half; rz < Ez; rz += 2) {
+      int gz = oz + rz;
+      gz += gz < 0 ? Kz : 0;
+      phi_reg[rz * plane + t] = __ldg(col + (size_t)gz * zstride);
+    }
   }
   __syncthreads();
   const int n = a.n;
