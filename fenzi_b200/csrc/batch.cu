@@ -321,10 +321,15 @@ static fz_status build_batch_kernels(fz_batch* b) {
 }
 
 // the batched step: kick/drift (one launch per unit class), outer-list rebuild, then PME
-// on a second stream beside prune, pair and bonded kernels, then kick/RATTLE
-static void batched_step_body(fz_batch* b, cudaStream_t st) {
+// on a second stream beside prune, pair and bonded kernels, then kick/RATTLE.  open /
+// close as for the single-system step: inside a chunk graph the kick/RATTLE of a step
+// and the kick/drift of the next are one pass.
+static void batched_step_body(fz_batch* b, cudaStream_t st, bool open = true, bool close = true) {
   BatchKernels& k = *b->bk;
-  for (const auto& c : k.classes) fzk::launch_kick_drift_b(c, st);
+  for (const auto& c : k.classes) {
+    if (open) fzk::launch_kick_drift_b(c, st);
+    else fzk::launch_close_kick_drift_b(c, st);
+  }
   fzk::launch_rebuild_build_b(k.rb, k.t, st);
   cudaEventRecord(b->ev_fork, st);
   cudaStreamWaitEvent(b->aux, b->ev_fork, 0);
@@ -334,7 +339,8 @@ static void batched_step_body(fz_batch* b, cudaStream_t st) {
   fzk::launch_bonded_b(k.bd, k.t, st);
   cudaEventRecord(b->ev_join, b->aux);
   cudaStreamWaitEvent(st, b->ev_join, 0);
-  for (const auto& c : k.classes) fzk::launch_kick_rattle_b(c, st);
+  if (close)
+    for (const auto& c : k.classes) fzk::launch_kick_rattle_b(c, st);
 }
 
 static fz_status capture(fz_batch* b) {
@@ -367,7 +373,8 @@ static fz_status capture(fz_batch* b) {
       if (b->chunk > 0) b->chunk = std::max(0, std::min(1000, std::atoi(c)));
     if (b->chunk > 1) {
       FZ_CUDA(cudaStreamBeginCapture(b->master, cudaStreamCaptureModeThreadLocal));
-      for (int k = 0; k < b->chunk; ++k) batched_step_body(b, b->master);
+      const bool fuse = !std::getenv("FZ_FUSE_CLOSE") || std::atoi(std::getenv("FZ_FUSE_CLOSE")) != 0;
+      for (int k = 0; k < b->chunk; ++k) batched_step_body(b, b->master, k == 0 || !fuse, k == b->chunk - 1 || !fuse);
       FZ_CUDA(cudaStreamEndCapture(b->master, &b->chunk_graph));
       FZ_CUDA(cudaGraphInstantiate(&b->chunk_exec, b->chunk_graph, 0));
     }

@@ -488,6 +488,15 @@ __global__ void __launch_bounds__(128, SETTLE ? 4 : 1) k_close_kick_drift(Integr
 }
 
 template <int NA, int NC, bool SETTLE>
+__global__ void __launch_bounds__(128, SETTLE ? 4 : 1) k_close_kick_drift_b(const IntegrateArgs* __restrict__ args,
+                                                                           const int4* __restrict__ tab) {
+  griddep_wait();
+  const int4 t = tab[blockIdx.x];
+  const IntegrateArgs a = args[t.x];
+  kick_drift_body<false, NA, NC, SETTLE, true>(a, t.y);
+}
+
+template <int NA, int NC, bool SETTLE>
 __global__ void __launch_bounds__(128) k_kick_drift_b(const IntegrateArgs* __restrict__ args, const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const IntegrateArgs a = args[t.x];
@@ -898,6 +907,20 @@ void launch_kick_drift_b(const ClassBatch& c, cudaStream_t st) {
       }
     }
     launch_pdl(k_kick_drift_b<NA, NC, false>, dim3(c.nblocks), dim3(128), 0, st, c.args, c.tab);
+  });
+}
+
+void launch_close_kick_drift_b(const ClassBatch& c, cudaStream_t st) {
+  if (c.nblocks <= 0) return;
+  class_dispatch(c.na, c.nc, [&](auto na, auto nc) {
+    constexpr int NA = decltype(na)::value, NC = decltype(nc)::value;
+    if constexpr (NA == 3 && NC == 3) {
+      if (c.settle) {
+        launch_pdl(k_close_kick_drift_b<3, 3, true>, dim3(c.nblocks), dim3(128), 0, st, c.args, c.tab);
+        return;
+      }
+    }
+    launch_pdl(k_close_kick_drift_b<NA, NC, false>, dim3(c.nblocks), dim3(128), 0, st, c.args, c.tab);
   });
 }
 

@@ -210,6 +210,7 @@ struct ClassBatch {
 };
 void launch_kick_drift_b(const ClassBatch& c, cudaStream_t st);
 void launch_kick_rattle_b(const ClassBatch& c, cudaStream_t st);
+void launch_close_kick_drift_b(const ClassBatch& c, cudaStream_t st);
 void launch_kick_drift(const IntegrateArgs& a, cudaStream_t st);
 // the previous step's closing kick + RATTLE and this step's kick + drift + SHAKE in one
 // pass (constant volume; bit-identical to launch_kick_rattle then launch_kick_drift)
