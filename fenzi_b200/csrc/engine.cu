@@ -614,16 +614,18 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
     if (const char* v = std::getenv("FZ_PRUNE_SPLIT"))
       e->prune_split = (std::atoi(v) != 0 && fzk::prune_split_fits(e->ocap)) ? 1 : 0;
   }
-  // tiles per pair-kernel work item: ~16 items per pair-kernel warp, 2 to 4 tiles,
-  // so the warps run out of work together (the last items are short); measured at
-  // 230,400 atoms (ms/step): 64 tiles 0.544, 16 0.532, 8 0.526, 4 0.526, 3 0.526, 2 0.539.
-  // This is the default; the autotuner below times the alternatives on the device.
+  // tiles per pair-kernel work item: ~8 items per pair-kernel warp, 3 to 6 tiles, so
+  // the warps run out of work together (the last items are short).  Measured (us per
+  // step, 1,000 steps): 230,400 atoms 426 (3 tiles), 423 (4), 422 (6), 424 (8); 17,280
+  // atoms 88.4 (2), 86.4 (3), 86.0 (4), 86.6 (6); 9,000 atoms 65.9 (2), 62.1 (3), 65.0
+  // (4), 73.9 (6).  The item size changes the order of the i-force sums, so it is a
+  // fixed rule, not a shape the autotuner times.
   {
     int cnt2[fzk::CNT_COUNT];
     FZ_CUDA(cudaMemcpyAsync(cnt2, e->counters, sizeof(cnt2), cudaMemcpyDeviceToHost, e->st));
     FZ_CUDA(cudaStreamSynchronize(e->st));
     e->tiles = cnt2[fzk::CNT_TILES];
-    int want = std::max(2, std::min(4, e->tiles / (e->n_sm * 4 * fzk::kWarpsPerCta * 16)));
+    int want = std::max(3, std::min(6, e->tiles / (e->n_sm * 4 * fzk::kWarpsPerCta * 8)));
     if (const char* v = std::getenv("FZ_CHUNK_TILES")) want = std::max(1, std::min(64, std::atoi(v)));
     if (want != e->chunk) {
       e->chunk = want;
