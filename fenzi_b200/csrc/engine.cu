@@ -254,8 +254,12 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
   const double V = c.box[0] * c.box[1] * c.box[2];
   const double rho = n / V;
   // column cross-section: a x a with a^3 holding `col_atoms` atoms (32: one sorted
-  // block is a near-cube; smaller values make narrower, taller blocks)
-  double col_atoms = 32.0;
+  // block is a near-cube; smaller values make narrower, taller blocks).  16: a block
+  // is two near-cubes stacked in z, so each 16-atom i-group is a compact cube and
+  // fewer pairs of its tiles fall outside the cutoff.  Measured (us per step, 1,000
+  // steps): 230,400 atoms 421 (32) / 413-418 (16); 17,280 atoms 85.9 / 83.7; 256
+  // boxes 1.655 / 1.608 ms.
+  double col_atoms = 16.0;
   if (const char* v = std::getenv("FZ_COL_ATOMS")) col_atoms = std::min(64.0, std::max(8.0, std::atof(v)));
   const double a = std::cbrt(col_atoms / rho);
   int ncx = std::max(1, (int)std::floor(c.box[0] / a)), ncy = std::max(1, (int)std::floor(c.box[1] / a));
@@ -297,9 +301,11 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
   }
   if (const char* v = std::getenv("FZ_PME_GATHER")) e->gather_mode = std::max(0, std::min(3, std::atoi(v)));
   // per-block list capacity: atoms within rlist of a block box (Minkowski volume of a
-  // box ~1.4 a), with room for blocks that see all their neighbours at higher index
-  const double ab = 1.4 * a, R = plist;
-  const double vm = ab * ab * ab + 6 * ab * ab * R + 3 * M_PI * ab * R * R + 4.0 / 3.0 * M_PI * R * R * R;
+  // box 1.4 a wide and 1.4 h tall, h the mean height of 32 atoms in a column), with
+  // room for blocks that see all their neighbours at higher index
+  const double ab = 1.4 * a, hb = 1.4 * 32.0 / (rho * a * a), R = plist;
+  const double vm = ab * ab * hb + 2 * R * (ab * ab + 2 * ab * hb) + M_PI * R * R * (2 * ab + hb) +
+                    4.0 / 3.0 * M_PI * R * R * R;
   e->ocap = (int)std::ceil(std::max(256.0, 1.25 * rho * vm) / 32.0) * 32;
   e->mask_cap = (e->nslots / 32) * fzk::kNG * (e->ocap / 32);
   {
