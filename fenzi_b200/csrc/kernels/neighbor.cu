@@ -465,6 +465,35 @@ __device__ __forceinline__ uint32_t excl_mask(int I, uint32_t je, int lane, uint
   return r;
 }
 
+// The prune's distance tests in packed form: the block's 32 i atoms are held in pairs
+// (2p, 2p + 1), A[p] = (ax, ax', ay, ay') and B[p] = (az, az', aw, aw') with
+// a = (-2 (q - o), |q - o|^2), so one f32x2 FMA chain tests an entry against two i
+// atoms at once.  Each test is the scalar fma(ax, rx, fma(ay, ry, fma(az, rz, aw))) in
+// the same order, and the minimum does not depend on the order taken, so the kept
+// entries are exactly those of one test per atom.
+__device__ __forceinline__ void prune_store_i(float4* iA, float4* iB, int lane, float ax, float ay, float az,
+                                              float aw) {
+  float* a = reinterpret_cast<float*>(iA) + (lane >> 1) * 4 + (lane & 1);
+  float* b = reinterpret_cast<float*>(iB) + (lane >> 1) * 4 + (lane & 1);
+  a[0] = ax;
+  a[2] = ay;
+  b[0] = az;
+  b[2] = aw;
+}
+__device__ __forceinline__ void prune_min2(const float4* iA, const float4* iB, float rx, float ry, float rz,
+                                           float* m2) {
+  const float2 x2 = make_float2(rx, rx), y2 = make_float2(ry, ry), z2 = make_float2(rz, rz);
+#pragma unroll
+  for (int p = 0; p < 16; ++p) {
+    const float4 A = iA[p], B = iB[p];
+    float2 d = __ffma2_rn(make_float2(B.x, B.y), z2, make_float2(B.z, B.w));
+    d = __ffma2_rn(make_float2(A.z, A.w), y2, d);
+    d = __ffma2_rn(make_float2(A.x, A.y), x2, d);
+    const int g = (2 * p) / kIG;
+    m2[g] = fminf(m2[g], fminf(d.x, d.y));
+  }
+}
+
 // Inner (pruned) pair list, warp per i-block: keeps the outer entries that lie within
 // rc + delta of at least one atom of the block at the current positions, packs them
 // into full 32-entry tiles with their exclusion masks, and records the positions the
@@ -496,14 +525,15 @@ __device__ __forceinline__ void prune_body(const RebuildArgs& A, int bid, int nb
   int* status = A.status;
 
   if (!*flag_prune) return;
-  __shared__ float4 ipos_all[8][32];
+  __shared__ float4 iA_all[8][16], iB_all[8][16];
   __shared__ uint32_t buf_all[8][kNG][64];
   __shared__ uint32_t msk_all[8][32];
   const int nblk = counters[CNT_SLOTS] >> 5;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int I = bid * 8 + warp;
   if (I >= nblk) return;
-  float4* ipos = ipos_all[warp];
+  float4* iA = iA_all[warp];
+  float4* iB = iB_all[warp];
   uint32_t* msk = msk_all[warp];
   const int islot = I * 32 + lane;
   const float4 pi = xyzq_s[islot];
@@ -515,7 +545,7 @@ __device__ __forceinline__ void prune_body(const RebuildArgs& A, int bid, int nb
   const float4 o = xyzq_s[I * 32];
   {
     const float qx = pi.x - o.x, qy = pi.y - o.y, qz = pi.z - o.z;
-    ipos[lane] = make_float4(-2.f * qx, -2.f * qy, -2.f * qz, fmaf(qx, qx, fmaf(qy, qy, qz * qz)));
+    prune_store_i(iA, iB, lane, -2.f * qx, -2.f * qy, -2.f * qz, fmaf(qx, qx, fmaf(qy, qy, qz * qz)));
   }
   // diagonal tile mask (exclusions inside the block)
   dmask[islot] = excl_mask(I, (uint32_t)islot, lane, msk, xn, xs, xmax);
@@ -579,11 +609,7 @@ __device__ __forceinline__ void prune_body(const RebuildArgs& A, int bid, int nb
     float m2[kNG];
 #pragma unroll
     for (int s = 0; s < kNG; ++s) m2[s] = 3e38f;
-#pragma unroll
-    for (int k = 0; k < 32; ++k) {
-      const float4 q = ipos[k];
-      m2[k / kIG] = fminf(m2[k / kIG], fmaf(q.x, r.x, fmaf(q.y, r.y, fmaf(q.z, r.z, q.w))));
-    }
+    prune_min2(iA, iB, r.x, r.y, r.z, m2);
 #pragma unroll
     for (int s = 0; s < kNG; ++s) {
       uint32_t* buf = buf_all[warp][s];
@@ -655,7 +681,7 @@ __device__ __forceinline__ void prune_split_body(const RebuildArgs& A, int I) {
   const int nblk = A.counters[CNT_SLOTS] >> 5;
   if (I >= nblk) return;
   extern __shared__ uint32_t kept[];  // [kNG][ocap]
-  __shared__ float4 ipos[32];
+  __shared__ float4 iA[16], iB[16];
   __shared__ uint32_t msk_all[kPruneWarps][32];
   __shared__ int cnt[kPruneWarps][kNG];
   __shared__ int off[kPruneWarps + 1][kNG];
@@ -669,7 +695,7 @@ __device__ __forceinline__ void prune_split_body(const RebuildArgs& A, int I) {
     const int ia = A.perm[islot];
     if (ia >= 0) A.pos_prune[ia] = pi;
     const float qx = pi.x - o.x, qy = pi.y - o.y, qz = pi.z - o.z;
-    ipos[lane] = make_float4(-2.f * qx, -2.f * qy, -2.f * qz, fmaf(qx, qx, fmaf(qy, qy, qz * qz)));
+    prune_store_i(iA, iB, lane, -2.f * qx, -2.f * qy, -2.f * qz, fmaf(qx, qx, fmaf(qy, qy, qz * qz)));
     A.dmask[islot] = excl_mask(I, (uint32_t)islot, lane, msk, A.xn, A.xs, A.xmax);
   }
   __syncthreads();
@@ -701,11 +727,7 @@ __device__ __forceinline__ void prune_split_body(const RebuildArgs& A, int I) {
     float m2[kNG];
 #pragma unroll
     for (int s = 0; s < kNG; ++s) m2[s] = 3e38f;
-#pragma unroll
-    for (int k = 0; k < 32; ++k) {
-      const float4 q = ipos[k];
-      m2[k / kIG] = fminf(m2[k / kIG], fmaf(q.x, r.x, fmaf(q.y, r.y, fmaf(q.z, r.z, q.w))));
-    }
+    prune_min2(iA, iB, r.x, r.y, r.z, m2);
 #pragma unroll
     for (int s = 0; s < kNG; ++s) {
       const bool keep = valid && m2[s] + rr < rp2_keep;
