@@ -243,9 +243,12 @@ __global__ void __launch_bounds__(256) k_pme_spread(PmeArgs a) { griddep_wait();
 // brick spread's own (same expressions), and integer sums do not depend on the order, so
 // the grid is bit-identical to the brick spread's; with no brick lists the bin, scan and
 // scatter launches disappear, which is what a small system's step is made of.
+// Four threads per atom, one z layer of its stencil each (more threads in flight for
+// the small systems this mode serves).
 __global__ void __launch_bounds__(256) k_pme_spread_atoms(PmeArgs a) {
   griddep_wait();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t >> 2, jz = t & 3;
   if (i >= a.n) return;
   const int Kx = a.K[0], Ky = a.K[1], Kz = a.K[2];
   const float4 r = a.pos4[i];
@@ -258,15 +261,15 @@ __global__ void __launch_bounds__(256) k_pme_spread_atoms(PmeArgs a) {
   bsp4(tz, wz, nullptr);
   const float q = r.w * kFixQ32;
   int* g = reinterpret_cast<int*>(a.grid);
-#pragma unroll
-  for (int jz = 0; jz < 4; ++jz) {
+  const float wzj = jz == 0 ? wz[0] : (jz == 1 ? wz[1] : (jz == 2 ? wz[2] : wz[3]));
+  {
     int z = kz - jz;
     z += z < 0 ? Kz : 0;
 #pragma unroll
     for (int jy = 0; jy < 4; ++jy) {
       int y = ky - jy;
       y += y < 0 ? Ky : 0;
-      const float qzy = q * wz[jz] * wy[jy];
+      const float qzy = q * wzj * wy[jy];
       int* row = g + ((size_t)z * Ky + y) * Kx;
 #pragma unroll
       for (int jx = 0; jx < 4; ++jx) {
@@ -1257,7 +1260,7 @@ void launch_pme(const PmeArgs& a_in, bool energy, cudaStream_t st) {
   const size_t sp = (size_t)(a.B[0] + 3) * (a.B[1] + 3) * (a.B[2] + 3) * sizeof(int);
   if (a.gather == 3) {
     cudaMemsetAsync(a.grid, 0, (size_t)a.K[0] * a.K[1] * a.K[2] * sizeof(float), st);
-    launch_pdl(k_pme_spread_atoms, dim3((a.n + 255) / 256), dim3(256), 0, st, a);
+    launch_pdl(k_pme_spread_atoms, dim3((4 * a.n + 255) / 256), dim3(256), 0, st, a);
   } else {
     launch_pdl(k_pme_zero, dim3((nbr + 255) / 256), dim3(256), 0, st, a);
     launch_pdl(k_pme_bin, dim3((a.n + 255) / 256), dim3(256), 0, st, a);
