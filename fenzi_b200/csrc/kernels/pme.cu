@@ -519,9 +519,12 @@ __global__ void __launch_bounds__(256) k_fft_x_c2r(PmeArgs a, FftPlan pl, int nl
 // its region and compute in two long serial phases).
 __device__ __forceinline__ void pme_gather_atoms_body(const PmeArgs& a, int bid, int nbid) {
   griddep_wait();
+  // four threads per atom, one z layer of its stencil each; the layer sums meet as
+  // (l0 + l1) + (l2 + l3), the order every gather uses
   const int t = bid * blockDim.x + threadIdx.x;
-  if (t >= a.n) return;
-  const int i = a.gather == 3 ? t : a.brick_atoms[t];  // mode 3: no brick lists, atom order
+  const int ta = t >> 2, jz = t & 3;
+  const bool valid = ta < a.n;
+  const int i = !valid ? 0 : (a.gather == 3 ? ta : a.brick_atoms[ta]);  // mode 3: atom order
   const int Kx = a.K[0], Ky = a.K[1], Kz = a.K[2];
   const float4 r = a.pos4[i];
   float tx, ty, tz, wx[4], wy[4], wz[4], dx[4], dy[4], dz[4];
@@ -531,30 +534,36 @@ __device__ __forceinline__ void pme_gather_atoms_body(const PmeArgs& a, int bid,
   bsp4(tx, wx, dx);
   bsp4(ty, wy, dy);
   bsp4(tz, wz, dz);
+  const float wzj = jz == 0 ? wz[0] : (jz == 1 ? wz[1] : (jz == 2 ? wz[2] : wz[3]));
+  const float dzj = jz == 0 ? dz[0] : (jz == 1 ? dz[1] : (jz == 2 ? dz[2] : dz[3]));
+  int z = kz - jz;
+  z += z < 0 ? Kz : 0;
   float gx = 0.f, gy = 0.f, gz = 0.f;
 #pragma unroll
-  for (int jz = 0; jz < 4; ++jz) {
-    int z = kz - jz;
-    z += z < 0 ? Kz : 0;
+  for (int jy = 0; jy < 4; ++jy) {
+    int y = ky - jy;
+    y += y < 0 ? Ky : 0;
+    const float* row = a.grid + ((size_t)z * Ky + y) * Kx;
+    float sx = 0.f, sdx = 0.f;
 #pragma unroll
-    for (int jy = 0; jy < 4; ++jy) {
-      int y = ky - jy;
-      y += y < 0 ? Ky : 0;
-      const float* row = a.grid + ((size_t)z * Ky + y) * Kx;
-      float sx = 0.f, sdx = 0.f;
-#pragma unroll
-      for (int jx = 0; jx < 4; ++jx) {
-        int x = kx - jx;
-        x += x < 0 ? Kx : 0;
-        const float phi = __ldg(row + x);
-        sx = fmaf(wx[jx], phi, sx);
-        sdx = fmaf(dx[jx], phi, sdx);
-      }
-      gx = fmaf(sdx, wy[jy] * wz[jz], gx);
-      gy = fmaf(sx, dy[jy] * wz[jz], gy);
-      gz = fmaf(sx, wy[jy] * dz[jz], gz);
+    for (int jx = 0; jx < 4; ++jx) {
+      int x = kx - jx;
+      x += x < 0 ? Kx : 0;
+      const float phi = valid ? __ldg(row + x) : 0.f;
+      sx = fmaf(wx[jx], phi, sx);
+      sdx = fmaf(dx[jx], phi, sdx);
     }
+    gx = fmaf(sdx, wy[jy] * wzj, gx);
+    gy = fmaf(sx, dy[jy] * wzj, gy);
+    gz = fmaf(sx, wy[jy] * dzj, gz);
   }
+  gx += __shfl_xor_sync(0xffffffffu, gx, 1);
+  gy += __shfl_xor_sync(0xffffffffu, gy, 1);
+  gz += __shfl_xor_sync(0xffffffffu, gz, 1);
+  gx += __shfl_xor_sync(0xffffffffu, gx, 2);
+  gy += __shfl_xor_sync(0xffffffffu, gy, 2);
+  gz += __shfl_xor_sync(0xffffffffu, gz, 2);
+  if (!valid || jz != 0) return;
   const float q = r.w;
   const int n = a.n;
   red_add(a.facc + i, to_fix(-q * gx * (float)Kx * a.p.inv_box.x));
@@ -608,9 +617,12 @@ __device__ __forceinline__ void pme_gather_body(const PmeArgs& a, int bid, int n
     bsp4(tx, wx, dx);
     bsp4(ty, wy, dy);
     bsp4(tz, wz, dz);
-    float gx = 0.f, gy = 0.f, gz = 0.f;
+    // one partial per z layer of the stencil, summed as (l0 + l1) + (l2 + l3): the
+    // order of the four-thread per-atom gather, so both give the same forces
+    float gx = 0.f, gy = 0.f, gz = 0.f, hx = 0.f, hy = 0.f, hz = 0.f;
 #pragma unroll
     for (int jz = 0; jz < 4; ++jz) {
+      float lx = 0.f, ly = 0.f, lz = 0.f;
 #pragma unroll
       for (int jy = 0; jy < 4; ++jy) {
         const float* row = phi_reg + ((kz - jz) * Ey + (ky - jy)) * Ex + kx;
@@ -621,11 +633,24 @@ __device__ __forceinline__ void pme_gather_body(const PmeArgs& a, int bid, int n
           sx = fmaf(wx[jx], phi, sx);
           sdx = fmaf(dx[jx], phi, sdx);
         }
-        gx = fmaf(sdx, wy[jy] * wz[jz], gx);
-        gy = fmaf(sx, dy[jy] * wz[jz], gy);
-        gz = fmaf(sx, wy[jy] * dz[jz], gz);
+        lx = fmaf(sdx, wy[jy] * wz[jz], lx);
+        ly = fmaf(sx, dy[jy] * wz[jz], ly);
+        lz = fmaf(sx, wy[jy] * dz[jz], lz);
+      }
+      // layers 0 and 1 into g, layers 2 and 3 into h
+      if (jz == 0 || jz == 2) {
+        (jz == 0 ? gx : hx) = lx;
+        (jz == 0 ? gy : hy) = ly;
+        (jz == 0 ? gz : hz) = lz;
+      } else {
+        (jz == 1 ? gx : hx) += lx;
+        (jz == 1 ? gy : hy) += ly;
+        (jz == 1 ? gz : hz) += lz;
       }
     }
+    gx += hx;
+    gy += hy;
+    gz += hz;
     const float q = r.w;
     red_add(a.facc + i, to_fix(-q * gx * (float)Kx * a.p.inv_box.x));
     red_add(a.facc + n + i, to_fix(-q * gy * (float)Ky * a.p.inv_box.y));
@@ -1306,7 +1331,7 @@ void launch_pme(const PmeArgs& a_in, bool energy, cudaStream_t st) {
   if (gmode == 1 || (gmode == 0 && (size_t)a.n <= (size_t)kGatherBrickAtoms * nbr))
     launch_pdl(k_pme_gather, dim3(nbr), dim3(256), sp, st, a);
   else
-    launch_pdl(k_pme_gather_atoms, dim3((a.n + 255) / 256), dim3(256), 0, st, a);
+    launch_pdl(k_pme_gather_atoms, dim3((4 * a.n + 255) / 256), dim3(256), 0, st, a);
 }
 
 // ------------------------------------------------------------------ batched PME
