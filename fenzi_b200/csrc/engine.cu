@@ -613,8 +613,10 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
     FZ_CUDA(cudaMemcpyAsync(&st_h, e->status, sizeof(int), cudaMemcpyDeviceToHost, e->st));
     FZ_CUDA(cudaStreamSynchronize(e->st));
   }
-  // the prune: a warp per i-block fills the GPU above ~16 blocks per SM; below, one CTA
-  // of 8 warps per block (the same lists, so the same forces); FZ_PRUNE_SPLIT=0/1 forces it
+  // the outer-list build and the prune: a warp per i-block fills the GPU above ~16
+  // blocks per SM; below, one CTA of 8 warps per block (the same lists, so the same
+  // forces; 9,000 atoms 60.9 -> 54.9 us per step with the split build); FZ_PRUNE_SPLIT=0/1
+  // forces it
   {
     e->prune_split = (nblk < 16 * e->n_sm && fzk::prune_split_fits(e->ocap)) ? 1 : 0;
     if (const char* v = std::getenv("FZ_PRUNE_SPLIT"))

@@ -241,112 +241,138 @@ __device__ __forceinline__ float box_gap2(float3 d, float3 h) {
   return gx * gx + gy * gy + gz * gz;
 }
 
-// Outer pair list, warp per i-block: every atom of a block J >= I (Newton's third law),
-// at every periodic image, whose position lies within rlist of block I's bounding box.
-// The diagonal block (J == I, no image) is implicit and not stored.  Entries append to
-// the block's own region outer[I * ocap ...] in a fixed order (deterministic).
-__device__ __forceinline__ void rb_outer_body(const RebuildArgs& A, int bid, int nbid) {
-  griddep_wait();
-  const SysParams p = A.p;
-  const int* __restrict__ flag = A.flag;
-  const int* __restrict__ counters = A.counters;
-  const int* __restrict__ perm = A.perm;
-  const float4* __restrict__ xyzq_s = A.xyzq_s;
-  const float4* __restrict__ bb_lo = A.bb_lo;
-  const float4* __restrict__ bb_hi = A.bb_hi;
-  const int* __restrict__ blk_col = A.blk_col;
-  const int* __restrict__ col_start = A.col_start;
-  int dcx = A.dcx;
-  int dcy = A.dcy;
-  int all_images = A.all_images;
-  uint32_t* outer = A.outer;
-  int* outer_n = A.outer_n;
-  int ocap = A.ocap;
-  const int* __restrict__ xn = A.xn;
-  const int* __restrict__ xs = A.xs;
-  int xmax = A.xmax;
-  int* status = A.status;
-
-  if (!*flag) return;
-  const int nblk = counters[CNT_SLOTS] >> 5;
+// Outer pair list of i-block I: every atom of a block J >= I (Newton's third law), at
+// every periodic image, whose position lies within rlist of block I's bounding box.
+// The diagonal block (J == I, no image) is implicit and not stored.  Candidate j blocks
+// are those of the columns within rlist in x-y (periodic column offsets carry the x/y
+// image), each tested in z at its minimum image (or at all three z images for small
+// boxes).  One warp walks column offsets it0 .. it1 - 1 (row-major over (oy, ox)) in
+// order; with STORE it writes the entries from out[base + 0] on, else it only counts
+// them.  Returns the number of entries met (stored or not).
+template <bool STORE>
+__device__ __forceinline__ int outer_scan(const RebuildArgs& A, int I, int it0, int it1, uint32_t* out, int base) {
+  const SysParams& p = A.p;
   const int lane = threadIdx.x & 31;
-  const int I = bid * 8 + (threadIdx.x >> 5);
-  if (I >= nblk) return;
-  const float4 li = bb_lo[I], hi4 = bb_hi[I];
+  const float4 li = A.bb_lo[I], hi4 = A.bb_hi[I];
   const float3 ci = make_float3(0.5f * (li.x + hi4.x), 0.5f * (li.y + hi4.y), 0.5f * (li.z + hi4.z));
   const float3 hi = make_float3(0.5f * (hi4.x - li.x), 0.5f * (hi4.y - li.y), 0.5f * (hi4.z - li.z));
   const float rl2 = p.rlist * p.rlist;
-  uint32_t* out = outer + (size_t)I * ocap;
-  int count = 0;
-  // candidate j blocks: the blocks of the columns within rlist in x-y (periodic column
-  // offsets carry the x/y image), each tested in z at its minimum image (or at all three
-  // z images for small boxes)
-  const int cI = blk_col[I];
+  const int cI = A.blk_col[I];
   const int cx = cI % p.ncol[0], cy = cI / p.ncol[0];
-  const int nz = all_images ? 3 : 1;
-  for (int oy = -dcy; oy <= dcy; ++oy) {
+  const int nz = A.all_images ? 3 : 1;
+  const int nox = 2 * A.dcx + 1;
+  int count = 0;
+  for (int it = it0; it < it1; ++it) {
+    const int oy = it / nox - A.dcy, ox = it % nox - A.dcx;
     int yy = cy + oy;
     const int sy = yy < 0 ? -1 : (yy >= p.ncol[1] ? 1 : 0);
     yy -= sy * p.ncol[1];
-    for (int ox = -dcx; ox <= dcx; ++ox) {
-      int xx = cx + ox;
-      const int sx = xx < 0 ? -1 : (xx >= p.ncol[0] ? 1 : 0);
-      xx -= sx * p.ncol[0];
-      const int col = yy * p.ncol[0] + xx;
-      const int b0 = col_start[col] >> 5, b1 = col_start[col + 1] >> 5;
-      for (int J0 = b0; J0 < b1; J0 += 32) {
-        const int J = J0 + lane;
-        const bool inr = J < b1 && J >= I;
-        float3 cj = make_float3(0.f, 0.f, 0.f), hj = cj;
+    int xx = cx + ox;
+    const int sx = xx < 0 ? -1 : (xx >= p.ncol[0] ? 1 : 0);
+    xx -= sx * p.ncol[0];
+    const int col = yy * p.ncol[0] + xx;
+    const int b0 = A.col_start[col] >> 5, b1 = A.col_start[col + 1] >> 5;
+    for (int J0 = b0; J0 < b1; J0 += 32) {
+      const int J = J0 + lane;
+      const bool inr = J < b1 && J >= I;
+      float3 cj = make_float3(0.f, 0.f, 0.f), hj = cj;
+      if (inr) {
+        const float4 lj = A.bb_lo[J], hj4 = A.bb_hi[J];
+        cj = make_float3(0.5f * (lj.x + hj4.x), 0.5f * (lj.y + hj4.y), 0.5f * (lj.z + hj4.z));
+        hj = make_float3(0.5f * (hj4.x - lj.x), 0.5f * (hj4.y - lj.y), 0.5f * (hj4.z - lj.z));
+      }
+      for (int iz = 0; iz < nz; ++iz) {
+        bool pass = false;
+        int code = kNoShift;
         if (inr) {
-          const float4 lj = bb_lo[J], hj4 = bb_hi[J];
-          cj = make_float3(0.5f * (lj.x + hj4.x), 0.5f * (lj.y + hj4.y), 0.5f * (lj.z + hj4.z));
-          hj = make_float3(0.5f * (hj4.x - lj.x), 0.5f * (hj4.y - lj.y), 0.5f * (hj4.z - lj.z));
+          float3 d = make_float3(cj.x - ci.x + sx * p.box.x, cj.y - ci.y + sy * p.box.y, cj.z - ci.z);
+          const float sz = A.all_images ? (float)(iz - 1) : -rintf(d.z * p.inv_box.z);
+          d.z += sz * p.box.z;
+          code = (sx + 1) + 3 * (sy + 1) + 9 * ((int)sz + 1);
+          pass = box_gap2(d, make_float3(hi.x + hj.x, hi.y + hj.y, hi.z + hj.z)) < rl2;
+          // the self block: its diagonal is implicit, each +-image pair is taken once
+          if (J == I && code >= kNoShift) pass = false;
         }
-        for (int iz = 0; iz < nz; ++iz) {
-          bool pass = false;
-          int code = kNoShift;
-          if (inr) {
-            float3 d = make_float3(cj.x - ci.x + sx * p.box.x, cj.y - ci.y + sy * p.box.y, cj.z - ci.z);
-            const float sz = all_images ? (float)(iz - 1) : -rintf(d.z * p.inv_box.z);
-            d.z += sz * p.box.z;
-            code = (sx + 1) + 3 * (sy + 1) + 9 * ((int)sz + 1);
-            pass = box_gap2(d, make_float3(hi.x + hj.x, hi.y + hj.y, hi.z + hj.z)) < rl2;
-            // the self block: its diagonal is implicit, each +-image pair is taken once
-            if (J == I && code >= kNoShift) pass = false;
+        unsigned bal = __ballot_sync(0xffffffffu, pass);
+        while (bal) {
+          const int src = __ffs(bal) - 1;
+          bal &= bal - 1;
+          const int Jc = J0 + src;
+          const int cc = __shfl_sync(0xffffffffu, code, src);
+          const int s = Jc * 32 + lane;
+          const float3 sh = shift_of(cc, p);
+          const float4 r = A.xyzq_s[s];
+          const float3 d = make_float3(r.x + sh.x - ci.x, r.y + sh.y - ci.y, r.z + sh.z - ci.z);
+          const bool ok = A.perm[s] >= 0 && box_gap2(d, hi) < rl2;
+          const unsigned b2 = __ballot_sync(0xffffffffu, ok);
+          const int pos = base + count + __popc(b2 & ((1u << lane) - 1u));
+          if (STORE && ok && pos < A.ocap) {
+            // flag entries whose atom has an excluded partner in block I: only those
+            // need the prune's exclusion-mask walk
+            uint32_t fl = 0u;
+            const int m = A.xn[s];
+            for (int k = 0; k < m; ++k)
+              if ((A.xs[(size_t)s * A.xmax + k] >> 5) == I) fl = kExclBit;
+            out[pos] = (uint32_t)s | fl | ((uint32_t)cc << kSlotBits);
           }
-          unsigned bal = __ballot_sync(0xffffffffu, pass);
-          while (bal) {
-            const int src = __ffs(bal) - 1;
-            bal &= bal - 1;
-            const int Jc = J0 + src;
-            const int cc = __shfl_sync(0xffffffffu, code, src);
-            const int s = Jc * 32 + lane;
-            const float3 sh = shift_of(cc, p);
-            const float4 r = xyzq_s[s];
-            const float3 d = make_float3(r.x + sh.x - ci.x, r.y + sh.y - ci.y, r.z + sh.z - ci.z);
-            const bool ok = perm[s] >= 0 && box_gap2(d, hi) < rl2;
-            const unsigned b2 = __ballot_sync(0xffffffffu, ok);
-            const int pos = count + __popc(b2 & ((1u << lane) - 1u));
-            if (ok && pos < ocap) {
-              // flag entries whose atom has an excluded partner in block I: only those
-              // need the prune's exclusion-mask walk
-              uint32_t fl = 0u;
-              const int m = xn[s];
-              for (int k = 0; k < m; ++k)
-                if ((xs[(size_t)s * xmax + k] >> 5) == I) fl = kExclBit;
-              out[pos] = (uint32_t)s | fl | ((uint32_t)cc << kSlotBits);
-            }
-            count += __popc(b2);
-          }
+          count += __popc(b2);
         }
       }
     }
   }
+  return count;
+}
+
+// warp per i-block; entries append to the block's own region outer[I * ocap ...] in a
+// fixed order (deterministic)
+__device__ __forceinline__ void rb_outer_body(const RebuildArgs& A, int bid, int nbid) {
+  griddep_wait();
+  if (!*A.flag) return;
+  const int nblk = A.counters[CNT_SLOTS] >> 5;
+  const int lane = threadIdx.x & 31;
+  const int I = bid * 8 + (threadIdx.x >> 5);
+  if (I >= nblk) return;
+  const int nit = (2 * A.dcy + 1) * (2 * A.dcx + 1);
+  const int count = outer_scan<true>(A, I, 0, nit, A.outer + (size_t)I * A.ocap, 0);
   if (lane == 0) {
-    outer_n[I] = min(count, ocap);
-    if (count > ocap) atomicOr(status, ST_TILE_OVERFLOW);
+    A.outer_n[I] = min(count, A.ocap);
+    if (count > A.ocap) atomicOr(A.status, ST_TILE_OVERFLOW);
   }
+}
+
+// The same list with one CTA of kOuterWarps warps per i-block, for systems with too few
+// blocks to fill the GPU with a warp per block: the column offsets are cut into
+// contiguous runs, one per warp; each warp counts its run's entries, then stores them
+// after those of the runs before it, so the list is entry for entry the one above.
+constexpr int kOuterWarps = 8;
+
+__device__ __forceinline__ void rb_outer_split_body(const RebuildArgs& A, int I) {
+  griddep_wait();
+  if (!*A.flag) return;
+  const int nblk = A.counters[CNT_SLOTS] >> 5;
+  if (I >= nblk) return;
+  __shared__ int wcount[kOuterWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nit = (2 * A.dcy + 1) * (2 * A.dcx + 1);
+  const int it0 = (warp * nit) / kOuterWarps, it1 = ((warp + 1) * nit) / kOuterWarps;
+  const int mine = outer_scan<false>(A, I, it0, it1, nullptr, 0);
+  if (lane == 0) wcount[warp] = mine;
+  __syncthreads();
+  int base = 0, total = 0;
+  for (int w = 0; w < kOuterWarps; ++w) {
+    base += w < warp ? wcount[w] : 0;
+    total += wcount[w];
+  }
+  outer_scan<true>(A, I, it0, it1, A.outer + (size_t)I * A.ocap, base);
+  if (threadIdx.x == 0) {
+    A.outer_n[I] = min(total, A.ocap);
+    if (total > A.ocap) atomicOr(A.status, ST_TILE_OVERFLOW);
+  }
+}
+
+__global__ void __launch_bounds__(kOuterWarps * 32) k_rb_outer_split(RebuildArgs a) {
+  griddep_wait();
+  rb_outer_split_body(a, blockIdx.x);
 }
 
 __global__ void __launch_bounds__(256) k_rb_outer(RebuildArgs a) { griddep_wait(); rb_outer_body(a, blockIdx.x, gridDim.x); }
@@ -847,7 +873,10 @@ void launch_rebuild_build(const RebuildArgs& a, cudaStream_t st) {
   launch_pdl(k_rb_scatter, dim3((p.n + 255) / 256), dim3(256), 0, st, a);
   launch_pdl(k_rb_colsort, dim3(ncol), dim3(256), kColCap * sizeof(unsigned long long), st, a);
   launch_pdl(k_rb_slots, dim3((p.nslots + 255) / 256), dim3(256), 0, st, a);
-  launch_pdl(k_rb_outer, dim3((maxblk + 7) / 8), dim3(256), 0, st, a);
+  if (a.prune_split)
+    launch_pdl(k_rb_outer_split, dim3(maxblk), dim3(kOuterWarps * 32), 0, st, a);
+  else
+    launch_pdl(k_rb_outer, dim3((maxblk + 7) / 8), dim3(256), 0, st, a);
 }
 
 void launch_rebuild_prune(const RebuildArgs& a, cudaStream_t st) {
