@@ -621,6 +621,8 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
     e->prune_split = (nblk < 16 * e->n_sm && fzk::prune_split_fits(e->ocap)) ? 1 : 0;
     if (const char* v = std::getenv("FZ_PRUNE_SPLIT"))
       e->prune_split = (std::atoi(v) != 0 && fzk::prune_split_fits(e->ocap)) ? 1 : 0;
+    e->outer_split = e->prune_split;
+    if (const char* v = std::getenv("FZ_OUTER_SPLIT")) e->outer_split = std::atoi(v) != 0 ? 1 : 0;
   }
   // tiles per pair-kernel work item: ~8 items per pair-kernel warp, 3 to 6 tiles, so
   // the warps run out of work together (the last items are short).  Measured (us per

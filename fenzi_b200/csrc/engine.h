@@ -113,6 +113,7 @@ struct Engine {
   bool fuse_close = true;
   // prune with one CTA per i-block (systems with few blocks; identical lists)
   int prune_split = 0;
+  int outer_split = 0;
   bool use_graph = true;
   // With cond_graph (env FZ_GRAPH_COND=1) the rebuild and prune kernels of captured
   // steps are the bodies of two conditional IF nodes set from the device flags, else
@@ -240,6 +241,7 @@ struct Engine {
     a.items = items;
     a.chunk = chunk;
     a.prune_split = prune_split;
+    a.outer_split = outer_split;
     a.blk_col = blk_col;
     a.dcx = dcx;
     a.dcy = dcy;

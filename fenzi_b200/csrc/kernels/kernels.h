@@ -69,7 +69,8 @@ struct RebuildArgs {
   float4* pos_prune;
   int2* items;   // pair-kernel work items (i-block, first tile)
   int chunk;     // tiles per work item
-  int prune_split;  // 1: outer-list build and prune with a CTA per i-block (small systems), same lists
+  int prune_split;  // 1: prune with a CTA per i-block (small systems), same lists
+  int outer_split;  // 1: outer-list build with a CTA per i-block, same lists
 };
 // whether the CTA-per-block prune's shared memory (kNG x ocap entries) fits
 bool prune_split_fits(int ocap);

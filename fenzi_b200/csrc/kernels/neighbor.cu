@@ -873,7 +873,7 @@ void launch_rebuild_build(const RebuildArgs& a, cudaStream_t st) {
   launch_pdl(k_rb_scatter, dim3((p.n + 255) / 256), dim3(256), 0, st, a);
   launch_pdl(k_rb_colsort, dim3(ncol), dim3(256), kColCap * sizeof(unsigned long long), st, a);
   launch_pdl(k_rb_slots, dim3((p.nslots + 255) / 256), dim3(256), 0, st, a);
-  if (a.prune_split)
+  if (a.outer_split)
     launch_pdl(k_rb_outer_split, dim3(maxblk), dim3(kOuterWarps * 32), 0, st, a);
   else
     launch_pdl(k_rb_outer, dim3((maxblk + 7) / 8), dim3(256), 0, st, a);
