@@ -411,7 +411,9 @@ static fz_status build_engine(fz_system* s, int device, void* stream) {
   }
   if ((r = e->upload(&e->excl_off, t.excl_off)) || (r = e->upload(&e->excl_idx, t.excl_idx))) return r;
   for (int i = 0; i < n; ++i) e->xmax = std::max(e->xmax, t.excl_off[i + 1] - t.excl_off[i]);
-  if ((r = e->alloc(&e->xn, nslots)) || (r = e->alloc(&e->xs, (size_t)nslots * e->xmax))) return r;
+  if ((r = e->alloc(&e->xn, nslots)) || (r = e->alloc(&e->xs, (size_t)nslots * e->xmax)) ||
+      (r = e->alloc(&e->xrange, nslots)))
+    return r;
   // LJ tables with a zero padding type at index nt
   {
     const int nt1 = nt + 1;

@@ -48,6 +48,7 @@ struct Engine {
   int tiles = 0;  // pair tiles of the first pruned list (sizes the work items)
   int *excl_off = nullptr, *excl_idx = nullptr;
   int *xn = nullptr, *xs = nullptr, xmax = 1;  // per-slot excluded-partner slots
+  int2* xrange = nullptr;                          // per slot: partner block range
   int *flag = nullptr, *counters = nullptr, *status = nullptr;
   float2 *ljtab = nullptr, *lj14 = nullptr;
   // bonded
@@ -224,6 +225,7 @@ struct Engine {
     a.excl_idx = excl_idx;
     a.xn = xn;
     a.xs = xs;
+    a.xrange = xrange;
     a.xmax = xmax;
     a.masks = masks;
     a.mask_cap = mask_cap;

@@ -52,6 +52,7 @@ struct RebuildArgs {
   const int *excl_off, *excl_idx;
   int *xn, *xs;  // per slot: count and slots (stride xmax) of its excluded partners
   int xmax;
+  int2* xrange;   // per slot: lowest and highest 32-slot block holding one of its partners
   uint32_t* masks;
   int mask_cap, all_images;
   int* blk_col;   // block -> column

@@ -308,11 +308,15 @@ __device__ __forceinline__ int outer_scan(const RebuildArgs& A, int I, int it0, 
           const int pos = base + count + __popc(b2 & ((1u << lane) - 1u));
           if (STORE && ok && pos < A.ocap) {
             // flag entries whose atom has an excluded partner in block I: only those
-            // need the prune's exclusion-mask walk
+            // need the prune's exclusion-mask walk (the partner walk only when I lies
+            // in the range of the partners' blocks, which for most entries it does not)
             uint32_t fl = 0u;
-            const int m = A.xn[s];
-            for (int k = 0; k < m; ++k)
-              if ((A.xs[(size_t)s * A.xmax + k] >> 5) == I) fl = kExclBit;
+            const int2 xr = A.xrange[s];
+            if (I >= xr.x && I <= xr.y) {
+              const int m = A.xn[s];
+              for (int k = 0; k < m; ++k)
+                if ((A.xs[(size_t)s * A.xmax + k] >> 5) == I) fl = kExclBit;
+            }
             out[pos] = (uint32_t)s | fl | ((uint32_t)cc << kSlotBits);
           }
           count += __popc(b2);
@@ -405,13 +409,19 @@ __device__ __forceinline__ void rb_slots_body(const RebuildArgs& A, int bid, int
   const int sl = bid * blockDim.x + threadIdx.x;
   if (sl >= p.nslots) return;  // nslots is a multiple of 32: whole warps leave together
   const int a = perm[sl];
-  int m = 0;
+  int m = 0, blo = 0x7fffffff, bhi = -1;
   if (a >= 0) {
     const int e0 = excl_off[a];
     m = min(excl_off[a + 1] - e0, xmax);
-    for (int k = 0; k < m; ++k) xs[(size_t)sl * xmax + k] = inv_perm[excl_idx[e0 + k]];
+    for (int k = 0; k < m; ++k) {
+      const int ps = inv_perm[excl_idx[e0 + k]];
+      xs[(size_t)sl * xmax + k] = ps;
+      blo = min(blo, ps >> 5);
+      bhi = max(bhi, ps >> 5);
+    }
   }
   xn[sl] = m;
+  A.xrange[sl] = make_int2(blo, bhi);
   const int w = sl >> 5, lane = sl & 31;
   if (w >= (counters[CNT_SLOTS] >> 5)) return;  // uniform per warp
   const bool ok = a >= 0;
