@@ -305,6 +305,7 @@ __device__ __forceinline__ int outer_scan(const RebuildArgs& A, int I, int it0, 
       const int c = c0 + lane;
       bool pass = false;
       int J = 0, code = kNoShift;
+      float3 shv = make_float3(0.f, 0.f, 0.f);  // the candidate's periodic shift
       if (c < total) {
         int lo = 0, hi_ = itn - 1;  // the first offset k whose candidates end after c
         while (lo < hi_) {
@@ -324,6 +325,7 @@ __device__ __forceinline__ int outer_scan(const RebuildArgs& A, int I, int it0, 
         const float sz = A.all_images ? (float)(iz - 1) : -rintf(d.z * p.inv_box.z);
         d.z += sz * p.box.z;
         code = (sx + 1) + 3 * (sy + 1) + 9 * ((int)sz + 1);
+        shv = make_float3(sx * p.box.x, sy * p.box.y, sz * p.box.z);
         pass = box_gap2(d, make_float3(hi.x + hj.x, hi.y + hj.y, hi.z + hj.z)) < rl2;
         // the self block: its diagonal is implicit, each +-image pair is taken once
         if (J == I && code >= kNoShift) pass = false;
@@ -335,6 +337,8 @@ __device__ __forceinline__ int outer_scan(const RebuildArgs& A, int I, int it0, 
       int src = __ffs(bal) - 1;
       bal &= bal - 1;
       int cc = __shfl_sync(full, code, src);
+      float3 sh = make_float3(__shfl_sync(full, shv.x, src), __shfl_sync(full, shv.y, src),
+                              __shfl_sync(full, shv.z, src));
       int s = __shfl_sync(full, J, src) * 32 + lane;
       float4 r = A.xyzq_s[s];
       int pm = A.perm[s];
@@ -344,16 +348,18 @@ __device__ __forceinline__ int outer_scan(const RebuildArgs& A, int I, int it0, 
         int cn = 0, sn = 0, pmn = 0;
         float4 rn = r;
         int2 xrn = xr;
+        float3 shn = sh;
         if (more) {
           const int nsrc = __ffs(bal) - 1;
           bal &= bal - 1;
           cn = __shfl_sync(full, code, nsrc);
+          shn = make_float3(__shfl_sync(full, shv.x, nsrc), __shfl_sync(full, shv.y, nsrc),
+                            __shfl_sync(full, shv.z, nsrc));
           sn = __shfl_sync(full, J, nsrc) * 32 + lane;
           rn = A.xyzq_s[sn];
           pmn = A.perm[sn];
           if (STORE) xrn = A.xrange[sn];
         }
-        const float3 sh = shift_of(cc, p);
         const float3 d = make_float3(r.x + sh.x - ci.x, r.y + sh.y - ci.y, r.z + sh.z - ci.z);
         const bool ok = pm >= 0 && box_gap2(d, hi) < rl2;
         const unsigned b2 = __ballot_sync(full, ok);
@@ -373,6 +379,7 @@ __device__ __forceinline__ int outer_scan(const RebuildArgs& A, int I, int it0, 
         count += __popc(b2);
         if (!more) break;
         cc = cn;
+        sh = shn;
         s = sn;
         r = rn;
         pm = pmn;
@@ -798,7 +805,7 @@ __device__ __forceinline__ void prune_body(const RebuildArgs& A, int bid, int nb
   }
 }
 
-__global__ void __launch_bounds__(256, 6) k_prune(RebuildArgs a) { griddep_wait(); prune_body(a, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(256, 4) k_prune(RebuildArgs a) { griddep_wait(); prune_body(a, blockIdx.x, gridDim.x); }
 __global__ void __launch_bounds__(256, 6) k_prune_b(const RebuildArgs* __restrict__ args, const int4* __restrict__ tab) { griddep_wait();
   const int4 t = tab[blockIdx.x];
   const RebuildArgs a = args[t.x];
