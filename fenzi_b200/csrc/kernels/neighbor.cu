@@ -251,14 +251,8 @@ __device__ __forceinline__ float box_gap2(float3 d, float3 h) {
 // them.  Returns the number of entries met (stored or not).
 template <bool STORE>
 __device__ __forceinline__ int outer_scan(const RebuildArgs& A, int I, int it0, int it1, uint32_t* out, int base) {
-  // per warp (8 per CTA), for up to 32 column offsets at a time: [0] inclusive end of
-  // the offset's candidates, [1] its first block J >= I, [2] its x-y image code, [3] its
-  // number of blocks
-  __shared__ int cinfo_all[8][4][32];
-  int(*cinfo)[32] = cinfo_all[(threadIdx.x >> 5) & 7];
   const SysParams& p = A.p;
   const int lane = threadIdx.x & 31;
-  const unsigned full = 0xffffffffu;
   const float4 li = A.bb_lo[I], hi4 = A.bb_hi[I];
   const float3 ci = make_float3(0.5f * (li.x + hi4.x), 0.5f * (li.y + hi4.y), 0.5f * (li.z + hi4.z));
   const float3 hi = make_float3(0.5f * (hi4.x - li.x), 0.5f * (hi4.y - li.y), 0.5f * (hi4.z - li.z));
@@ -268,125 +262,67 @@ __device__ __forceinline__ int outer_scan(const RebuildArgs& A, int I, int it0, 
   const int nz = A.all_images ? 3 : 1;
   const int nox = 2 * A.dcx + 1;
   int count = 0;
-  for (int itb = it0; itb < it1; itb += 32) {
-    // lane k: column offset itb + k, its blocks J >= I (Newton's third law) and images
-    const int itn = min(32, it1 - itb);
-    int jb = 0, nbk = 0, sxy = 4;
-    if (lane < itn) {
-      const int it = itb + lane;
-      const int oy = it / nox - A.dcy, ox = it % nox - A.dcx;
-      int yy = cy + oy;
-      const int sy = yy < 0 ? -1 : (yy >= p.ncol[1] ? 1 : 0);
-      yy -= sy * p.ncol[1];
-      int xx = cx + ox;
-      const int sx = xx < 0 ? -1 : (xx >= p.ncol[0] ? 1 : 0);
-      xx -= sx * p.ncol[0];
-      const int col = yy * p.ncol[0] + xx;
-      const int b0 = A.col_start[col] >> 5, b1 = A.col_start[col + 1] >> 5;
-      jb = max(b0, I);
-      nbk = max(0, b1 - jb);
-      sxy = (sx + 1) + 3 * (sy + 1);
-    }
-    int incl = nbk * nz;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int v = __shfl_up_sync(full, incl, o);
-      if (lane >= o) incl += v;
-    }
-    const int total = __shfl_sync(full, incl, 31);
-    __syncwarp();
-    cinfo[0][lane] = incl;
-    cinfo[1][lane] = jb;
-    cinfo[2][lane] = sxy;
-    cinfo[3][lane] = nbk;
-    __syncwarp();
-    // candidates (column offset, z image, block) in that order, 32 at a time
-    for (int c0 = 0; c0 < total; c0 += 32) {
-      const int c = c0 + lane;
-      bool pass = false;
-      int J = 0, code = kNoShift;
-      float3 shv = make_float3(0.f, 0.f, 0.f);  // the candidate's periodic shift
-      if (c < total) {
-        int lo = 0, hi_ = itn - 1;  // the first offset k whose candidates end after c
-        while (lo < hi_) {
-          const int mid = (lo + hi_) >> 1;
-          if (cinfo[0][mid] > c) hi_ = mid;
-          else lo = mid + 1;
-        }
-        const int nb = cinfo[3][lo];
-        const int within = c - (cinfo[0][lo] - nb * nz);
-        const int iz = within / nb;
-        J = cinfo[1][lo] + (within - iz * nb);
-        const int sx = cinfo[2][lo] % 3 - 1, sy = cinfo[2][lo] / 3 - 1;
+  for (int it = it0; it < it1; ++it) {
+    const int oy = it / nox - A.dcy, ox = it % nox - A.dcx;
+    int yy = cy + oy;
+    const int sy = yy < 0 ? -1 : (yy >= p.ncol[1] ? 1 : 0);
+    yy -= sy * p.ncol[1];
+    int xx = cx + ox;
+    const int sx = xx < 0 ? -1 : (xx >= p.ncol[0] ? 1 : 0);
+    xx -= sx * p.ncol[0];
+    const int col = yy * p.ncol[0] + xx;
+    const int b0 = A.col_start[col] >> 5, b1 = A.col_start[col + 1] >> 5;
+    for (int J0 = b0; J0 < b1; J0 += 32) {
+      const int J = J0 + lane;
+      const bool inr = J < b1 && J >= I;
+      float3 cj = make_float3(0.f, 0.f, 0.f), hj = cj;
+      if (inr) {
         const float4 lj = A.bb_lo[J], hj4 = A.bb_hi[J];
-        const float3 cj = make_float3(0.5f * (lj.x + hj4.x), 0.5f * (lj.y + hj4.y), 0.5f * (lj.z + hj4.z));
-        const float3 hj = make_float3(0.5f * (hj4.x - lj.x), 0.5f * (hj4.y - lj.y), 0.5f * (hj4.z - lj.z));
-        float3 d = make_float3(cj.x - ci.x + sx * p.box.x, cj.y - ci.y + sy * p.box.y, cj.z - ci.z);
-        const float sz = A.all_images ? (float)(iz - 1) : -rintf(d.z * p.inv_box.z);
-        d.z += sz * p.box.z;
-        code = (sx + 1) + 3 * (sy + 1) + 9 * ((int)sz + 1);
-        shv = make_float3(sx * p.box.x, sy * p.box.y, sz * p.box.z);
-        pass = box_gap2(d, make_float3(hi.x + hj.x, hi.y + hj.y, hi.z + hj.z)) < rl2;
-        // the self block: its diagonal is implicit, each +-image pair is taken once
-        if (J == I && code >= kNoShift) pass = false;
+        cj = make_float3(0.5f * (lj.x + hj4.x), 0.5f * (lj.y + hj4.y), 0.5f * (lj.z + hj4.z));
+        hj = make_float3(0.5f * (hj4.x - lj.x), 0.5f * (hj4.y - lj.y), 0.5f * (hj4.z - lj.z));
       }
-      // the passing blocks in candidate order, each one's atoms loaded while the
-      // previous one's are tested
-      unsigned bal = __ballot_sync(full, pass);
-      if (!bal) continue;
-      int src = __ffs(bal) - 1;
-      bal &= bal - 1;
-      int cc = __shfl_sync(full, code, src);
-      float3 sh = make_float3(__shfl_sync(full, shv.x, src), __shfl_sync(full, shv.y, src),
-                              __shfl_sync(full, shv.z, src));
-      int s = __shfl_sync(full, J, src) * 32 + lane;
-      float4 r = A.xyzq_s[s];
-      int pm = A.perm[s];
-      int2 xr = STORE ? A.xrange[s] : make_int2(0, -1);
-      for (;;) {
-        const bool more = bal != 0;
-        int cn = 0, sn = 0, pmn = 0;
-        float4 rn = r;
-        int2 xrn = xr;
-        float3 shn = sh;
-        if (more) {
-          const int nsrc = __ffs(bal) - 1;
+      for (int iz = 0; iz < nz; ++iz) {
+        bool pass = false;
+        int code = kNoShift;
+        if (inr) {
+          float3 d = make_float3(cj.x - ci.x + sx * p.box.x, cj.y - ci.y + sy * p.box.y, cj.z - ci.z);
+          const float sz = A.all_images ? (float)(iz - 1) : -rintf(d.z * p.inv_box.z);
+          d.z += sz * p.box.z;
+          code = (sx + 1) + 3 * (sy + 1) + 9 * ((int)sz + 1);
+          pass = box_gap2(d, make_float3(hi.x + hj.x, hi.y + hj.y, hi.z + hj.z)) < rl2;
+          // the self block: its diagonal is implicit, each +-image pair is taken once
+          if (J == I && code >= kNoShift) pass = false;
+        }
+        unsigned bal = __ballot_sync(0xffffffffu, pass);
+        while (bal) {
+          const int src = __ffs(bal) - 1;
           bal &= bal - 1;
-          cn = __shfl_sync(full, code, nsrc);
-          shn = make_float3(__shfl_sync(full, shv.x, nsrc), __shfl_sync(full, shv.y, nsrc),
-                            __shfl_sync(full, shv.z, nsrc));
-          sn = __shfl_sync(full, J, nsrc) * 32 + lane;
-          rn = A.xyzq_s[sn];
-          pmn = A.perm[sn];
-          if (STORE) xrn = A.xrange[sn];
-        }
-        const float3 d = make_float3(r.x + sh.x - ci.x, r.y + sh.y - ci.y, r.z + sh.z - ci.z);
-        const bool ok = pm >= 0 && box_gap2(d, hi) < rl2;
-        const unsigned b2 = __ballot_sync(full, ok);
-        const int pos = base + count + __popc(b2 & ((1u << lane) - 1u));
-        if (STORE && ok && pos < A.ocap) {
-          // flag entries whose atom has an excluded partner in block I: only those
-          // need the prune's exclusion-mask walk (the partner walk only when I lies
-          // in the range of the partners' blocks, which for most entries it does not)
-          uint32_t fl = 0u;
-          if (I >= xr.x && I <= xr.y) {
-            const int m = A.xn[s];
-            for (int k = 0; k < m; ++k)
-              if ((A.xs[(size_t)s * A.xmax + k] >> 5) == I) fl = kExclBit;
+          const int Jc = J0 + src;
+          const int cc = __shfl_sync(0xffffffffu, code, src);
+          const int s = Jc * 32 + lane;
+          const float3 sh = shift_of(cc, p);
+          const float4 r = A.xyzq_s[s];
+          const float3 d = make_float3(r.x + sh.x - ci.x, r.y + sh.y - ci.y, r.z + sh.z - ci.z);
+          const bool ok = A.perm[s] >= 0 && box_gap2(d, hi) < rl2;
+          const unsigned b2 = __ballot_sync(0xffffffffu, ok);
+          const int pos = base + count + __popc(b2 & ((1u << lane) - 1u));
+          if (STORE && ok && pos < A.ocap) {
+            // flag entries whose atom has an excluded partner in block I: only those
+            // need the prune's exclusion-mask walk (the partner walk only when I lies
+            // in the range of the partners' blocks, which for most entries it does not)
+            uint32_t fl = 0u;
+            const int2 xr = A.xrange[s];
+            if (I >= xr.x && I <= xr.y) {
+              const int m = A.xn[s];
+              for (int k = 0; k < m; ++k)
+                if ((A.xs[(size_t)s * A.xmax + k] >> 5) == I) fl = kExclBit;
+            }
+            out[pos] = (uint32_t)s | fl | ((uint32_t)cc << kSlotBits);
           }
-          out[pos] = (uint32_t)s | fl | ((uint32_t)cc << kSlotBits);
+          count += __popc(b2);
         }
-        count += __popc(b2);
-        if (!more) break;
-        cc = cn;
-        sh = shn;
-        s = sn;
-        r = rn;
-        pm = pmn;
-        xr = xrn;
       }
     }
-    __syncwarp();
   }
   return count;
 }
